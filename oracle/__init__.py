@@ -1,0 +1,202 @@
+"""ctypes front end of the CPU FP64 oracle (rod_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by bench.py's CPU-baseline leg, always as the checker or the timed CPU
+baseline, never by the product package.
+
+``RodArrays`` holds one ragged batch of rods in the slot layout described in
+``rod_oracle.h`` (rod r owns slots ``offset[r] .. offset[r] + n_r``;
+component-major fields).  It is deliberately independent of the product's
+host code so that a layout bug on the product side cannot cancel out.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librod_oracle.so")
+
+_P = ctypes.POINTER(ctypes.c_double)
+
+
+class _OrcRods(ctypes.Structure):
+    _fields_ = [
+        ("n_rods", ctypes.c_int64),
+        ("n_slots", ctypes.c_int64),
+        ("offset", ctypes.POINTER(ctypes.c_int64)),
+        ("x", _P), ("v", _P), ("Q", _P), ("w", _P),
+        ("mass", _P), ("rest_length", _P), ("rest_voronoi", _P), ("volume", _P),
+        ("rest_sigma", _P), ("rest_kappa", _P), ("shear_diag", _P), ("bend_diag", _P),
+        ("inertia_diag", _P), ("inv_inertia", _P), ("nu_force", _P), ("nu_torque", _P),
+        ("clamp", ctypes.POINTER(ctypes.c_uint8)), ("clamp_x", _P), ("clamp_Q", _P),
+        ("end_torque", _P), ("damper_nu", _P),
+        ("gravity", ctypes.c_double * 3),
+        ("d_length", _P), ("d_dilatation", _P), ("d_tangent", _P), ("d_vdilatation", _P),
+        ("d_sigma", _P), ("d_kappa", _P), ("d_stress", _P), ("d_couple", _P),
+        ("d_loads", _P), ("d_torques", _P), ("d_accel", _P), ("d_alpha", _P),
+        ("d_dimension", _P),
+    ]
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (in-tree .so)."""
+    if force or not os.path.exists(LIB_PATH) or (
+        os.path.getmtime(LIB_PATH) < max(os.path.getmtime(os.path.join(HERE, f))
+                                         for f in ("rod_oracle.cpp", "rod_oracle.h"))):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.orc_step.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64, ctypes.c_int]
+        _lib.orc_force_eval.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_int]
+        _lib.orc_energy.argtypes = [ctypes.POINTER(_OrcRods), _P, ctypes.c_int]
+        _lib.orc_straight_rod.argtypes = [ctypes.c_int64, _P, _P, _P, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double] + [_P] * 11
+    return _lib
+
+
+STATE = ("x", "v", "Q", "w")
+PARAMS = ("mass", "rest_length", "rest_voronoi", "volume", "rest_sigma", "rest_kappa",
+          "shear_diag", "bend_diag", "inertia_diag", "inv_inertia")
+DIAG = ("d_length", "d_dilatation", "d_tangent", "d_vdilatation", "d_sigma", "d_kappa",
+        "d_stress", "d_couple", "d_loads", "d_torques", "d_accel", "d_alpha", "d_dimension")
+NCOMP = {"x": 3, "v": 3, "Q": 9, "w": 3, "rest_sigma": 3, "rest_kappa": 3, "shear_diag": 3,
+         "bend_diag": 3, "inertia_diag": 3, "inv_inertia": 3, "d_tangent": 3, "d_sigma": 3,
+         "d_kappa": 3, "d_stress": 3, "d_couple": 3, "d_loads": 3, "d_torques": 3,
+         "d_accel": 3, "d_alpha": 3}
+
+
+def straight_rod(n, origin, direction, normal, length, radius, density, youngs, shear):
+    """Reference straight-rod initializer for one rod; returns a dict of
+    per-rod arrays in the reference's shapes (3 x N, 3 x 3 x N, N)."""
+    L = lib()
+    n = int(n)
+    out = {
+        "x": np.zeros(3 * (n + 1)), "Q": np.zeros(9 * n), "l0": np.zeros(n), "D0": np.zeros(n - 1),
+        "V": np.zeros(n), "radius": np.zeros(n), "mass": np.zeros(n + 1), "J": np.zeros(3 * n),
+        "Jinv": np.zeros(3 * n), "S": np.zeros(3 * n), "B": np.zeros(3 * (n - 1)),
+    }
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(_P)
+    o, d, nm = (np.asarray(a, dtype=np.float64) for a in (origin, direction, normal))
+    rc = L.orc_straight_rod(n, f(o), f(d), f(nm), float(length), float(radius), float(density),
+                            float(youngs), float(shear), *(out[k].ctypes.data_as(_P) for k in
+                                                           ("x", "Q", "l0", "D0", "V", "radius", "mass", "J", "Jinv", "S", "B")))
+    if rc != 0:
+        raise ValueError("invalid straight rod parameters")
+    out["x"] = out["x"].reshape(3, n + 1)
+    out["Q"] = out["Q"].reshape(3, 3, n)
+    for k in ("J", "Jinv", "S"):
+        out[k] = out[k].reshape(3, n)
+    out["B"] = out["B"].reshape(3, n - 1)
+    return out
+
+
+class RodArrays:
+    """Slot-layout batch of rods for the oracle."""
+
+    def __init__(self, n_elems, damped: bool = False):
+        self.n_elems = np.asarray(n_elems, dtype=np.int64)
+        self.n_rods = len(self.n_elems)
+        self.offset = np.zeros(self.n_rods + 1, dtype=np.int64)
+        np.cumsum(self.n_elems + 1, out=self.offset[1:])
+        S = self.n_slots = int(self.offset[-1])
+        self.arrays = {}
+        for k in STATE + PARAMS:
+            self.arrays[k] = np.zeros(NCOMP.get(k, 1) * S)
+        self.damped = damped
+        if damped:
+            self.arrays["nu_force"] = np.zeros(S)
+            self.arrays["nu_torque"] = np.zeros(S)
+        self.clamp = np.zeros(self.n_rods, dtype=np.uint8)
+        self.clamp_x = np.zeros(3 * self.n_rods)
+        self.clamp_Q = np.zeros(9 * self.n_rods)
+        self.end_torque = np.zeros(3 * self.n_rods)
+        self.damper_nu = np.zeros(2 * self.n_rods)
+        self.gravity = np.zeros(3)
+        self.diag = None
+
+    # -- per-rod views in the reference's shapes --------------------------
+    def comp(self, key):
+        a = self.arrays[key]
+        return a.reshape(NCOMP.get(key, 1), self.n_slots)
+
+    def rod_view(self, key, r, count):
+        """(ncomp, count) view of rod r's first `count` slots."""
+        o = int(self.offset[r])
+        return self.comp(key)[:, o:o + count]
+
+    def set_rod(self, key, r, values):
+        values = np.asarray(values, dtype=np.float64)
+        nc = NCOMP.get(key, 1)
+        values = values.reshape(nc, -1)
+        self.rod_view(key, r, values.shape[1])[...] = values
+
+    def get_rod(self, key, r, count):
+        return self.rod_view(key, r, count).copy()
+
+    def enable_diagnostics(self):
+        self.diag = {k: np.zeros(NCOMP.get(k, 1) * self.n_slots) for k in DIAG}
+
+    def get_diag(self, key, r, count):
+        o = int(self.offset[r])
+        return self.diag[key].reshape(NCOMP.get(key, 1), self.n_slots)[:, o:o + count].copy()
+
+    # -- ctypes struct -----------------------------------------------------
+    def _struct(self):
+        s = _OrcRods()
+        s.n_rods = self.n_rods
+        s.n_slots = self.n_slots
+        s.offset = self.offset.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        for k, a in self.arrays.items():
+            setattr(s, k, a.ctypes.data_as(_P))
+        s.clamp = self.clamp.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        s.clamp_x = self.clamp_x.ctypes.data_as(_P)
+        s.clamp_Q = self.clamp_Q.ctypes.data_as(_P)
+        s.end_torque = self.end_torque.ctypes.data_as(_P)
+        s.damper_nu = self.damper_nu.ctypes.data_as(_P)
+        for i in range(3):
+            s.gravity[i] = float(self.gravity[i])
+        if self.diag is not None:
+            for k, a in self.diag.items():
+                setattr(s, k, a.ctypes.data_as(_P))
+        return s
+
+    def step(self, dt, n_steps=1, n_threads=0):
+        s = self._struct()
+        rc = lib().orc_step(ctypes.byref(s), float(dt), int(n_steps), int(n_threads))
+        if rc != 0:
+            raise RuntimeError("orc_step failed")
+
+    def force_eval(self):
+        s = self._struct()
+        if lib().orc_force_eval(ctypes.byref(s), 0) != 0:
+            raise RuntimeError("orc_force_eval failed")
+
+    def energy(self):
+        out = np.zeros(4 * self.n_rods)
+        s = self._struct()
+        if lib().orc_energy(ctypes.byref(s), out.ctypes.data_as(_P), 0) != 0:
+            raise RuntimeError("orc_energy failed")
+        return out.reshape(self.n_rods, 4)
+
+    def copy(self):
+        c = RodArrays.__new__(RodArrays)
+        c.__dict__.update(self.__dict__)
+        c.arrays = {k: a.copy() for k, a in self.arrays.items()}
+        for k in ("clamp", "clamp_x", "clamp_Q", "end_torque", "damper_nu", "gravity"):
+            setattr(c, k, getattr(self, k).copy())
+        c.diag = None if self.diag is None else {k: a.copy() for k, a in self.diag.items()}
+        return c
