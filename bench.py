@@ -1,0 +1,353 @@
+"""Rod-step throughput (element-steps/s) of the B200 FP64 drop-in.
+
+Default workload: the uneven FP64 batch — 16,384 clamped rods, n ~ U{32..512}
+elements (~4.44 M elements), gravity, analytical damper 0.1, one PositionVerlet
+step per bench step (one fused kernel launch).  Seeded synthetic inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own independent batch (seed + rank) on its
+own GPU with no data-path collective (weak scaling); the timed region is
+bracketed by a barrier and a device synchronize and the max over ranks is
+reported.  Rank 0 prints one JSON line.
+
+``--impl reference`` times the CPU restatement of the reference's scalar path
+(the oracle, OpenMP over rods on every host core) on the same workload; only
+rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "element-steps/s"
+UNIT = "element-steps/s"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+E2E_STEPS_PER_CYCLE = 100  # run_for interval between host syncs (examples/dynamic_cantilever/helpers/data.py:60 uses 100-500)
+
+
+def algorithmic_bytes(n_elems: np.ndarray, damped: bool) -> float:
+    """Bytes one step must move at minimum: the state x, v (nodes) and Q, w
+    (elements) read and written once, plus each parameter read once
+    (m per node; l0, sigma0, S, J per element; D0, kappa0, B per Voronoi
+    point; nu_f / nu_t for explicitly damped rods).  Derived quantities
+    (lengths, strains, curvature, loads, 1/m, 1/J) are recomputed, not counted.
+    Per element this is 432 B (448 B with explicit damping), the per-unit
+    figure times the elements of one launch."""
+    per_elem = 432.0 + (16.0 if damped else 0.0)
+    return per_elem * float(np.sum(n_elems))
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH, encoding="utf-8") as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    try:
+        with open(path, encoding="utf-8") as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"eb_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path, encoding="utf-8") as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_rate(wl, n_steps: int, budget_s: float = None, max_rods: int | None = None):
+    """Oracle (CPU restatement of the reference's scalar path) throughput on
+    this host, OpenMP over rods on every core.  Returns (rate, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle  # noqa: F401  (checker / CPU baseline only)
+    import oracle_bridge
+
+    sub = wl
+    if max_rods is not None and max_rods < len(wl.rods):
+        import copy
+
+        sub = copy.copy(wl)
+        sub.rods = wl.rods[:max_rods]
+        sub.velocities = None if wl.velocities is None else wl.velocities[:max_rods]
+        sub.rest_curvature = None if wl.rest_curvature is None else wl.rest_curvature[:max_rods]
+        sub.end_torque = None if wl.end_torque is None else wl.end_torque[:max_rods]
+    orc = oracle_bridge.oracle_from_workload(sub)
+    cores = os.cpu_count() or 1
+    orc.step(wl.dt, 1, n_threads=cores)  # warm-up
+    done, t0 = 0, time.perf_counter()
+    while True:
+        orc.step(wl.dt, 1, n_threads=cores)
+        done += 1
+        el = time.perf_counter() - t0
+        if (budget_s is None and done >= n_steps) or (budget_s is not None and el >= budget_s):
+            break
+    rate = sub.total_elements * done / el
+    sample = f"{len(sub.rods)} rods / {sub.total_elements} elements x {done} steps"
+    return rate, cores, sample
+
+
+def run_reference(args, wl_fn):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    wl = wl_fn(0)
+    cores = os.cpu_count() or 1
+    # warm-up steps, then K timed steps over the whole workload
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bridge as ob  # CPU restatement of the reference path (the checker)
+
+    orc = ob.oracle_from_workload(wl)
+    for _ in range(args.warmup):
+        orc.step(wl.dt, 1, n_threads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.step(wl.dt, 1, n_threads=cores)
+    el = time.perf_counter() - t0
+    value = wl.total_elements * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": workload_config(wl, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"whole workload ({len(wl.rods)} rods, {wl.total_elements} elements) "
+                                   f"x {args.steps} steps; CPU restatement of the reference's scalar "
+                                   "path (reference not buildable here: Blaze/TBB absent)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(wl, world):
+    return {"workload": wl.name, "rods": len(wl.rods), "elements": wl.total_elements,
+            "n_elements": [int(wl.n_elements.min()), int(wl.n_elements.max())], "dt": wl.dt,
+            "seed": wl.seed, "stepper": "PositionVerlet",
+            "constraints": "clamp(node 0) + analytical damper 0.1", "gravity": list(wl.gravity or []),
+            "parallelism": f"{world} independent rod shards (weak)" if world > 1 else "single GPU",
+            "l2": "no flush: state + parameters exceed the 126 MB L2 many times over"}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="uneven_batch")
+    ap.add_argument("--e2e-cycles", type=int, default=3)
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+
+    from elasticapp_b200 import workloads as W
+
+    wl_fn = lambda rank: W.CONFIGS[args.workload](seed=1002 + rank) if args.workload != "cantilever" \
+        else W.cantilever()
+    if args.impl == "reference":
+        return run_reference(args, wl_fn)
+
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    import elasticapp_b200 as eb
+
+    wl = wl_fn(rank)
+    sim = wl.build(device=local)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
+    t = 0.0
+    t = sim.step(eb.PositionVerlet(), t, wl.dt, args.warmup)
+    sim.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    # ---- device-timed region: exactly K steps, one launch each
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = sim.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        t = sim.step(eb.PositionVerlet(), t, wl.dt, 1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    launches = sim.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_t = torch.tensor([ms], device="cuda")
+    elems_t = torch.tensor([float(wl.total_elements)], device="cuda", dtype=torch.float64)
+    if pg is not None:
+        pg.all_reduce(ms_t, op=pg.ReduceOp.MAX)
+        pg.all_reduce(elems_t)
+    ms_max = float(ms_t.item())
+    total_elems = float(elems_t.item())
+    value = total_elems * args.steps / (ms_max / 1e3)
+
+    # ---- roofline of the step kernel (this rank)
+    peak, peak_kind = hbm_peak()
+    alg = algorithmic_bytes(wl.n_elements, damped=False)
+    per_launch_s = (ms / 1e3) / args.steps
+    achieved = alg / per_launch_s / 1e9
+    traffic = profile_traffic("rod_step_fp64", wl.name)
+
+    # ---- end to end through the public API with host buffers: each cycle
+    # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE
+    # steps and reads the state back (the reference's run_for + communicate)
+    S = sim.n_slots()
+    names = ("Position", "Velocity", "Director", "AngularVelocity")
+    ncomp = {"Position": 3, "Velocity": 3, "Director": 9, "AngularVelocity": 3}
+    host = {n: torch.empty((ncomp[n], S), dtype=torch.float64, pin_memory=True).numpy() for n in names}
+    for n in names:
+        sim.get_slots(n, out=host[n])
+    bytes_cycle = sum(8 * ncomp[n] * S for n in names)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_cycles):
+        for n in names:
+            sim.set_slots(n, host[n])
+        t = sim.step(eb.PositionVerlet(), t, wl.dt, E2E_STEPS_PER_CYCLE)
+        for n in names:
+            sim.get_slots(n, out=host[n])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if pg is not None:
+        pg.all_reduce(e2e_ms, op=pg.ReduceOp.MAX)
+    e2e_value = total_elems * E2E_STEPS_PER_CYCLE * args.e2e_cycles / (float(e2e_ms.item()) / 1e3)
+    finite = all(np.isfinite(host[n]).all() for n in names)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, sample = cpu_reference_rate(wl, 0, budget_s=args.cpu_budget_s, max_rods=2048)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": sample + " (CPU restatement of the reference's scalar path, OpenMP over rods)"}
+
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": workload_config(wl, world),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s",
+                         "kernel": "rod_step_fp64", "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cycle,
+                    "d2h_bytes_per_step": bytes_cycle, "steps_per_e2e_step": E2E_STEPS_PER_CYCLE,
+                    "cycles": args.e2e_cycles},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "state_finite": bool(finite),
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

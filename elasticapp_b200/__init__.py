@@ -1,0 +1,14 @@
+"""elasticapp_b200: B200-native Cosserat-rod step behind the reference's
+Simulator plugin surface (see include/elastica_b200.h for the C-ABI).
+
+The compute path is libelastica_b200.so (hand-written sm_100a kernels); it is
+built in-tree by ``python -m elasticapp_b200.build`` and there is no CPU
+fallback.
+"""
+from .simulator import (AnalyticalLinearDamper, Clamp, CosseratRod, CosseratRodWithoutDamping,
+                        EndTorque, GravityField, Material, PositionVerlet, RodRef, Simulator,
+                        StraightRod)
+from . import _lib
+
+__all__ = ["AnalyticalLinearDamper", "Clamp", "CosseratRod", "CosseratRodWithoutDamping", "EndTorque",
+           "GravityField", "Material", "PositionVerlet", "RodRef", "Simulator", "StraightRod", "_lib"]

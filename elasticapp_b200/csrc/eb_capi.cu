@@ -1,0 +1,722 @@
+// Host side of the C-ABI (include/elastica_b200.h): the simulator object,
+// rod registry, straight-rod initializer, device buffers and the step loop.
+//
+// The simulator mirrors the reference's Simulator/Block plugin surface
+// (elastica/Simulator/Interface/Simulator/Simulator.hpp,
+// elastica/Simulator/Interface/Systems/Module.hpp): rods are emplaced and
+// configured on the host, eb_finalize uploads them into the slot layout
+// (csrc/eb_internal.h), and eb_step runs the fused step kernels on the
+// simulator's own CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/elastica_b200.h"
+#include "eb_internal.h"
+
+namespace eb {
+cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_step_fp64_strict(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
+                              const double* state, const double* params, double* out,
+                              cudaStream_t stream);
+}  // namespace eb
+
+namespace {
+
+thread_local std::string g_last_error;
+
+eb_status fail(eb_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+#define EB_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(EB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+enum Place { kNode = 0, kElement = 1, kVoronoi = 2 };
+enum Kind { kState = 0, kParam = 1, kDiag = 2 };
+
+struct FieldInfo {
+  Place place;
+  int ncomp;
+  Kind kind;
+  int offset;  // in units of stride inside its buffer
+};
+
+const FieldInfo kFields[EB_FIELD_COUNT] = {
+    {kNode, 3, kState, eb::kX},             // EB_POSITION
+    {kNode, 3, kState, eb::kV},             // EB_VELOCITY
+    {kElement, 9, kState, eb::kQ},          // EB_DIRECTOR
+    {kElement, 3, kState, eb::kW},          // EB_ANGULAR_VELOCITY
+    {kNode, 1, kParam, eb::kMass},          // EB_MASS
+    {kElement, 1, kParam, eb::kL0},         // EB_REFERENCE_ELEMENT_LENGTH
+    {kVoronoi, 1, kParam, eb::kD0},         // EB_REFERENCE_VORONOI_LENGTH
+    {kElement, 1, kParam, eb::kVol},        // EB_ELEMENT_VOLUME
+    {kElement, 3, kParam, eb::kSig0},       // EB_REFERENCE_SHEAR_STRETCH_STRAIN
+    {kVoronoi, 3, kParam, eb::kKap0},       // EB_REFERENCE_CURVATURE
+    {kElement, 3, kParam, eb::kShear},      // EB_SHEAR_STRETCH_RIGIDITY_MATRIX
+    {kVoronoi, 3, kParam, eb::kBend},       // EB_BENDING_TWIST_RIGIDITY_MATRIX
+    {kElement, 3, kParam, eb::kJ},          // EB_MASS_SECOND_MOMENT_OF_INERTIA
+    {kElement, 3, kParam, eb::kJinv},       // EB_INV_MASS_SECOND_MOMENT_OF_INERTIA
+    {kNode, 1, kParam, eb::kNuF},           // EB_FORCE_DAMPING_RATE
+    {kElement, 1, kParam, eb::kNuT},        // EB_TORQUE_DAMPING_RATE
+    {kElement, 1, kDiag, eb::kDLength},     // EB_ELEMENT_LENGTH
+    {kElement, 1, kDiag, eb::kDDil},        // EB_ELEMENT_DILATATION
+    {kElement, 3, kDiag, eb::kDTangent},    // EB_TANGENT
+    {kVoronoi, 1, kDiag, eb::kDVDil},       // EB_VORONOI_DILATATION
+    {kElement, 3, kDiag, eb::kDSigma},      // EB_SHEAR_STRETCH_STRAIN
+    {kVoronoi, 3, kDiag, eb::kDKappa},      // EB_CURVATURE
+    {kElement, 3, kDiag, eb::kDStress},     // EB_INTERNAL_STRESS
+    {kVoronoi, 3, kDiag, eb::kDCouple},     // EB_INTERNAL_COUPLE
+    {kNode, 3, kDiag, eb::kDLoads},         // EB_INTERNAL_LOADS
+    {kElement, 3, kDiag, eb::kDTorques},    // EB_INTERNAL_TORQUES
+    {kNode, 3, kDiag, eb::kDAccel},         // EB_ACCELERATION
+    {kElement, 3, kDiag, eb::kDAlpha},      // EB_ANGULAR_ACCELERATION
+    {kElement, 1, kDiag, eb::kDDim},        // EB_ELEMENT_DIMENSION
+};
+
+int64_t place_count(Place p, int64_t n) { return p == kNode ? n + 1 : (p == kElement ? n : n - 1); }
+
+struct RodHost {
+  int64_t n = 0;
+  int32_t model = EB_ROD_UNDAMPED;
+  // local slot-layout arrays: field f component c at (f + c) * (n + 1) + j
+  std::vector<double> state, param, diag;
+  eb::RodInfo info{};
+  double damper_nu_t = 0.0;
+};
+
+}  // namespace
+
+struct eb_sim {
+  eb_config cfg{};
+  bool finalized = false;
+  std::vector<RodHost> rods;
+  double gravity[3] = {0.0, 0.0, 0.0};
+  bool has_gravity = false;
+  uint32_t sim_flags = 0;
+  bool any_damped = false;
+  // device
+  cudaStream_t stream = nullptr;
+  int64_t n_slots = 0, stride = 0;
+  std::vector<int64_t> offsets;
+  double* d_state[2] = {nullptr, nullptr};
+  double* d_param = nullptr;
+  double* d_diag = nullptr;
+  uint32_t* d_meta = nullptr;
+  eb::RodInfo* d_rods = nullptr;
+  int64_t* d_offsets = nullptr;
+  double* d_energy = nullptr;
+  int cur = 0;
+  double damper_dt = -1.0;
+  int64_t launches = 0;
+};
+
+namespace {
+
+eb_status check_sim(const eb_sim* s) {
+  if (!s) return fail(EB_ERR_INVALID_ARGUMENT, "null simulator");
+  return EB_OK;
+}
+
+eb_status set_device(const eb_sim* s) {
+  EB_CUDA(cudaSetDevice(s->cfg.device));
+  return EB_OK;
+}
+
+double norm3(const double a[3]) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+void cross3(const double m[3], const double v[3], double o[3]) {
+  o[0] = m[1] * v[2] - m[2] * v[1];
+  o[1] = m[2] * v[0] - m[0] * v[2];
+  o[2] = m[0] * v[1] - m[1] * v[0];
+}
+
+// StraightCosseratRodInitializer and the component initialize() chains:
+// positions by linspace (elastica/Utilities/Generators.hpp:86-119), directors
+// from the normal and tangent (elastica/Utilities/Math/Orthogonal.cpp:32-55,
+// 98-116), rest geometry (CosseratRodSpanwiseGeometry.hpp:526-545), cross
+// section (CosseratRodCrossSectionInterface.hpp:266-307,
+// CircleCrossSectionOperations.hpp:84-132), rigidities
+// (LinearHyperElasticityFacade.hpp:273-327; Initializers/detail/Elasticity.hpp:
+// 54-77) and kinematics (WithRodKinematics.hpp:344-424).
+eb_status init_straight_rod(const eb_straight_rod& p, RodHost& r) {
+  const int64_t n = p.n_elements;
+  if (n < 2) return fail(EB_ERR_INVALID_ARGUMENT, "a rod needs at least 2 elements");
+  if (!(p.radius > 0.0) || !(p.length > 0.0) || !(p.density > 0.0))
+    return fail(EB_ERR_INVALID_ARGUMENT, "radius, length and density must be positive");
+  if (p.model != EB_ROD_DAMPED && p.model != EB_ROD_UNDAMPED)
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown rod model");
+  if (p.model == EB_ROD_DAMPED && (p.force_damping_rate < 0.0 || p.torque_damping_rate < 0.0))
+    return fail(EB_ERR_INVALID_ARGUMENT, "damping rates must be non-negative");
+  const double dn = norm3(p.direction), nn = norm3(p.normal);
+  if (dn == 0.0) return fail(EB_ERR_INVALID_ARGUMENT, "direction is zero");
+  if (nn == 0.0) return fail(EB_ERR_INVALID_ARGUMENT, "normal is zero");
+  const double t[3] = {p.direction[0] / dn, p.direction[1] / dn, p.direction[2] / dn};
+  const double nv[3] = {p.normal[0] / nn, p.normal[1] / nn, p.normal[2] / nn};
+  if (std::fabs(t[0] * nv[0] + t[1] * nv[1] + t[2] * nv[2]) > 1e-10)
+    return fail(EB_ERR_INVALID_ARGUMENT, "the proposed normal and tangent are non-orthogonal");
+
+  r.n = n;
+  r.model = p.model;
+  const int64_t W = n + 1;
+  r.state.assign(static_cast<size_t>(eb::kStateFields * W), 0.0);
+  r.param.assign(static_cast<size_t>(eb::kParamFields * W), 0.0);
+  r.diag.assign(static_cast<size_t>(eb::kDiagFields * W), 0.0);
+  auto S = [&](int f, int64_t j) -> double& { return r.state[static_cast<size_t>(f * W + j)]; };
+  auto P = [&](int f, int64_t j) -> double& { return r.param[static_cast<size_t>(f * W + j)]; };
+
+  for (int d = 0; d < 3; ++d) {
+    const double stop = p.origin[d] + p.length * t[d];
+    const double step = (stop - p.origin[d]) / static_cast<double>(n);
+    for (int64_t j = 0; j <= n; ++j) S(eb::kX + d, j) = p.origin[d] + static_cast<double>(j) * step;
+  }
+  double v1[3] = {nv[0], nv[1], nv[2]}, v2[3], v3[3], tmp[3];
+  cross3(t, nv, v2);
+  cross3(v1, v2, v3);
+  cross3(v3, v1, tmp);
+  std::memcpy(v2, tmp, sizeof(tmp));
+  const double n2 = norm3(v2), n3 = norm3(v3);
+  const double rows[9] = {v1[0],      v1[1],      v1[2],      v2[0] / n2, v2[1] / n2,
+                          v2[2] / n2, v3[0] / n3, v3[1] / n3, v3[2] / n3};
+  for (int k = 0; k < 9; ++k)
+    for (int64_t i = 0; i < n; ++i) S(eb::kQ + k, i) = rows[k];
+
+  std::vector<double> l0(n), rad(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const double dx[3] = {S(eb::kX, i + 1) - S(eb::kX, i), S(eb::kX + 1, i + 1) - S(eb::kX + 1, i),
+                          S(eb::kX + 2, i + 1) - S(eb::kX + 2, i)};
+    l0[i] = norm3(dx) / 1.0;
+    P(eb::kL0, i) = l0[i];
+  }
+  for (int64_t k = 0; k + 1 < n; ++k) P(eb::kD0, k) = 0.5 * (l0[k] + l0[k + 1]);
+  const double A = static_cast<double>(M_PI) * (p.radius * p.radius);
+  for (int64_t i = 0; i < n; ++i) {
+    P(eb::kVol, i) = A * l0[i];
+    rad[i] = std::sqrt(M_1_PI * P(eb::kVol, i) / l0[i]);
+    r.diag[static_cast<size_t>(eb::kDDim * W + i)] = rad[i];
+  }
+  auto I_of = [&](int64_t i, int d) {
+    const double Ai = static_cast<double>(M_PI) * (rad[i] * rad[i]);
+    const double I1 = (0.25 * M_1_PI) * (Ai * Ai);
+    return d == 2 ? 2.0 * I1 : I1;
+  };
+  const double E = p.youngs_modulus, G = p.shear_modulus;
+  const double stiff_b[3] = {E, E, G}, stiff_s[3] = {G, G, E};
+  const double alpha_c = 13.5 / 14.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double Ai = static_cast<double>(M_PI) * (rad[i] * rad[i]);
+    const double eff[3] = {Ai * alpha_c, Ai * alpha_c, Ai};
+    for (int d = 0; d < 3; ++d) {
+      P(eb::kShear + d, i) = stiff_s[d] * eff[d];
+      P(eb::kJ + d, i) = I_of(i, d) * p.density * l0[i];
+      P(eb::kJinv + d, i) = 1.0 / (I_of(i, d) * p.density * l0[i]);
+    }
+  }
+  for (int64_t k = 0; k + 1 < n; ++k)
+    for (int d = 0; d < 3; ++d)
+      P(eb::kBend + d, k) =
+          (l0[k] * stiff_b[d] * I_of(k, d) + l0[k + 1] * stiff_b[d] * I_of(k + 1, d)) / (l0[k] + l0[k + 1]);
+  for (int64_t j = 0; j <= n; ++j) P(eb::kMass, j) = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double me = p.density * P(eb::kVol, i);
+    P(eb::kMass, i) += 0.5 * me;
+    P(eb::kMass, i + 1) += 0.5 * me;
+  }
+  if (p.model == EB_ROD_DAMPED) {
+    for (int64_t j = 0; j <= n; ++j) P(eb::kNuF, j) = p.force_damping_rate;
+    for (int64_t i = 0; i < n; ++i) P(eb::kNuT, i) = p.torque_damping_rate;
+  }
+  // benign values in the unused element / Voronoi entries of the last slots
+  for (int d = 0; d < 3; ++d) {
+    P(eb::kJ + d, n) = 1.0;
+    P(eb::kJinv + d, n) = 1.0;
+  }
+  P(eb::kL0, n) = 1.0;
+  P(eb::kD0, n - 1) = 1.0;
+  P(eb::kD0, n) = 1.0;
+  return EB_OK;
+}
+
+eb_status rod_field_check(const eb_sim* s, int64_t rod, int32_t field, int64_t count,
+                          const FieldInfo** fi, int64_t* expected) {
+  if (field < 0 || field >= EB_FIELD_COUNT) return fail(EB_ERR_INVALID_ARGUMENT, "unknown field");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size()))
+    return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  *fi = &kFields[field];
+  *expected = (*fi)->ncomp * place_count((*fi)->place, s->rods[rod].n);
+  if (count != *expected)
+    return fail(EB_ERR_INVALID_ARGUMENT, "value count " + std::to_string(count) + " != " +
+                                             std::to_string(*expected));
+  return EB_OK;
+}
+
+double* device_base(eb_sim* s, const FieldInfo& f) {
+  double* base = f.kind == kState ? s->d_state[s->cur] : (f.kind == kParam ? s->d_param : s->d_diag);
+  return base ? base + static_cast<int64_t>(f.offset) * s->stride : nullptr;
+}
+
+void host_free(eb_sim* s) {
+  for (int b = 0; b < 2; ++b)
+    if (s->d_state[b]) cudaFree(s->d_state[b]);
+  if (s->d_param) cudaFree(s->d_param);
+  if (s->d_diag) cudaFree(s->d_diag);
+  if (s->d_meta) cudaFree(s->d_meta);
+  if (s->d_rods) cudaFree(s->d_rods);
+  if (s->d_offsets) cudaFree(s->d_offsets);
+  if (s->d_energy) cudaFree(s->d_energy);
+  s->d_state[0] = s->d_state[1] = s->d_param = s->d_diag = s->d_energy = nullptr;
+  s->d_meta = nullptr;
+  s->d_rods = nullptr;
+  s->d_offsets = nullptr;
+}
+
+eb_status upload_rod_table(eb_sim* s) {
+  std::vector<eb::RodInfo> info(s->rods.size());
+  for (size_t r = 0; r < s->rods.size(); ++r) info[r] = s->rods[r].info;
+  EB_CUDA(cudaMemcpyAsync(s->d_rods, info.data(), info.size() * sizeof(eb::RodInfo),
+                          cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+EB_API const char* eb_last_error(void) { return g_last_error.c_str(); }
+EB_API const char* eb_version(void) { return "elastica_b200 0.1 (sm_100a)"; }
+
+EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
+  if (!out) return fail(EB_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = nullptr;
+  eb_config cfg{};
+  if (config) cfg = *config;
+  if (cfg.precision != EB_PRECISION_FP64 && cfg.precision != EB_PRECISION_MIXED)
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (cfg.precision == EB_PRECISION_MIXED)
+    return fail(EB_ERR_UNSUPPORTED, "mixed precision is not built into this library yet");
+  int ndev = 0;
+  EB_CUDA(cudaGetDeviceCount(&ndev));
+  if (cfg.device < 0 || cfg.device >= ndev) return fail(EB_ERR_INVALID_ARGUMENT, "no such CUDA device");
+  eb_sim* s = new eb_sim();
+  s->cfg = cfg;
+  cudaError_t e = cudaSetDevice(cfg.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete s;
+    return fail(EB_ERR_CUDA, std::string("stream creation: ") + cudaGetErrorString(e));
+  }
+  *out = s;
+  return EB_OK;
+}
+
+EB_API eb_status eb_sim_destroy(eb_sim* s) {
+  if (!s) return EB_OK;
+  cudaSetDevice(s->cfg.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  host_free(s);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return EB_OK;
+}
+
+EB_API eb_status eb_emplace_straight_rods(eb_sim* s, const eb_straight_rod* rods, int64_t count,
+                                          int64_t* ids_out) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add rods after finalize");
+  if (count < 0 || (count > 0 && !rods)) return fail(EB_ERR_INVALID_ARGUMENT, "bad rod array");
+  std::vector<RodHost> made(static_cast<size_t>(count));
+  for (int64_t i = 0; i < count; ++i) {
+    const eb_status st = init_straight_rod(rods[i], made[i]);
+    if (st != EB_OK) return st;
+  }
+  const int64_t first = static_cast<int64_t>(s->rods.size());
+  if (first + count >= (int64_t(1) << (32 - eb::kRodShift)))
+    return fail(EB_ERR_UNSUPPORTED, "too many rods in one simulator");
+  for (auto& r : made) {
+    if (r.model == EB_ROD_DAMPED) s->any_damped = true;
+    s->rods.push_back(std::move(r));
+  }
+  if (ids_out)
+    for (int64_t i = 0; i < count; ++i) ids_out[i] = first + i;
+  return EB_OK;
+}
+
+EB_API eb_status eb_rod_count(const eb_sim* s, int64_t* count) {
+  if (check_sim(s) || !count) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  *count = static_cast<int64_t>(s->rods.size());
+  return EB_OK;
+}
+
+EB_API eb_status eb_rod_elements(const eb_sim* s, int64_t rod, int64_t* n) {
+  if (check_sim(s) || !n) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  *n = s->rods[rod].n;
+  return EB_OK;
+}
+
+EB_API eb_status eb_slot_count(const eb_sim* s, int64_t* n_slots) {
+  if (check_sim(s) || !n_slots) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  int64_t total = 0;
+  for (const auto& r : s->rods) total += r.n + 1;
+  *n_slots = total;
+  return EB_OK;
+}
+
+EB_API eb_status eb_slot_offsets(const eb_sim* s, int64_t* offsets_out, int64_t count) {
+  if (check_sim(s) || !offsets_out) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (count != static_cast<int64_t>(s->rods.size()) + 1)
+    return fail(EB_ERR_INVALID_ARGUMENT, "offsets need rod_count + 1 entries");
+  int64_t total = 0;
+  for (size_t r = 0; r < s->rods.size(); ++r) {
+    offsets_out[r] = total;
+    total += s->rods[r].n + 1;
+  }
+  offsets_out[s->rods.size()] = total;
+  return EB_OK;
+}
+
+EB_API eb_status eb_field_size(const eb_sim* s, int64_t rod, int32_t field, int64_t* count) {
+  if (check_sim(s) || !count) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (field < 0 || field >= EB_FIELD_COUNT) return fail(EB_ERR_INVALID_ARGUMENT, "unknown field");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  *count = kFields[field].ncomp * place_count(kFields[field].place, s->rods[rod].n);
+  return EB_OK;
+}
+
+EB_API eb_status eb_set_field(eb_sim* s, int64_t rod, int32_t field, const double* values, int64_t count) {
+  if (check_sim(s) || !values) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  const FieldInfo* fi;
+  int64_t expected;
+  if (eb_status st = rod_field_check(s, rod, field, count, &fi, &expected)) return st;
+  RodHost& r = s->rods[rod];
+  const int64_t per = place_count(fi->place, r.n);
+  if (!s->finalized) {
+    std::vector<double>& buf = fi->kind == kState ? r.state : (fi->kind == kParam ? r.param : r.diag);
+    for (int c = 0; c < fi->ncomp; ++c)
+      std::memcpy(&buf[static_cast<size_t>((fi->offset + c) * (r.n + 1))], values + c * per,
+                  static_cast<size_t>(per) * sizeof(double));
+    return EB_OK;
+  }
+  if (eb_status st = set_device(s)) return st;
+  double* base = device_base(s, *fi);
+  if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  EB_CUDA(cudaMemcpy2DAsync(base + s->offsets[rod], s->stride * sizeof(double), values,
+                            per * sizeof(double), per * sizeof(double), fi->ncomp,
+                            cudaMemcpyHostToDevice, s->stream));
+  if (fi->kind == kState) {
+    // keep the other ping-pong buffer consistent for the unused slot entries
+    double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi->offset) * s->stride;
+    EB_CUDA(cudaMemcpy2DAsync(other + s->offsets[rod], s->stride * sizeof(double), values,
+                              per * sizeof(double), per * sizeof(double), fi->ncomp,
+                              cudaMemcpyHostToDevice, s->stream));
+  }
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+EB_API eb_status eb_get_field(eb_sim* s, int64_t rod, int32_t field, double* values, int64_t count) {
+  if (check_sim(s) || !values) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  const FieldInfo* fi;
+  int64_t expected;
+  if (eb_status st = rod_field_check(s, rod, field, count, &fi, &expected)) return st;
+  const RodHost& r = s->rods[rod];
+  const int64_t per = place_count(fi->place, r.n);
+  if (!s->finalized) {
+    const std::vector<double>& buf = fi->kind == kState ? r.state : (fi->kind == kParam ? r.param : r.diag);
+    for (int c = 0; c < fi->ncomp; ++c)
+      std::memcpy(values + c * per, &buf[static_cast<size_t>((fi->offset + c) * (r.n + 1))],
+                  static_cast<size_t>(per) * sizeof(double));
+    return EB_OK;
+  }
+  if (eb_status st = set_device(s)) return st;
+  double* base = device_base(s, *fi);
+  if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  EB_CUDA(cudaMemcpy2DAsync(values, per * sizeof(double), base + s->offsets[rod],
+                            s->stride * sizeof(double), per * sizeof(double), fi->ncomp,
+                            cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* host, int64_t count,
+                            bool to_device) {
+  if (check_sim(s) || !host) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "batch access needs a finalized simulator");
+  if (field < 0 || field >= EB_FIELD_COUNT) return fail(EB_ERR_INVALID_ARGUMENT, "unknown field");
+  const FieldInfo& fi = kFields[field];
+  if (eb_status st = set_device(s)) return st;
+  double* base = device_base(s, fi);
+  if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  const size_t pitch = static_cast<size_t>(s->stride) * sizeof(double);
+  if (layout == EB_LAYOUT_SLOTS) {
+    if (count != fi.ncomp * s->n_slots)
+      return fail(EB_ERR_INVALID_ARGUMENT, "slot layout needs ncomp * slot_count values");
+    const size_t w = static_cast<size_t>(s->n_slots) * sizeof(double);
+    if (to_device) {
+      EB_CUDA(cudaMemcpy2DAsync(base, pitch, host, w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+      if (fi.kind == kState) {
+        double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi.offset) * s->stride;
+        EB_CUDA(cudaMemcpy2DAsync(other, pitch, host, w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+      }
+    } else {
+      EB_CUDA(cudaMemcpy2DAsync(host, w, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToHost, s->stream));
+    }
+    EB_CUDA(cudaStreamSynchronize(s->stream));
+    return EB_OK;
+  }
+  if (layout != EB_LAYOUT_PER_ROD) return fail(EB_ERR_INVALID_ARGUMENT, "unknown layout");
+  int64_t total = 0;
+  for (const auto& r : s->rods) total += fi.ncomp * place_count(fi.place, r.n);
+  if (count != total) return fail(EB_ERR_INVALID_ARGUMENT, "per-rod layout count mismatch");
+  // stage through the slot layout; start from the device contents so the
+  // unused slot entries keep their values
+  std::vector<double> tmp(static_cast<size_t>(fi.ncomp * s->n_slots), 0.0);
+  const size_t w = static_cast<size_t>(s->n_slots) * sizeof(double);
+  EB_CUDA(cudaMemcpy2DAsync(tmp.data(), w, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  int64_t pos = 0;
+  for (size_t r = 0; r < s->rods.size(); ++r) {
+    const int64_t per = place_count(fi.place, s->rods[r].n);
+    for (int c = 0; c < fi.ncomp; ++c) {
+      double* slot = tmp.data() + c * s->n_slots + s->offsets[r];
+      if (to_device)
+        std::memcpy(slot, host + pos, static_cast<size_t>(per) * sizeof(double));
+      else
+        std::memcpy(host + pos, slot, static_cast<size_t>(per) * sizeof(double));
+      pos += per;
+    }
+  }
+  if (!to_device) return EB_OK;
+  EB_CUDA(cudaMemcpy2DAsync(base, pitch, tmp.data(), w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+  if (fi.kind == kState) {
+    double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi.offset) * s->stride;
+    EB_CUDA(cudaMemcpy2DAsync(other, pitch, tmp.data(), w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+  }
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+EB_API eb_status eb_set_field_batch(eb_sim* s, int32_t field, int32_t layout, const double* values,
+                                    int64_t count) {
+  return batch_copy(s, field, layout, const_cast<double*>(values), count, true);
+}
+
+EB_API eb_status eb_get_field_batch(eb_sim* s, int32_t field, int32_t layout, double* values,
+                                    int64_t count) {
+  return batch_copy(s, field, layout, values, count, false);
+}
+
+EB_API eb_status eb_constrain_clamp(eb_sim* s, int64_t rod, int64_t index) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add constraints after finalize");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  if (index != 0) return fail(EB_ERR_UNSUPPORTED, "only the clamp at index 0 is supported");
+  RodHost& r = s->rods[rod];
+  const int64_t W = r.n + 1;
+  for (int d = 0; d < 3; ++d) r.info.clamp_x[d] = r.state[static_cast<size_t>((eb::kX + d) * W)];
+  for (int k = 0; k < 9; ++k) r.info.clamp_Q[k] = r.state[static_cast<size_t>((eb::kQ + k) * W)];
+  r.info.flags |= eb::kRodClamp;
+  s->sim_flags |= eb::kSimClamp;
+  return EB_OK;
+}
+
+EB_API eb_status eb_add_gravity(eb_sim* s, const double gravity[3]) {
+  if (check_sim(s) || !gravity) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add environments after finalize");
+  if (s->has_gravity) return fail(EB_ERR_INVALID_STATE, "the gravity field is a singleton environment");
+  for (int d = 0; d < 3; ++d) s->gravity[d] = gravity[d];
+  s->has_gravity = true;
+  s->sim_flags |= eb::kSimGravity;
+  return EB_OK;
+}
+
+EB_API eb_status eb_add_end_torque(eb_sim* s, int64_t rod, const double torque_lab[3]) {
+  if (check_sim(s) || !torque_lab) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add forcing after finalize");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  RodHost& r = s->rods[rod];
+  for (int d = 0; d < 3; ++d) r.info.end_torque[d] += torque_lab[d];
+  r.info.flags |= eb::kRodEndTorque;
+  s->sim_flags |= eb::kSimEndTorque;
+  return EB_OK;
+}
+
+EB_API eb_status eb_add_analytical_damper(eb_sim* s, int64_t rod, double translational_rate,
+                                          double rotational_rate) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add constraints after finalize");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  if (!(translational_rate >= 0.0) || !(rotational_rate >= 0.0))
+    return fail(EB_ERR_INVALID_ARGUMENT, "damping rates must be non-negative");
+  RodHost& r = s->rods[rod];
+  if (r.info.flags & eb::kRodDamper) return fail(EB_ERR_INVALID_STATE, "rod already has a damper");
+  r.damper_nu_t = translational_rate;
+  r.info.damper_r = rotational_rate;
+  r.info.flags |= eb::kRodDamper;
+  s->sim_flags |= eb::kSimDamper;
+  return EB_OK;
+}
+
+EB_API eb_status eb_finalize(eb_sim* s) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "already finalized");
+  if (s->rods.empty()) return fail(EB_ERR_INVALID_STATE, "no rods");
+  if (eb_status st = set_device(s)) return st;
+  const int64_t nr = static_cast<int64_t>(s->rods.size());
+  s->offsets.assign(static_cast<size_t>(nr + 1), 0);
+  for (int64_t r = 0; r < nr; ++r) s->offsets[r + 1] = s->offsets[r] + s->rods[r].n + 1;
+  s->n_slots = s->offsets[nr];
+  s->stride = (s->n_slots + 31) / 32 * 32;
+  const int64_t S = s->stride;
+  const bool want_diag = (s->cfg.flags & EB_FLAG_RECORD_DIAGNOSTICS) != 0;
+
+  std::vector<double> hs(static_cast<size_t>(eb::kStateFields * S), 0.0);
+  std::vector<double> hp(static_cast<size_t>(eb::kParamFields * S), 0.0);
+  std::vector<double> hd;
+  if (want_diag) hd.assign(static_cast<size_t>(eb::kDiagFields * S), 0.0);
+  std::vector<uint32_t> meta(static_cast<size_t>(S), 0u);
+  for (int64_t r = 0; r < nr; ++r) {
+    const RodHost& R = s->rods[r];
+    const int64_t W = R.n + 1, o = s->offsets[r];
+    for (int f = 0; f < eb::kStateFields; ++f)
+      std::memcpy(&hs[static_cast<size_t>(f * S + o)], &R.state[static_cast<size_t>(f * W)], W * sizeof(double));
+    for (int f = 0; f < eb::kParamFields; ++f)
+      std::memcpy(&hp[static_cast<size_t>(f * S + o)], &R.param[static_cast<size_t>(f * W)], W * sizeof(double));
+    if (want_diag)
+      for (int f = 0; f < eb::kDiagFields; ++f)
+        std::memcpy(&hd[static_cast<size_t>(f * S + o)], &R.diag[static_cast<size_t>(f * W)], W * sizeof(double));
+    for (int64_t j = 0; j <= R.n; ++j) {
+      uint32_t m = static_cast<uint32_t>(r) << eb::kRodShift;
+      if (j < R.n) m |= eb::kElem;
+      if (j < R.n - 1) m |= eb::kVor;
+      if (j == 0) m |= eb::kFirst;
+      if (j == R.n) m |= eb::kLastNode;
+      if (j == R.n - 1) m |= eb::kLastElem;
+      meta[static_cast<size_t>(o + j)] = m;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  alloc(reinterpret_cast<void**>(&s->d_state[0]), hs.size() * sizeof(double));
+  alloc(reinterpret_cast<void**>(&s->d_state[1]), hs.size() * sizeof(double));
+  alloc(reinterpret_cast<void**>(&s->d_param), hp.size() * sizeof(double));
+  if (want_diag) alloc(reinterpret_cast<void**>(&s->d_diag), hd.size() * sizeof(double));
+  alloc(reinterpret_cast<void**>(&s->d_meta), meta.size() * sizeof(uint32_t));
+  alloc(reinterpret_cast<void**>(&s->d_rods), static_cast<size_t>(nr) * sizeof(eb::RodInfo));
+  alloc(reinterpret_cast<void**>(&s->d_offsets), static_cast<size_t>(nr + 1) * sizeof(int64_t));
+  alloc(reinterpret_cast<void**>(&s->d_energy), static_cast<size_t>(4 * nr) * sizeof(double));
+  if (e != cudaSuccess) {
+    host_free(s);
+    return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA,
+                std::string("device allocation: ") + cudaGetErrorString(e));
+  }
+  EB_CUDA(cudaMemcpyAsync(s->d_state[0], hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(s->d_state[1], hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(s->d_param, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  if (want_diag)
+    EB_CUDA(cudaMemcpyAsync(s->d_diag, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(s->d_meta, meta.data(), meta.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(s->d_offsets, s->offsets.data(), s->offsets.size() * sizeof(int64_t),
+                          cudaMemcpyHostToDevice, s->stream));
+  s->cur = 0;
+  s->finalized = true;
+  if (eb_status st = upload_rod_table(s)) return st;
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "finalize before stepping");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(EB_ERR_INVALID_ARGUMENT, "dt must be positive and finite");
+  if (n_steps < 0) return fail(EB_ERR_INVALID_ARGUMENT, "negative step count");
+  if (n_steps == 0) return EB_OK;
+  if (eb_status st = set_device(s)) return st;
+  if ((s->sim_flags & eb::kSimDamper) && dt != s->damper_dt) {
+    // the reference builds the damper's exponential constants once for the
+    // simulation's dt (AnalyticalLinearDamper.hpp:40-57)
+    for (auto& r : s->rods)
+      if (r.info.flags & eb::kRodDamper) r.info.damper_t = std::exp(-r.damper_nu_t * dt);
+    if (eb_status st = upload_rod_table(s)) return st;
+    s->damper_dt = dt;
+  }
+  eb::StepArgs a{};
+  a.stride = s->stride;
+  a.n_slots = s->n_slots;
+  a.par = s->d_param;
+  a.meta = s->d_meta;
+  a.rods = s->d_rods;
+  a.dt = dt;
+  a.half_dt = 0.5 * dt;
+  for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
+  a.sim_flags = s->sim_flags;
+  const bool diag = s->d_diag != nullptr;
+  for (int64_t k = 0; k < n_steps; ++k) {
+    a.in = s->d_state[s->cur];
+    a.out = s->d_state[s->cur ^ 1];
+    const bool rec = diag && (k == n_steps - 1);
+    a.diag = rec ? s->d_diag : nullptr;
+    if (s->cfg.flags & EB_FLAG_STRICT_FP64)
+      EB_CUDA(eb::launch_rod_step_fp64_strict(a, rec, s->any_damped, s->stream));
+    else
+      EB_CUDA(eb::launch_rod_step_fp64(a, rec, s->any_damped, s->stream));
+    s->cur ^= 1;
+    ++s->launches;
+    if (time) {
+      // two TimeUpdate substeps of dt/2 (PositionVerlet.hpp:52-58)
+      *time += 0.5 * dt;
+      *time += 0.5 * dt;
+    }
+  }
+  return EB_OK;
+}
+
+EB_API eb_status eb_synchronize(eb_sim* s) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (!s->stream) return EB_OK;
+  if (eb_status st = set_device(s)) return st;
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+EB_API eb_status eb_energy(eb_sim* s, double* out, int64_t count) {
+  if (check_sim(s) || !out) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "finalize first");
+  const int64_t nr = static_cast<int64_t>(s->rods.size());
+  if (count != 4 * nr) return fail(EB_ERR_INVALID_ARGUMENT, "energy needs 4 values per rod");
+  if (eb_status st = set_device(s)) return st;
+  EB_CUDA(eb::launch_rod_energy(nr, s->stride, s->d_offsets, s->d_state[s->cur], s->d_param,
+                                s->d_energy, s->stream));
+  ++s->launches;
+  EB_CUDA(cudaMemcpyAsync(out, s->d_energy, static_cast<size_t>(4 * nr) * sizeof(double),
+                          cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+EB_API eb_status eb_get_stream(const eb_sim* s, void** stream) {
+  if (check_sim(s) || !stream) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  *stream = static_cast<void*>(s->stream);
+  return EB_OK;
+}
+
+EB_API eb_status eb_launch_count(const eb_sim* s, int64_t* count) {
+  if (check_sim(s) || !count) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  *count = s->launches;
+  return EB_OK;
+}
+
+}  // extern "C"

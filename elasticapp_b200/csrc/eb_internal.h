@@ -1,0 +1,105 @@
+// Internal layout shared by the host side (eb_capi.cu) and the kernels.
+//
+// Device layout ("slots"): rod r with n_r elements owns n_r + 1 consecutive
+// slots starting at offset[r].  Slot offset[r] + j holds node j (j <= n_r),
+// element j (j < n_r) and Voronoi point j (j < n_r - 1), so every stagger
+// shares one index and one offset table.  The reference instead pads each rod
+// with ghost slots (1 node, 2 element, 3 Voronoi ghosts, elastica/Systems/
+// CosseratRods/Traits/PlacementTraits/PlacementTraits.hpp:53-56,82-85,124-127)
+// to give every stagger the stride n + 2; here the only unused entries are
+// the element at j = n and the Voronoi points at j >= n - 1.
+//
+// Every field is a separate 1-D array of `stride` entries (stride = slot
+// count rounded up to 32 so each array starts on a 256-byte boundary);
+// component c of a vector field lives at base + c * stride.
+#pragma once
+
+#include <cstdint>
+
+namespace eb {
+
+// per-slot metadata word: flag bits | rod id << kRodShift
+enum SlotFlags : uint32_t {
+  kElem = 1u << 0,      // slot holds an element (j < n)
+  kVor = 1u << 1,       // slot holds a Voronoi point (j < n - 1)
+  kFirst = 1u << 2,     // j == 0
+  kLastNode = 1u << 3,  // j == n
+  kLastElem = 1u << 4,  // j == n - 1
+};
+constexpr int kRodShift = 5;
+constexpr uint32_t kFlagMask = (1u << kRodShift) - 1u;
+
+// state arrays (per ping-pong buffer), in units of `stride`
+enum StateField : int {
+  kX = 0,   // 3: node positions
+  kV = 3,   // 3: node velocities
+  kQ = 6,   // 9: element directors, Q(k, j) at kQ + 3k + j
+  kW = 15,  // 3: element angular velocities (material frame)
+  kStateFields = 18
+};
+
+// parameter arrays, in units of `stride`
+enum ParamField : int {
+  kMass = 0,    // node mass
+  kNuF = 1,     // node force damping rate
+  kNuT = 2,     // element torque damping rate
+  kL0 = 3,      // element rest length
+  kD0 = 4,      // Voronoi rest length
+  kVol = 5,     // element volume (read only for the element dimension)
+  kSig0 = 6,    // 3: element rest shear/stretch strain
+  kKap0 = 9,    // 3: Voronoi rest curvature
+  kShear = 12,  // 3: element shear/stretch rigidity diagonal
+  kBend = 15,   // 3: Voronoi bend/twist rigidity diagonal
+  kJ = 18,      // 3: element mass second moment of inertia diagonal
+  kJinv = 21,   // 3: its inverse
+  kParamFields = 24
+};
+
+// derived (diagnostic) arrays, in units of `stride`
+enum DiagField : int {
+  kDLength = 0,
+  kDDil = 1,
+  kDTangent = 2,   // 3
+  kDVDil = 5,
+  kDSigma = 6,     // 3
+  kDKappa = 9,     // 3
+  kDStress = 12,   // 3
+  kDCouple = 15,   // 3
+  kDLoads = 18,    // 3
+  kDTorques = 21,  // 3
+  kDAccel = 24,    // 3
+  kDAlpha = 27,    // 3
+  kDDim = 30,
+  kDiagFields = 31
+};
+
+enum RodFlags : uint32_t { kRodClamp = 1u, kRodEndTorque = 2u, kRodDamper = 4u };
+
+struct RodInfo {
+  double clamp_x[3];
+  double clamp_Q[9];
+  double end_torque[3];  // lab frame
+  double damper_t;       // exp(-nu_t dt) for the dt of the current launch
+  double damper_r;       // nu_r
+  uint32_t flags;
+  uint32_t pad;
+};
+
+struct StepArgs {
+  int64_t stride;   // array stride (>= n_slots, multiple of 32)
+  int64_t n_slots;  // used slots
+  const double* in;     // state buffer read this step
+  double* out;          // state buffer written this step
+  const double* par;    // parameters
+  const uint32_t* meta; // slot metadata
+  const RodInfo* rods;
+  double* diag;         // derived fields, or nullptr
+  double dt;
+  double half_dt;
+  double gravity[3];
+  uint32_t sim_flags;   // kSim* below
+};
+
+enum SimFlags : uint32_t { kSimGravity = 1u, kSimDamper = 2u, kSimEndTorque = 4u, kSimClamp = 8u };
+
+}  // namespace eb

@@ -1,0 +1,324 @@
+"""Python mirror of the reference's Simulator plugin surface for the rod step.
+
+The reference drives rods as (elastica/Simulator/Interface/...):
+
+    simulator = elastica::make_simulator<...>(config);
+    rod = simulator->emplace_back<CosseratRod>(StraightInit{...}.initialize<CosseratRod>());
+    simulator->constrain(rod).at(0UL).with(clamp_generator());
+    simulator->finalize();
+    simulator->step(time_stepper, time, dt);
+
+Here the same calls exist with the same meaning, backed by the C-ABI of
+libelastica_b200.so (include/elastica_b200.h):
+
+    sim = Simulator()
+    rod = sim.emplace_back(CosseratRod, StraightRod(...))
+    sim.constrain(rod).at(0).using(Clamp())
+    sim.finalize()
+    t = sim.step(PositionVerlet(), t, dt)
+
+Variables are read and written with ``rod.get("Position")`` /
+``rod.set("Position", array)`` in the reference's shapes (3 x N, 3 x 3 x N,
+N), mirroring ``blocks::get<elastica::tags::Position>(rod)``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+# -- rod models (elastica/Systems/CosseratRods/Aliases) ---------------------
+class CosseratRod:
+    """Circular rod with diagonal linear elasticity and explicit damping
+    (Aliases/CosseratRod.hpp:33-40)."""
+
+    model = L.EB_ROD_DAMPED
+
+
+class CosseratRodWithoutDamping:
+    """Same rod without the explicit damping adapter
+    (Aliases/CosseratRodWithoutDamping.hpp)."""
+
+    model = L.EB_ROD_UNDAMPED
+
+
+@dataclass
+class Material:
+    """The material entries a rod reads (Simulator/Materials/Materials.hpp:436-449)."""
+
+    density: float
+    youngs_modulus: float
+    shear_modulus: float
+
+
+@dataclass
+class StraightRod:
+    """StraightCosseratRodInitializer (Initializers/StraightCosseratRod.hpp)."""
+
+    n_elements: int
+    material: Material
+    radius: float
+    length: float
+    origin: Sequence[float] = (0.0, 0.0, 0.0)
+    direction: Sequence[float] = (1.0, 0.0, 0.0)
+    normal: Sequence[float] = (0.0, 1.0, 0.0)
+    force_damping_rate: float = 0.0
+    torque_damping_rate: float = 0.0
+
+    def to_c(self, model: int) -> L.EbStraightRod:
+        r = L.EbStraightRod()
+        r.n_elements = int(self.n_elements)
+        r.model = int(model)
+        r.density = float(self.material.density)
+        r.youngs_modulus = float(self.material.youngs_modulus)
+        r.shear_modulus = float(self.material.shear_modulus)
+        r.radius = float(self.radius)
+        r.length = float(self.length)
+        for i in range(3):
+            r.origin[i] = float(self.origin[i])
+            r.direction[i] = float(self.direction[i])
+            r.normal[i] = float(self.normal[i])
+        r.force_damping_rate = float(self.force_damping_rate)
+        r.torque_damping_rate = float(self.torque_damping_rate)
+        return r
+
+
+# -- constraints, forcing, environments, stepper -----------------------------
+@dataclass
+class Clamp:
+    """Value constraint x_0 = origin, Q_0 = Q_0(init) plus rate constraint
+    v_0 = w_0 = 0 (pattern of examples/dynamic_cantilever/
+    DynamicCantileverCaseStudy.cpp:73-89)."""
+
+
+@dataclass
+class AnalyticalLinearDamper:
+    """Rate constraint of examples/fish_swimming/FishModel/Dissipations/
+    AnalyticalLinearDamper.hpp:15-76 (physical version)."""
+
+    translational_rate: float
+    rotational_rate: float
+
+
+@dataclass
+class EndTorque:
+    """Constant lab-frame torque at the last element (Forcing/MakeForcing.hpp)."""
+
+    torque: Sequence[float]
+
+
+@dataclass
+class GravityField:
+    """Environments/GravityField/GravityField.hpp:239-246."""
+
+    gravity: Sequence[float] = (0.0, 0.0, -9.81)
+
+
+@dataclass
+class PositionVerlet:
+    """Time/SymplecticSteppers/Algorithms/PositionVerlet.hpp:49-88."""
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class RodRef:
+    """Stable handle of one emplaced rod (the reference's BlockSlice ref)."""
+
+    def __init__(self, sim: "Simulator", rod_id: int, n_elements: int):
+        self.sim = sim
+        self.id = int(rod_id)
+        self.n_elements = int(n_elements)
+
+    def shape(self, name: str) -> tuple:
+        place, nc = L.FIELD_SHAPE[name]
+        n = self.n_elements
+        count = n + 1 if place == 0 else (n if place == 1 else n - 1)
+        if name == "Director":
+            return (3, 3, count)
+        return (nc, count) if nc > 1 else (count,)
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape(name), dtype=np.float64)
+        L.call("eb_get_field", self.sim._h, self.id, L.FIELD_ID[name], _dptr(out), out.size)
+        return out
+
+    def set(self, name: str, values) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if a.size != int(np.prod(self.shape(name))):
+            raise ValueError(f"{name} expects shape {self.shape(name)}, got {a.shape}")
+        L.call("eb_set_field", self.sim._h, self.id, L.FIELD_ID[name], _dptr(a), a.size)
+
+    # common accessors, as in the reference's rod member API
+    # (tests/Unit/Systems/CosseratRods/FullRodTest/Test_RodAPI.cpp:13-40)
+    def get_position(self):
+        return self.get("Position")
+
+    def get_velocity(self):
+        return self.get("Velocity")
+
+    def get_director(self):
+        return self.get("Director")
+
+    def get_angular_velocity(self):
+        return self.get("AngularVelocity")
+
+
+class _At:
+    def __init__(self, owner, rod: RodRef, kind: str):
+        self.owner, self.rod, self.kind, self.index = owner, rod, kind, None
+
+    def at(self, index: int) -> "_At":
+        self.index = int(index)
+        return self
+
+    def using(self, item) -> None:
+        self.owner._attach(self.kind, self.rod, self.index, item)
+
+    with_ = using
+
+
+class Simulator:
+    """Owns one eb_sim (device memory and a CUDA stream)."""
+
+    def __init__(self, device: int = 0, precision: str = "fp64", record_diagnostics: bool = False,
+                 strict_fp64: bool = False):
+        cfg = L.EbConfig()
+        cfg.device = int(device)
+        cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
+        cfg.flags = (L.EB_FLAG_RECORD_DIAGNOSTICS if record_diagnostics else 0) | (
+            L.EB_FLAG_STRICT_FP64 if strict_fp64 else 0)
+        h = ctypes.c_void_p()
+        L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
+        self._h = h
+        self.rods: list[RodRef] = []
+        self.finalized = False
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            L.load().eb_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- systems -----------------------------------------------------------
+    def emplace_back(self, model, initializer: StraightRod) -> RodRef:
+        return self.emplace_back_many(model, [initializer])[0]
+
+    def emplace_back_many(self, model, initializers: Iterable[StraightRod]) -> list[RodRef]:
+        inits = list(initializers)
+        arr = (L.EbStraightRod * len(inits))(*[i.to_c(model.model) for i in inits])
+        ids = (ctypes.c_int64 * len(inits))()
+        L.call("eb_emplace_straight_rods", self._h, arr, len(inits), ids)
+        refs = [RodRef(self, ids[k], inits[k].n_elements) for k in range(len(inits))]
+        self.rods.extend(refs)
+        return refs
+
+    # -- modules ---------------------------------------------------------------
+    def constrain(self, rod: RodRef) -> _At:
+        return _At(self, rod, "constrain")
+
+    def force(self, rod: RodRef) -> _At:
+        return _At(self, rod, "force")
+
+    def add_environment(self, env) -> None:
+        if isinstance(env, GravityField):
+            g = np.asarray(env.gravity, dtype=np.float64)
+            L.call("eb_add_gravity", self._h, _dptr(g))
+        else:
+            raise TypeError(f"unsupported environment {env!r}")
+
+    def _attach(self, kind, rod, index, item):
+        if kind == "constrain" and isinstance(item, Clamp):
+            L.call("eb_constrain_clamp", self._h, rod.id, 0 if index is None else index)
+        elif kind == "constrain" and isinstance(item, AnalyticalLinearDamper):
+            L.call("eb_add_analytical_damper", self._h, rod.id, float(item.translational_rate),
+                   float(item.rotational_rate))
+        elif kind == "force" and isinstance(item, EndTorque):
+            if index not in (None, rod.n_elements - 1):
+                raise ValueError("the end torque acts on the last element")
+            t = np.asarray(item.torque, dtype=np.float64)
+            L.call("eb_add_end_torque", self._h, rod.id, _dptr(t))
+        else:
+            raise TypeError(f"unsupported {kind} item {item!r}")
+
+    def finalize(self) -> None:
+        L.call("eb_finalize", self._h)
+        self.finalized = True
+
+    # -- time stepping -------------------------------------------------------
+    def step(self, stepper, time: float, dt: float, n_steps: int = 1) -> float:
+        if not isinstance(stepper, PositionVerlet):
+            raise TypeError("only PositionVerlet is provided")
+        t = ctypes.c_double(time)
+        L.call("eb_step", self._h, ctypes.byref(t), float(dt), int(n_steps))
+        return t.value
+
+    def synchronize(self) -> None:
+        L.call("eb_synchronize", self._h)
+
+    def energy(self) -> np.ndarray:
+        out = np.empty((len(self.rods), 4), dtype=np.float64)
+        L.call("eb_energy", self._h, _dptr(out), out.size)
+        return out
+
+    def stream_handle(self) -> int:
+        """The simulator's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        h = ctypes.c_void_p()
+        L.call("eb_get_stream", self._h, ctypes.byref(h))
+        return int(h.value or 0)
+
+    def launch_count(self) -> int:
+        c = ctypes.c_int64()
+        L.call("eb_launch_count", self._h, ctypes.byref(c))
+        return c.value
+
+    # -- batch access ----------------------------------------------------------
+    def slot_offsets(self) -> np.ndarray:
+        out = np.empty(len(self.rods) + 1, dtype=np.int64)
+        L.call("eb_slot_offsets", self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), out.size)
+        return out
+
+    def n_slots(self) -> int:
+        c = ctypes.c_int64()
+        L.call("eb_slot_count", self._h, ctypes.byref(c))
+        return c.value
+
+    def get_slots(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Field in the device slot layout, shape (ncomp, n_slots)."""
+        nc = L.FIELD_SHAPE[name][1]
+        if out is None:
+            out = np.empty((nc, self.n_slots()), dtype=np.float64)
+        L.call("eb_get_field_batch", self._h, L.FIELD_ID[name], L.EB_LAYOUT_SLOTS, _dptr(out), out.size)
+        return out
+
+    def set_slots(self, name: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        L.call("eb_set_field_batch", self._h, L.FIELD_ID[name], L.EB_LAYOUT_SLOTS, _dptr(a), a.size)
+
+    def get_batch(self, name: str) -> np.ndarray:
+        """Field of all rods concatenated in the per-rod layout (flat)."""
+        total = sum(int(np.prod(r.shape(name))) for r in self.rods)
+        out = np.empty(total, dtype=np.float64)
+        L.call("eb_get_field_batch", self._h, L.FIELD_ID[name], L.EB_LAYOUT_PER_ROD, _dptr(out), out.size)
+        return out
+
+    def set_batch(self, name: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        L.call("eb_set_field_batch", self._h, L.FIELD_ID[name], L.EB_LAYOUT_PER_ROD, _dptr(a), a.size)

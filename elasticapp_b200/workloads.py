@@ -1,0 +1,135 @@
+"""Seeded synthetic rod workloads with the shapes of the reference's target
+configurations.  No dataset is involved; every draw is from numpy's PCG64
+with the seed recorded in the workload.
+
+* ``cantilever``   — 1 rod, 100 elements, L 1 m, r 0.025 m, rho 1000, E 1e6,
+  G = E/3, along +x with normal +y, clamped at node 0, gravity -9.81 z,
+  analytical damper 0.1, dt 1e-5 (the template is
+  examples/dynamic_cantilever/DynamicCantileverCaseStudy.cpp).
+* ``uneven_batch`` — 16,384 clamped rods, n ~ U{32..512}, L ~ U[0.5, 2],
+  r ~ U[0.005, 0.05], log10 E ~ U[5, 7], Poisson 0.5 (G = E/3), rho 1000,
+  analytical damper 0.1, random direction, node velocities N(0, 1e-3^2),
+  gravity -9.81 z, dt = 0.1 min(l / sqrt(E / rho)).
+* ``mixed_batch``  — 65,536 rods, n ~ U{64..256}, parameters as above, rest
+  curvature k u (k ~ U[0, 10] 1/m, u a random body-frame unit vector) and an
+  end torque of 1e-3 N m about the initial tangent.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .simulator import (AnalyticalLinearDamper, Clamp, CosseratRodWithoutDamping, EndTorque,
+                        GravityField, Material, Simulator, StraightRod)
+
+
+@dataclass
+class Workload:
+    name: str
+    seed: int
+    rods: list  # StraightRod
+    model: type = CosseratRodWithoutDamping
+    clamp: bool = True
+    damper: tuple | None = (0.1, 0.1)
+    gravity: tuple | None = (0.0, 0.0, -9.81)
+    end_torque: np.ndarray | None = None      # (n_rods, 3) lab frame
+    velocities: list | None = None            # per rod (3, n + 1)
+    rest_curvature: list | None = None        # per rod (3, n - 1)
+    dt: float = 1e-5
+    n_steps: int = 1000
+
+    @property
+    def n_elements(self) -> np.ndarray:
+        return np.array([r.n_elements for r in self.rods], dtype=np.int64)
+
+    @property
+    def total_elements(self) -> int:
+        return int(self.n_elements.sum())
+
+    def build(self, device: int = 0, record_diagnostics: bool = False, precision: str = "fp64") -> Simulator:
+        """Create the simulator through the reference-style plugin surface."""
+        sim = Simulator(device=device, precision=precision, record_diagnostics=record_diagnostics)
+        refs = sim.emplace_back_many(self.model, self.rods)
+        if self.gravity is not None:
+            sim.add_environment(GravityField(self.gravity))
+        for k, ref in enumerate(refs):
+            if self.velocities is not None:
+                ref.set("Velocity", self.velocities[k])
+            if self.rest_curvature is not None:
+                ref.set("ReferenceCurvature", self.rest_curvature[k])
+            if self.clamp:
+                sim.constrain(ref).at(0).using(Clamp())
+            if self.damper is not None:
+                sim.constrain(ref).using(AnalyticalLinearDamper(*self.damper))
+            if self.end_torque is not None:
+                sim.force(ref).at(ref.n_elements - 1).using(EndTorque(self.end_torque[k]))
+        sim.finalize()
+        return sim
+
+
+def _unit_vectors(rng, n):
+    v = rng.standard_normal((n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _normals(rng, directions):
+    """Random unit normals exactly orthogonalised against the directions."""
+    out = np.empty_like(directions)
+    for i, d in enumerate(directions):
+        while True:
+            c = rng.standard_normal(3)
+            c = c - np.dot(c, d) * d
+            nrm = np.linalg.norm(c)
+            if nrm > 1e-3:
+                c = c / nrm
+                c = c - np.dot(c, d) * d
+                out[i] = c / np.linalg.norm(c)
+                break
+    return out
+
+
+def cantilever(n_elements: int = 100, seed: int = 1001) -> Workload:
+    E = 1e6
+    rod = StraightRod(n_elements=n_elements, material=Material(1000.0, E, E / 3.0), radius=0.025,
+                      length=1.0, origin=(0.0, 0.0, 0.0), direction=(1.0, 0.0, 0.0),
+                      normal=(0.0, 1.0, 0.0))
+    return Workload("cantilever", seed, [rod], dt=1e-5, n_steps=100_000)
+
+
+def _random_rods(rng, n_rods, n_lo, n_hi):
+    n = rng.integers(n_lo, n_hi + 1, size=n_rods)
+    L = rng.uniform(0.5, 2.0, size=n_rods)
+    r = rng.uniform(0.005, 0.05, size=n_rods)
+    E = 10.0 ** rng.uniform(5.0, 7.0, size=n_rods)
+    d = _unit_vectors(rng, n_rods)
+    nv = _normals(rng, d)
+    origins = rng.uniform(-1.0, 1.0, size=(n_rods, 3))
+    rods = [StraightRod(n_elements=int(n[k]), material=Material(1000.0, float(E[k]), float(E[k]) / 3.0),
+                        radius=float(r[k]), length=float(L[k]), origin=tuple(origins[k]),
+                        direction=tuple(d[k]), normal=tuple(nv[k])) for k in range(n_rods)]
+    return rods, n, L, E, d
+
+
+def uneven_batch(n_rods: int = 16384, seed: int = 1002, n_range=(32, 512), n_steps: int = 1000) -> Workload:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rods, n, L, E, d = _random_rods(rng, n_rods, *n_range)
+    vel = [rng.normal(0.0, 1e-3, size=(3, int(n[k]) + 1)) for k in range(n_rods)]
+    dt = 0.1 * float(np.min((L / n) / np.sqrt(E / 1000.0)))
+    return Workload("uneven_batch", seed, rods, velocities=vel, dt=dt, n_steps=n_steps)
+
+
+def mixed_batch(n_rods: int = 65536, seed: int = 1003, n_range=(64, 256), n_steps: int = 10_000,
+                dt: float = 1e-5) -> Workload:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rods, n, L, E, d = _random_rods(rng, n_rods, *n_range)
+    vel = [rng.normal(0.0, 1e-3, size=(3, int(n[k]) + 1)) for k in range(n_rods)]
+    k_mag = rng.uniform(0.0, 10.0, size=n_rods)
+    axes = _unit_vectors(rng, n_rods)
+    kappa = [np.repeat((k_mag[k] * axes[k])[:, None], int(n[k]) - 1, axis=1) for k in range(n_rods)]
+    torque = 1e-3 * d
+    return Workload("mixed_batch", seed, rods, velocities=vel, rest_curvature=kappa,
+                    end_torque=torque, dt=dt, n_steps=n_steps)
+
+
+CONFIGS = {"cantilever": cantilever, "uneven_batch": uneven_batch, "mixed_batch": mixed_batch}

@@ -1,0 +1,238 @@
+/* elastica_b200.h — C-ABI of the B200-native Cosserat-rod step.
+ *
+ * This is the drop-in boundary for the rod-block update of Elastica++
+ * (GazzolaLab/elasticapp).  Each entry point names the reference interface it
+ * replaces (paths relative to the reference repository).  All entry points
+ * are plain C: pointers and sizes, no C++ or torch types, no exceptions.
+ *
+ * Conventions
+ * - Every function returns an eb_status; on failure eb_last_error() returns
+ *   a message for the calling thread.  The reference throws std::logic_error
+ *   for use after finalize (elastica/Simulator/Interface/Simulator/
+ *   Simulator.hpp:485-509) and std::domain_error for bad parameters
+ *   (elastica/Systems/CosseratRods/Initializers/detail/Elasticity.hpp:106-116);
+ *   those become EB_ERR_INVALID_STATE and EB_ERR_INVALID_ARGUMENT.
+ * - The simulator owns all device memory; the caller owns host buffers.
+ * - Calls on one simulator must be serialised by the caller; several
+ *   simulators may coexist (one CUDA stream each).
+ * - Frames and layouts are the reference's (CosseratRodTraits.hpp:450-468):
+ *   per rod, vector fields are 3 x N row-major (row = x, y, z), the director
+ *   is 3 x 3 x N page-major (Q[k][j][i] = component j of director d_k of
+ *   element i), scalars are N.  Loads are lab frame on nodes; torques,
+ *   couples and angular velocities are material frame on elements.
+ */
+#ifndef ELASTICA_B200_H
+#define ELASTICA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EB_API __attribute__((visibility("default")))
+#else
+#define EB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum eb_status {
+  EB_OK = 0,
+  EB_ERR_INVALID_ARGUMENT = 1,
+  EB_ERR_INVALID_STATE = 2,
+  EB_ERR_UNSUPPORTED = 3,
+  EB_ERR_OUT_OF_MEMORY = 4,
+  EB_ERR_CUDA = 5,
+  EB_ERR_NOT_FOUND = 6,
+  EB_ERR_NUMERICAL = 7
+} eb_status;
+
+typedef enum eb_precision {
+  /* all arithmetic and state in FP64, as the reference (real_t = double,
+   * elastica/Utilities/DefineTypes.h:6) */
+  EB_PRECISION_FP64 = 0,
+  /* element-local arithmetic in FP32, state accumulation in FP64 */
+  EB_PRECISION_MIXED = 1
+} eb_precision;
+
+/* eb_config.flags */
+#define EB_FLAG_RECORD_DIAGNOSTICS 0x1u /* keep the derived per-element fields
+                                           (strains, curvature, loads, ...) of
+                                           the last step of every eb_step call */
+#define EB_FLAG_STRICT_FP64 0x2u        /* FP64 step without fused multiply-add
+                                           contraction: every product and sum
+                                           rounded separately, as the
+                                           reference's scalar C++ code */
+
+typedef struct eb_config {
+  int32_t device;    /* CUDA device ordinal */
+  int32_t precision; /* eb_precision */
+  uint32_t flags;    /* EB_FLAG_* */
+  int32_t reserved;
+} eb_config;
+
+/* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and
+ * Aliases/CosseratRodWithoutDamping.hpp). */
+typedef enum eb_rod_model {
+  EB_ROD_DAMPED = 0,  /* CosseratRod: explicit force/torque damping */
+  EB_ROD_UNDAMPED = 1 /* CosseratRodWithoutDamping */
+} eb_rod_model;
+
+/* Parameters of StraightCosseratRodInitializer
+ * (elastica/Systems/CosseratRods/Initializers/StraightCosseratRod.hpp,
+ * Initializers/detail/Geometry.hpp:110-214) plus the material entries the
+ * rod reads (elastica/Simulator/Materials/Materials.hpp:436-449). */
+typedef struct eb_straight_rod {
+  int64_t n_elements;
+  int32_t model; /* eb_rod_model */
+  int32_t reserved;
+  double density;
+  double youngs_modulus;
+  double shear_modulus;
+  double radius;
+  double length;
+  double origin[3];
+  double direction[3];
+  double normal[3]; /* must be orthogonal to direction */
+  double force_damping_rate;  /* EB_ROD_DAMPED only */
+  double torque_damping_rate; /* EB_ROD_DAMPED only */
+} eb_straight_rod;
+
+/* Rod variables, named after elastica::tags (elastica/Systems/CosseratRods/
+ * Tags.hpp).  Shapes per rod with n elements: N = nodes (n+1), E = elements
+ * (n), V = Voronoi points (n-1).
+ * Settable state and parameters: */
+typedef enum eb_field {
+  EB_POSITION = 0,                        /* 3 x N */
+  EB_VELOCITY = 1,                        /* 3 x N */
+  EB_DIRECTOR = 2,                        /* 3 x 3 x E */
+  EB_ANGULAR_VELOCITY = 3,                /* 3 x E */
+  EB_MASS = 4,                            /* N */
+  EB_REFERENCE_ELEMENT_LENGTH = 5,        /* E */
+  EB_REFERENCE_VORONOI_LENGTH = 6,        /* V */
+  EB_ELEMENT_VOLUME = 7,                  /* E */
+  EB_REFERENCE_SHEAR_STRETCH_STRAIN = 8,  /* 3 x E */
+  EB_REFERENCE_CURVATURE = 9,             /* 3 x V */
+  EB_SHEAR_STRETCH_RIGIDITY_MATRIX = 10,  /* 3 x E (diagonal) */
+  EB_BENDING_TWIST_RIGIDITY_MATRIX = 11,  /* 3 x V (diagonal) */
+  EB_MASS_SECOND_MOMENT_OF_INERTIA = 12,  /* 3 x E (diagonal) */
+  EB_INV_MASS_SECOND_MOMENT_OF_INERTIA = 13, /* 3 x E (diagonal) */
+  EB_FORCE_DAMPING_RATE = 14,             /* N (EB_ROD_DAMPED) */
+  EB_TORQUE_DAMPING_RATE = 15,            /* E (EB_ROD_DAMPED) */
+  /* Derived per-step fields (mid-step values of the last step; need
+   * EB_FLAG_RECORD_DIAGNOSTICS).  Setting them is allowed, as in the
+   * reference, but the next step overwrites them. */
+  EB_ELEMENT_LENGTH = 16,        /* E */
+  EB_ELEMENT_DILATATION = 17,    /* E */
+  EB_TANGENT = 18,               /* 3 x E */
+  EB_VORONOI_DILATATION = 19,    /* V */
+  EB_SHEAR_STRETCH_STRAIN = 20,  /* 3 x E */
+  EB_CURVATURE = 21,             /* 3 x V */
+  EB_INTERNAL_STRESS = 22,       /* 3 x E */
+  EB_INTERNAL_COUPLE = 23,       /* 3 x V */
+  EB_INTERNAL_LOADS = 24,        /* 3 x N */
+  EB_INTERNAL_TORQUES = 25,      /* 3 x E */
+  EB_ACCELERATION = 26,          /* 3 x N */
+  EB_ANGULAR_ACCELERATION = 27,  /* 3 x E */
+  EB_ELEMENT_DIMENSION = 28,     /* E */
+  EB_FIELD_COUNT = 29
+} eb_field;
+
+/* Layout of the batch accessors. */
+typedef enum eb_layout {
+  /* rods concatenated in id order, each in the per-rod layout above */
+  EB_LAYOUT_PER_ROD = 0,
+  /* the device layout: component-major over slots, component c of slot s at
+   * c * eb_slot_count() + s; rod r owns slots [offset[r], offset[r] + n_r] */
+  EB_LAYOUT_SLOTS = 1
+} eb_layout;
+
+/* --- lifecycle: elastica::make_simulator (Simulator.hpp:1087-1093) ----- */
+EB_API eb_status eb_sim_create(const eb_config* config, struct eb_sim** out);
+EB_API eb_status eb_sim_destroy(struct eb_sim* sim);
+EB_API const char* eb_last_error(void);
+EB_API const char* eb_version(void);
+
+/* --- systems: simulator->emplace_back<CosseratRod>(initializer)
+ * (elastica/Simulator/Interface/Systems/Module.hpp:898-955).  ids_out
+ * receives stable rod handles (0, 1, 2, ... in insertion order). ---------- */
+EB_API eb_status eb_emplace_straight_rods(struct eb_sim* sim, const eb_straight_rod* rods,
+                                          int64_t count, int64_t* ids_out);
+EB_API eb_status eb_rod_count(const struct eb_sim* sim, int64_t* count);
+EB_API eb_status eb_rod_elements(const struct eb_sim* sim, int64_t rod, int64_t* n_elements);
+EB_API eb_status eb_slot_count(const struct eb_sim* sim, int64_t* n_slots);
+/* offsets_out has rod_count + 1 entries */
+EB_API eb_status eb_slot_offsets(const struct eb_sim* sim, int64_t* offsets_out, int64_t count);
+/* Number of doubles eb_get_field/eb_set_field expect for this rod. */
+EB_API eb_status eb_field_size(const struct eb_sim* sim, int64_t rod, int32_t field, int64_t* count);
+
+/* --- variable access: blocks::get<tags::X>(rod_slice) = values
+ * (elastica/Systems/Block, used by the reference's golden tests,
+ * tests/Unit/Systems/CosseratRods/FullRodTest/Test_PerturbedRodStep.cpp:115-142).
+ * Allowed before and after eb_finalize. -------------------------------- */
+EB_API eb_status eb_set_field(struct eb_sim* sim, int64_t rod, int32_t field,
+                              const double* values, int64_t count);
+EB_API eb_status eb_get_field(struct eb_sim* sim, int64_t rod, int32_t field, double* values,
+                              int64_t count);
+/* All rods at once (after eb_finalize), in the given eb_layout.  For
+ * EB_LAYOUT_SLOTS the transfer is one host<->device copy per field; pinned
+ * host memory makes it asynchronous-speed. */
+EB_API eb_status eb_set_field_batch(struct eb_sim* sim, int32_t field, int32_t layout,
+                                    const double* values, int64_t count);
+EB_API eb_status eb_get_field_batch(struct eb_sim* sim, int32_t field, int32_t layout,
+                                    double* values, int64_t count);
+
+/* --- constraints: simulator->constrain(rod).at(0).with(clamp), the value
+ * constraint fixing x_0, Q_0 and the rate constraint zeroing v_0, w_0
+ * (elastica/Simulator/Constraints/MakeConstraint.hpp:458-494; pattern of
+ * examples/dynamic_cantilever/DynamicCantileverCaseStudy.cpp:73-89).  The
+ * clamp target is the rod's node-0 position and element-0 director at the
+ * time of eb_finalize.  Only index 0 is supported. */
+EB_API eb_status eb_constrain_clamp(struct eb_sim* sim, int64_t rod, int64_t index);
+
+/* --- environments: GravityField, F_ext += g m
+ * (elastica/Simulator/Environments/GravityField/GravityField.hpp:239-246). */
+EB_API eb_status eb_add_gravity(struct eb_sim* sim, const double gravity[3]);
+
+/* --- forcing: simulator->force(rod).at(n-1).with(make_forcing(...)) with a
+ * constant lab-frame torque applied at the last element in the material
+ * frame as Q T (elastica/Simulator/Forcing/MakeForcing.hpp:74-165;
+ * examples/axial_stretching/AxialStretchingCaseStudy.cpp:125-134). */
+EB_API eb_status eb_add_end_torque(struct eb_sim* sim, int64_t rod, const double torque_lab[3]);
+
+/* --- rate constraint: the analytical linear damper
+ * (examples/fish_swimming/FishModel/Dissipations/AnalyticalLinearDamper.hpp:
+ * 15-76): v *= exp(-nu_t dt); w_k *= exp(-nu_r m_e J^-1_k dt)^e. */
+EB_API eb_status eb_add_analytical_damper(struct eb_sim* sim, int64_t rod,
+                                          double translational_rate, double rotational_rate);
+
+/* --- simulator->finalize() (Simulator.hpp:538-578): allocates device
+ * memory and uploads the rods.  No rods or constraints may be added after. */
+EB_API eb_status eb_finalize(struct eb_sim* sim);
+
+/* --- simulator->step(PositionVerlet, t, dt) repeated n_steps times
+ * (elastica/Simulator/Interface/TimeSteppers/SymplecticSteppers.hpp:133-217;
+ * elastica/Time/SymplecticSteppers/Algorithms/PositionVerlet.hpp:49-88).
+ * *time is advanced by n_steps * dt.  Asynchronous on the simulator's
+ * stream; eb_get_* and eb_synchronize wait for it. */
+EB_API eb_status eb_step(struct eb_sim* sim, double* time, double dt, int64_t n_steps);
+EB_API eb_status eb_synchronize(struct eb_sim* sim);
+
+/* --- energies (elastica/Systems/CosseratRods/Utility/Energy.hpp:46-141) at
+ * the current state: out[4 r + {0,1,2,3}] = translational, rotational,
+ * shear/stretch, bend/twist energy of rod r. */
+EB_API eb_status eb_energy(struct eb_sim* sim, double* out, int64_t count);
+
+/* The cudaStream_t every kernel and copy of this simulator is issued on, for
+ * callers that order their own work or timing events against it. */
+EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
+
+/* Number of kernel launches this simulator has issued (diagnostic). */
+EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ELASTICA_B200_H */

@@ -1,0 +1,96 @@
+"""Build the oracle's view of a workload from the workload's own parameters
+(the oracle's straight-rod initializer, not the product's), so the product and
+the checker share only the numbers a user would pass in."""
+from __future__ import annotations
+
+import numpy as np
+
+import oracle
+
+
+def oracle_from_workload(wl, damped: bool = False, diagnostics: bool = False):
+    rods = oracle.RodArrays(wl.n_elements, damped=damped)
+    for r, p in enumerate(wl.rods):
+        n = int(p.n_elements)
+        init = oracle.straight_rod(n, p.origin, p.direction, p.normal, p.length, p.radius,
+                                   p.material.density, p.material.youngs_modulus, p.material.shear_modulus)
+        rods.set_rod("x", r, init["x"])
+        rods.set_rod("Q", r, init["Q"].reshape(9, n))
+        rods.set_rod("mass", r, init["mass"])
+        rods.set_rod("rest_length", r, init["l0"])
+        rods.set_rod("rest_voronoi", r, init["D0"])
+        rods.set_rod("volume", r, init["V"])
+        rods.set_rod("shear_diag", r, init["S"])
+        rods.set_rod("bend_diag", r, init["B"])
+        rods.set_rod("inertia_diag", r, init["J"])
+        rods.set_rod("inv_inertia", r, init["Jinv"])
+        if damped:
+            rods.set_rod("nu_force", r, np.full(n + 1, p.force_damping_rate))
+            rods.set_rod("nu_torque", r, np.full(n, p.torque_damping_rate))
+        if wl.velocities is not None:
+            rods.set_rod("v", r, wl.velocities[r])
+        if wl.rest_curvature is not None:
+            rods.set_rod("rest_kappa", r, wl.rest_curvature[r])
+        if wl.clamp:
+            rods.clamp[r] = 1
+            rods.clamp_x[3 * r:3 * r + 3] = init["x"][:, 0]
+            rods.clamp_Q[9 * r:9 * r + 9] = init["Q"][:, :, 0].ravel()
+        if wl.damper is not None:
+            rods.damper_nu[2 * r:2 * r + 2] = wl.damper
+        if wl.end_torque is not None:
+            rods.end_torque[3 * r:3 * r + 3] = wl.end_torque[r]
+    if wl.gravity is not None:
+        rods.gravity[:] = wl.gravity
+    if diagnostics:
+        rods.enable_diagnostics()
+    return rods
+
+
+STATE_MAP = {"Position": "x", "Velocity": "v", "Director": "Q", "AngularVelocity": "w"}
+
+
+def state_slots(rods):
+    """Oracle state as {field: (ncomp, n_slots)} in the product's slot layout."""
+    return {name: rods.comp(key) for name, key in STATE_MAP.items()}
+
+
+def valid_mask(n_elems, place):
+    """Boolean mask over slots of the entries that exist for a stagger."""
+    out = []
+    for n in n_elems:
+        n = int(n)
+        m = np.zeros(n + 1, dtype=bool)
+        cnt = n + 1 if place == 0 else (n if place == 1 else n - 1)
+        m[:cnt] = True
+        out.append(m)
+    return np.concatenate(out)
+
+
+def max_rel_error(got, want, mask):
+    """Normwise relative error: max |got - want| / max |want| over the valid
+    entries of one field (all components)."""
+    g = np.asarray(got)[:, mask]
+    w = np.asarray(want)[:, mask]
+    scale = np.max(np.abs(w))
+    if scale == 0.0:
+        return float(np.max(np.abs(g)))
+    return float(np.max(np.abs(g - w)) / scale)
+
+
+def max_rel_error_per_rod(got, want, n_elems, place):
+    """Largest per-rod normwise relative error of one field:
+    max over rods of max|got - want| / max|want| (entries of that rod's
+    stagger only)."""
+    worst = 0.0
+    o = 0
+    for n in n_elems:
+        n = int(n)
+        cnt = n + 1 if place == 0 else (n if place == 1 else n - 1)
+        g = np.asarray(got)[:, o:o + cnt]
+        w = np.asarray(want)[:, o:o + cnt]
+        scale = np.max(np.abs(w))
+        err = np.max(np.abs(g - w))
+        rel = err / scale if scale > 0 else err
+        worst = max(worst, float(rel))
+        o += n + 1
+    return worst
