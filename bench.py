@@ -212,16 +212,23 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="uneven_batch")
+    ap.add_argument("--rods", type=int, default=None, help="smaller batch (profiling captures only)")
     ap.add_argument("--e2e-cycles", type=int, default=3)
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fma", action="store_true", help="FP64 kernel with FMA contraction")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
 
     from elasticapp_b200 import workloads as W
 
-    wl_fn = lambda rank: W.CONFIGS[args.workload](seed=1002 + rank) if args.workload != "cantilever" \
-        else W.cantilever()
+    def wl_fn(rank):
+        if args.workload == "cantilever":
+            return W.cantilever()
+        kw = {"seed": 1002 + rank}
+        if args.rods is not None:
+            kw["n_rods"] = args.rods
+        return W.CONFIGS[args.workload](**kw)
     if args.impl == "reference":
         return run_reference(args, wl_fn)
 
@@ -242,7 +249,7 @@ def main(argv=None) -> int:
     import elasticapp_b200 as eb
 
     wl = wl_fn(rank)
-    sim = wl.build(device=local)
+    sim = wl.build(device=local, fma=args.fma)
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
     t = 0.0
     t = sim.step(eb.PositionVerlet(), t, wl.dt, args.warmup)
@@ -301,7 +308,7 @@ def main(argv=None) -> int:
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_cycles):
+    for _ in range(max(args.e2e_cycles, 0)):
         for n in names:
             sim.set_slots(n, host[n])
         t = sim.step(eb.PositionVerlet(), t, wl.dt, E2E_STEPS_PER_CYCLE)
@@ -313,7 +320,8 @@ def main(argv=None) -> int:
     e2e_ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
     if pg is not None:
         pg.all_reduce(e2e_ms, op=pg.ReduceOp.MAX)
-    e2e_value = total_elems * E2E_STEPS_PER_CYCLE * args.e2e_cycles / (float(e2e_ms.item()) / 1e3)
+    e2e_value = (total_elems * E2E_STEPS_PER_CYCLE * args.e2e_cycles / (float(e2e_ms.item()) / 1e3)
+                 if args.e2e_cycles > 0 else None)
     finite = all(np.isfinite(host[n]).all() for n in names)
 
     cpu = None
@@ -335,7 +343,8 @@ def main(argv=None) -> int:
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "kernel": "rod_step_fp64", "algorithmic_bytes_per_launch": alg},
+                         "kernel": "rod_step_fp64" + ("_fma" if args.fma else ""),
+                         "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cycle,
                     "d2h_bytes_per_step": bytes_cycle, "steps_per_e2e_step": E2E_STEPS_PER_CYCLE,

@@ -21,8 +21,8 @@ LIB = os.path.join(HERE, "libelastica_b200.so")
 # (object name, source, extra nvcc flags)
 SOURCES = [
     ("eb_capi.o", "eb_capi.cu", []),
-    ("rod_step_fp64.o", "rod_step_fp64.cu", []),
-    ("rod_step_fp64_strict.o", "rod_step_fp64.cu", ["--fmad=false", "-DEB_STRICT_FP64"]),
+    ("rod_step_fp64.o", "rod_step_fp64.cu", ["--fmad=false"]),
+    ("rod_step_fp64_fma.o", "rod_step_fp64.cu", ["-DEB_FMA_FP64"]),
     ("rod_energy.o", "rod_energy.cu", []),
 ]
 HEADERS = ["eb_internal.h", "rod_math.cuh"]

@@ -21,7 +21,7 @@
 
 namespace eb {
 cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
-cudaError_t launch_rod_step_fp64_strict(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_step_fp64_fma(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -54,10 +54,10 @@ struct FieldInfo {
 };
 
 const FieldInfo kFields[EB_FIELD_COUNT] = {
-    {kNode, 3, kState, eb::kX},             // EB_POSITION
-    {kNode, 3, kState, eb::kV},             // EB_VELOCITY
-    {kElement, 9, kState, eb::kQ},          // EB_DIRECTOR
-    {kElement, 3, kState, eb::kW},          // EB_ANGULAR_VELOCITY
+    {kNode, 3, kState, eb::kStX},             // EB_POSITION
+    {kNode, 3, kState, eb::kStV},             // EB_VELOCITY
+    {kElement, 9, kState, eb::kStQ},          // EB_DIRECTOR
+    {kElement, 3, kState, eb::kStW},          // EB_ANGULAR_VELOCITY
     {kNode, 1, kParam, eb::kMass},          // EB_MASS
     {kElement, 1, kParam, eb::kL0},         // EB_REFERENCE_ELEMENT_LENGTH
     {kVoronoi, 1, kParam, eb::kD0},         // EB_REFERENCE_VORONOI_LENGTH
@@ -178,7 +178,7 @@ eb_status init_straight_rod(const eb_straight_rod& p, RodHost& r) {
   for (int d = 0; d < 3; ++d) {
     const double stop = p.origin[d] + p.length * t[d];
     const double step = (stop - p.origin[d]) / static_cast<double>(n);
-    for (int64_t j = 0; j <= n; ++j) S(eb::kX + d, j) = p.origin[d] + static_cast<double>(j) * step;
+    for (int64_t j = 0; j <= n; ++j) S(eb::kStX + d, j) = p.origin[d] + static_cast<double>(j) * step;
   }
   double v1[3] = {nv[0], nv[1], nv[2]}, v2[3], v3[3], tmp[3];
   cross3(t, nv, v2);
@@ -189,12 +189,12 @@ eb_status init_straight_rod(const eb_straight_rod& p, RodHost& r) {
   const double rows[9] = {v1[0],      v1[1],      v1[2],      v2[0] / n2, v2[1] / n2,
                           v2[2] / n2, v3[0] / n3, v3[1] / n3, v3[2] / n3};
   for (int k = 0; k < 9; ++k)
-    for (int64_t i = 0; i < n; ++i) S(eb::kQ + k, i) = rows[k];
+    for (int64_t i = 0; i < n; ++i) S(eb::kStQ + k, i) = rows[k];
 
   std::vector<double> l0(n), rad(n);
   for (int64_t i = 0; i < n; ++i) {
-    const double dx[3] = {S(eb::kX, i + 1) - S(eb::kX, i), S(eb::kX + 1, i + 1) - S(eb::kX + 1, i),
-                          S(eb::kX + 2, i + 1) - S(eb::kX + 2, i)};
+    const double dx[3] = {S(eb::kStX, i + 1) - S(eb::kStX, i), S(eb::kStX + 1, i + 1) - S(eb::kStX + 1, i),
+                          S(eb::kStX + 2, i + 1) - S(eb::kStX + 2, i)};
     l0[i] = norm3(dx) / 1.0;
     P(eb::kL0, i) = l0[i];
   }
@@ -524,8 +524,8 @@ EB_API eb_status eb_constrain_clamp(eb_sim* s, int64_t rod, int64_t index) {
   if (index != 0) return fail(EB_ERR_UNSUPPORTED, "only the clamp at index 0 is supported");
   RodHost& r = s->rods[rod];
   const int64_t W = r.n + 1;
-  for (int d = 0; d < 3; ++d) r.info.clamp_x[d] = r.state[static_cast<size_t>((eb::kX + d) * W)];
-  for (int k = 0; k < 9; ++k) r.info.clamp_Q[k] = r.state[static_cast<size_t>((eb::kQ + k) * W)];
+  for (int d = 0; d < 3; ++d) r.info.clamp_x[d] = r.state[static_cast<size_t>((eb::kStX + d) * W)];
+  for (int k = 0; k < 9; ++k) r.info.clamp_Q[k] = r.state[static_cast<size_t>((eb::kStQ + k) * W)];
   r.info.flags |= eb::kRodClamp;
   s->sim_flags |= eb::kSimClamp;
   return EB_OK;
@@ -669,8 +669,8 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     a.out = s->d_state[s->cur ^ 1];
     const bool rec = diag && (k == n_steps - 1);
     a.diag = rec ? s->d_diag : nullptr;
-    if (s->cfg.flags & EB_FLAG_STRICT_FP64)
-      EB_CUDA(eb::launch_rod_step_fp64_strict(a, rec, s->any_damped, s->stream));
+    if (s->cfg.flags & EB_FLAG_FMA_FP64)
+      EB_CUDA(eb::launch_rod_step_fp64_fma(a, rec, s->any_damped, s->stream));
     else
       EB_CUDA(eb::launch_rod_step_fp64(a, rec, s->any_damped, s->stream));
     s->cur ^= 1;

@@ -31,10 +31,10 @@ constexpr uint32_t kFlagMask = (1u << kRodShift) - 1u;
 
 // state arrays (per ping-pong buffer), in units of `stride`
 enum StateField : int {
-  kX = 0,   // 3: node positions
-  kV = 3,   // 3: node velocities
-  kQ = 6,   // 9: element directors, Q(k, j) at kQ + 3k + j
-  kW = 15,  // 3: element angular velocities (material frame)
+  kStX = 0,   // 3: node positions
+  kStV = 3,   // 3: node velocities
+  kStQ = 6,   // 9: element directors, Q(k, j) at kStQ + 3k + j
+  kStW = 15,  // 3: element angular velocities (material frame)
   kStateFields = 18
 };
 

@@ -27,18 +27,18 @@ __global__ void rod_energy_kernel(int64_t n_rods, int64_t S, const int64_t* __re
   double et = 0.0, er = 0.0, es = 0.0, eb = 0.0;
   for (int64_t j = lane; j <= n; j += 32) {
     const int64_t g = o + j;
-    const D3 v = ld3(st + kV * S, S, g);
+    const D3 v = ld3(st + kStV * S, S, g);
     et += par[kMass * S + g] * (v.x * v.x + v.y * v.y + v.z * v.z);
     if (j < n) {
-      const D3 dx = ld3(st + kX * S, S, g + 1) - ld3(st + kX * S, S, g);
+      const D3 dx = ld3(st + kStX * S, S, g + 1) - ld3(st + kStX * S, S, g);
       const double l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
       const double e = l / par[kL0 * S + g];
-      const D3 w = ld3(st + kW * S, S, g);
+      const D3 w = ld3(st + kStW * S, S, g);
       const D3 J = ld3(par + kJ * S, S, g);
       er += w.x * (J.x * w.x / e) + w.y * (J.y * w.y / e) + w.z * (J.z * w.z / e);
       double q[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) q[k] = st[(kQ + k) * S + g];
+      for (int k = 0; k < 9; ++k) q[k] = st[(kStQ + k) * S + g];
       const D3 qt = matvec(q, divide(dx, l));
       const D3 s0 = ld3(par + kSig0 * S, S, g);
       const D3 sh = ld3(par + kShear * S, S, g);
@@ -47,7 +47,7 @@ __global__ void rod_energy_kernel(int64_t n_rods, int64_t S, const int64_t* __re
       if (j + 1 < n) {
         double qn[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) qn[k] = st[(kQ + k) * S + g + 1];
+        for (int k = 0; k < 9; ++k) qn[k] = st[(kStQ + k) * S + g + 1];
         const D3 kp = inv_rotate_divide(q, qn, par[kD0 * S + g]);
         const D3 k0 = ld3(par + kKap0 * S, S, g);
         const D3 B = ld3(par + kBend * S, S, g);

@@ -188,12 +188,12 @@ class Simulator:
     """Owns one eb_sim (device memory and a CUDA stream)."""
 
     def __init__(self, device: int = 0, precision: str = "fp64", record_diagnostics: bool = False,
-                 strict_fp64: bool = False):
+                 fma: bool = False):
         cfg = L.EbConfig()
         cfg.device = int(device)
         cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
         cfg.flags = (L.EB_FLAG_RECORD_DIAGNOSTICS if record_diagnostics else 0) | (
-            L.EB_FLAG_STRICT_FP64 if strict_fp64 else 0)
+            L.EB_FLAG_FMA_FP64 if fma else 0)
         h = ctypes.c_void_p()
         L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h

