@@ -216,7 +216,9 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-cycles", type=int, default=3)
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--fma", action="store_true", help="FP64 kernel with FMA contraction")
+    ap.add_argument("--reference-rounding", action="store_true",
+                    help="FP64 build that rounds every operation as the reference's scalar code")
+    ap.add_argument("--window", type=int, default=0, help="slots per CTA of the step kernel (128/256)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
 
@@ -249,7 +251,7 @@ def main(argv=None) -> int:
     import elasticapp_b200 as eb
 
     wl = wl_fn(rank)
-    sim = wl.build(device=local, fma=args.fma)
+    sim = wl.build(device=local, reference_rounding=args.reference_rounding, window=args.window)
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
     t = 0.0
     t = sim.step(eb.PositionVerlet(), t, wl.dt, args.warmup)
@@ -343,7 +345,7 @@ def main(argv=None) -> int:
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "kernel": "rod_step_fp64" + ("_fma" if args.fma else ""),
+                         "kernel": "rod_step_fp64" + ("_reference" if args.reference_rounding else ""),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cycle,

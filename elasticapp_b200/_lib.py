@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "EB_OK", 1: "EB_ERR_INVALID_ARGUMENT", 2: "EB_ERR_INVALID_STA
 EB_PRECISION_FP64 = 0
 EB_PRECISION_MIXED = 1
 EB_FLAG_RECORD_DIAGNOSTICS = 0x1
-EB_FLAG_FMA_FP64 = 0x2
+EB_FLAG_REFERENCE_ROUNDING = 0x2
 EB_ROD_DAMPED = 0
 EB_ROD_UNDAMPED = 1
 EB_LAYOUT_PER_ROD = 0
@@ -55,7 +55,7 @@ DERIVED_FIELDS = set(FIELDS[16:])
 
 class EbConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("flags", ctypes.c_uint32), ("reserved", ctypes.c_int32)]
+                ("flags", ctypes.c_uint32), ("step_window", ctypes.c_int32)]
 
 
 class EbStraightRod(ctypes.Structure):

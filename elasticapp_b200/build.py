@@ -21,11 +21,11 @@ LIB = os.path.join(HERE, "libelastica_b200.so")
 # (object name, source, extra nvcc flags)
 SOURCES = [
     ("eb_capi.o", "eb_capi.cu", []),
-    ("rod_step_fp64.o", "rod_step_fp64.cu", ["--fmad=false"]),
-    ("rod_step_fp64_fma.o", "rod_step_fp64.cu", ["-DEB_FMA_FP64"]),
+    ("rod_step_fp64.o", "rod_step_fp64.cu", ["-DEB_FAST_FP64"]),
+    ("rod_step_fp64_reference.o", "rod_step_fp64.cu", ["--fmad=false"]),
     ("rod_energy.o", "rod_energy.cu", []),
 ]
-HEADERS = ["eb_internal.h", "rod_math.cuh"]
+HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

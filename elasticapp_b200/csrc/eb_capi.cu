@@ -20,8 +20,9 @@
 #include "eb_internal.h"
 
 namespace eb {
-cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
-cudaError_t launch_rod_step_fp64_fma(const StepArgs& args, bool diag, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream);
+cudaError_t launch_rod_step_fp64_reference(const StepArgs& args, bool diag, bool damped, int window,
+                                           cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -117,6 +118,7 @@ struct eb_sim {
   eb::RodInfo* d_rods = nullptr;
   int64_t* d_offsets = nullptr;
   double* d_energy = nullptr;
+  uint32_t* d_status = nullptr;
   int cur = 0;
   double damper_dt = -1.0;
   int64_t launches = 0;
@@ -274,10 +276,23 @@ void host_free(eb_sim* s) {
   if (s->d_rods) cudaFree(s->d_rods);
   if (s->d_offsets) cudaFree(s->d_offsets);
   if (s->d_energy) cudaFree(s->d_energy);
+  if (s->d_status) cudaFree(s->d_status);
+  s->d_status = nullptr;
   s->d_state[0] = s->d_state[1] = s->d_param = s->d_diag = s->d_energy = nullptr;
   s->d_meta = nullptr;
   s->d_rods = nullptr;
   s->d_offsets = nullptr;
+}
+
+// Read the device status word after the stream has drained.
+eb_status check_device_status(eb_sim* s) {
+  if (!s->d_status) return EB_OK;
+  uint32_t st = 0;
+  EB_CUDA(cudaMemcpyAsync(&st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  if (st & eb::kStatusCopyTimeout)
+    return fail(EB_ERR_CUDA, "a step kernel gave up waiting for its bulk copies (bounded wait expired)");
+  return EB_OK;
 }
 
 eb_status upload_rod_table(eb_sim* s) {
@@ -303,6 +318,8 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
   if (config) cfg = *config;
   if (cfg.precision != EB_PRECISION_FP64 && cfg.precision != EB_PRECISION_MIXED)
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (cfg.step_window != 0 && cfg.step_window != 128 && cfg.step_window != 256)
+    return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
   if (cfg.precision == EB_PRECISION_MIXED)
     return fail(EB_ERR_UNSUPPORTED, "mixed precision is not built into this library yet");
   int ndev = 0;
@@ -446,7 +463,7 @@ EB_API eb_status eb_get_field(eb_sim* s, int64_t rod, int32_t field, double* val
                             s->stride * sizeof(double), per * sizeof(double), fi->ncomp,
                             cudaMemcpyDeviceToHost, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
-  return EB_OK;
+  return check_device_status(s);
 }
 
 static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* host, int64_t count,
@@ -473,7 +490,7 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
       EB_CUDA(cudaMemcpy2DAsync(host, w, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToHost, s->stream));
     }
     EB_CUDA(cudaStreamSynchronize(s->stream));
-    return EB_OK;
+    return to_device ? EB_OK : check_device_status(s);
   }
   if (layout != EB_LAYOUT_PER_ROD) return fail(EB_ERR_INVALID_ARGUMENT, "unknown layout");
   int64_t total = 0;
@@ -618,6 +635,7 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   alloc(reinterpret_cast<void**>(&s->d_rods), static_cast<size_t>(nr) * sizeof(eb::RodInfo));
   alloc(reinterpret_cast<void**>(&s->d_offsets), static_cast<size_t>(nr + 1) * sizeof(int64_t));
   alloc(reinterpret_cast<void**>(&s->d_energy), static_cast<size_t>(4 * nr) * sizeof(double));
+  alloc(reinterpret_cast<void**>(&s->d_status), sizeof(uint32_t));
   if (e != cudaSuccess) {
     host_free(s);
     return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA,
@@ -631,6 +649,7 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   EB_CUDA(cudaMemcpyAsync(s->d_meta, meta.data(), meta.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaMemcpyAsync(s->d_offsets, s->offsets.data(), s->offsets.size() * sizeof(int64_t),
                           cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(uint32_t), s->stream));
   s->cur = 0;
   s->finalized = true;
   if (eb_status st = upload_rod_table(s)) return st;
@@ -663,16 +682,18 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   a.half_dt = 0.5 * dt;
   for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
   a.sim_flags = s->sim_flags;
+  a.status = s->d_status;
   const bool diag = s->d_diag != nullptr;
   for (int64_t k = 0; k < n_steps; ++k) {
     a.in = s->d_state[s->cur];
     a.out = s->d_state[s->cur ^ 1];
     const bool rec = diag && (k == n_steps - 1);
     a.diag = rec ? s->d_diag : nullptr;
-    if (s->cfg.flags & EB_FLAG_FMA_FP64)
-      EB_CUDA(eb::launch_rod_step_fp64_fma(a, rec, s->any_damped, s->stream));
+    const int window = s->cfg.step_window ? s->cfg.step_window : 128;
+    if (s->cfg.flags & EB_FLAG_REFERENCE_ROUNDING)
+      EB_CUDA(eb::launch_rod_step_fp64_reference(a, rec, s->any_damped, window, s->stream));
     else
-      EB_CUDA(eb::launch_rod_step_fp64(a, rec, s->any_damped, s->stream));
+      EB_CUDA(eb::launch_rod_step_fp64(a, rec, s->any_damped, window, s->stream));
     s->cur ^= 1;
     ++s->launches;
     if (time) {
@@ -689,7 +710,7 @@ EB_API eb_status eb_synchronize(eb_sim* s) {
   if (!s->stream) return EB_OK;
   if (eb_status st = set_device(s)) return st;
   EB_CUDA(cudaStreamSynchronize(s->stream));
-  return EB_OK;
+  return check_device_status(s);
 }
 
 EB_API eb_status eb_energy(eb_sim* s, double* out, int64_t count) {
@@ -704,7 +725,7 @@ EB_API eb_status eb_energy(eb_sim* s, double* out, int64_t count) {
   EB_CUDA(cudaMemcpyAsync(out, s->d_energy, static_cast<size_t>(4 * nr) * sizeof(double),
                           cudaMemcpyDeviceToHost, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
-  return EB_OK;
+  return check_device_status(s);
 }
 
 EB_API eb_status eb_get_stream(const eb_sim* s, void** stream) {

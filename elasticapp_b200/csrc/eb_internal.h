@@ -94,11 +94,15 @@ struct StepArgs {
   const uint32_t* meta; // slot metadata
   const RodInfo* rods;
   double* diag;         // derived fields, or nullptr
+  uint32_t* status;     // device status word (kStatus* bits), never cleared by kernels
   double dt;
   double half_dt;
   double gravity[3];
   uint32_t sim_flags;   // kSim* below
 };
+
+// device status bits reported back to the host
+enum StatusBits : uint32_t { kStatusCopyTimeout = 1u };
 
 enum SimFlags : uint32_t { kSimGravity = 1u, kSimDamper = 2u, kSimEndTorque = 4u, kSimClamp = 8u };
 

@@ -16,96 +16,190 @@
 // boundaries.  CTA b runs kWindow threads over the slots
 // [b*kTile - 2, b*kTile - 2 + kWindow); thread k owns slot b*kTile - 2 + k and
 // computes every phase for it.  The outputs of the kTile interior slots
-// (threads 2 .. kTile+1) are stored; the two slots on the left and on the
-// right are recomputed halo (the stencils reach one slot left and two right).
-// Because the step reads the previous state from one buffer and writes the
-// other, halos can be recomputed redundantly, so rods of any length map onto
-// the same tiles without packing.  Rod ends need no special code: at an end
-// the neighbouring slot holds no element / Voronoi point and contributes the
-// zero that the reference's ghost slots contribute.
+// (threads 2 .. kTile+1) are stored; the two slots on either side are
+// recomputed halo (the stencils reach one slot left and two right).  Because
+// the step reads the previous state from one buffer and writes the other,
+// halos can be recomputed redundantly, so rods of any length map onto the
+// same tiles without packing.  Rod ends need no special code: at an end the
+// neighbouring slot holds no element / Voronoi point and contributes the zero
+// that the reference's ghost slots contribute.
+//
+// Staging: one thread issues a bulk asynchronous copy (TMA, cp.async.bulk)
+// per input field of the window into shared memory, completing on one
+// mbarrier; the threads then compute from shared memory.  Every field row of
+// a window is 16-byte aligned in global memory because windows start on an
+// even slot and every field array starts on a 256-byte boundary.  The values
+// exchanged between neighbouring threads (element lengths, Q^T n_L / e, the
+// couple terms) are written over input rows that only their own thread reads
+// and has consumed, so shared memory holds one row per staged input field.
 #include <cuda_runtime.h>
 
+#include "bulk_copy.cuh"
 #include "eb_internal.h"
 #include "rod_math.cuh"
 
 namespace eb {
 namespace {
 
-constexpr int kWindow = 256;            // threads per CTA = slots per window
-constexpr int kTile = kWindow - 4;      // interior slots stored per CTA
-constexpr int kLeftHalo = 2;            // window starts 2 slots left of the tile
-constexpr int kMinBlocks = 2;           // CTAs per SM the register budget targets
-
-using D3 = Vec3<double>;
-
-struct Smem {
-  double x[3][kWindow];  // positions after the first half drift (later: h terms)
-  double v[3][kWindow];  // velocities (later: g terms)
-  double q[9][kWindow];  // directors after the first half drift
-  double l[kWindow];     // element lengths
-  double f[3][kWindow];  // Q^T n_L / e per element (zero where no element)
-  double m[kWindow];     // node masses
+// shared-memory row of every staged input field: the 18 state rows, then the
+// parameter rows the variant needs (nu_f/nu_t only for explicitly damped
+// rods, the volume only when diagnostics are recorded)
+template <bool kDamped, bool kDiag>
+struct RowMap {
+  static constexpr int param(int f) {
+    return kStateFields + f - ((!kDamped && f > kNuF) ? 1 : 0) - ((!kDamped && f > kNuT) ? 1 : 0) -
+           ((!kDiag && f > kVol) ? 1 : 0);
+  }
+  static constexpr bool needed(int f) {
+    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol));
+  }
+  static constexpr int rows() { return kStateFields + kParamFields - (kDamped ? 0 : 2) - (kDiag ? 0 : 1); }
 };
 
-__device__ __forceinline__ D3 ld3(const double* __restrict__ p, int64_t S, int64_t g) {
-  return {p[g], p[S + g], p[2 * S + g]};
-}
+constexpr uint32_t kMaxPolls = 1u << 22;
+using D3 = Vec3<double>;
+
+template <int W>
+struct Rows {
+  double* base;
+  __device__ __forceinline__ double* row(int r) const { return base + r * W; }
+  __device__ __forceinline__ double& at(int r, int s) const { return base[r * W + s]; }
+  __device__ __forceinline__ D3 get3(int r, int s) const {
+    return {base[r * W + s], base[(r + 1) * W + s], base[(r + 2) * W + s]};
+  }
+  __device__ __forceinline__ void put3(int r, int s, D3 v) const {
+    base[r * W + s] = v.x;
+    base[(r + 1) * W + s] = v.y;
+    base[(r + 2) * W + s] = v.z;
+  }
+};
+
 __device__ __forceinline__ void st3(double* __restrict__ p, int64_t S, int64_t g, D3 a) {
   p[g] = a.x;
   p[S + g] = a.y;
   p[2 * S + g] = a.z;
 }
-__device__ __forceinline__ D3 sm3(const double (*a)[kWindow], int s) { return {a[0][s], a[1][s], a[2][s]}; }
-__device__ __forceinline__ void ss3(double (*a)[kWindow], int s, D3 v) {
-  a[0][s] = v.x;
-  a[1][s] = v.y;
-  a[2][s] = v.z;
+
+__device__ __forceinline__ void so3(double q[9], double u0, double u1, double u2) {
+#ifdef EB_FAST_FP64
+  so3_update_fast(q, u0, u1, u2);
+#else
+  so3_update(q, u0, u1, u2);
+#endif
 }
 
-template <bool kDiag, bool kDamped>
-__global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(const StepArgs a) {
-  __shared__ Smem sm;
+__device__ __forceinline__ D3 curvature(const double qc[9], const double qn[9], double span) {
+#ifdef EB_FAST_FP64
+  return inv_rotate_divide_fast(qc, qn, span);
+#else
+  return inv_rotate_divide(qc, qn, span);
+#endif
+}
+
+// a / d for three numerators (the fast build forms one reciprocal)
+__device__ __forceinline__ D3 div3(D3 a, double d) {
+#ifdef EB_FAST_FP64
+  const double r = 1.0 / d;
+  return {a.x * r, a.y * r, a.z * r};
+#else
+  return divide(a, d);
+#endif
+}
+
+template <int W, bool kDiag, bool kDamped>
+__device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem) {
+  using M = RowMap<kDamped, kDiag>;
+  constexpr int kTile = W - 4;  // interior slots stored per CTA (even)
+  constexpr int kLeftHalo = 2;  // window starts 2 slots left of the tile
+  constexpr int kRows = M::rows();
+  // rows of the inputs
+  constexpr int rX = kStX, rV = kStV, rQ = kStQ, rW = kStW;
+  constexpr int rMass = M::param(kMass), rL0 = M::param(kL0), rD0 = M::param(kD0);
+  constexpr int rSig0 = M::param(kSig0), rKap0 = M::param(kKap0), rShear = M::param(kShear);
+  constexpr int rBend = M::param(kBend), rJ = M::param(kJ), rJinv = M::param(kJinv);
+  constexpr int rNuF = M::param(kNuF), rNuT = M::param(kNuT), rVol = M::param(kVol);
+  // exchange rows, each over rows only the owning thread reads:
+  //   f (written in phase 2) over the angular velocity rows (read in phase 1)
+  //   l (phase 2) over the first rest-strain row (read earlier in phase 2)
+  //   g, h (phase 3) over the inertia and shear rigidity rows (read in phase 2)
+  constexpr int rF = rW, rL = rSig0, rG = rJ, rH = rShear;
+
+  const Rows<W> R{smem};
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kRows * W);
+
   const int s = threadIdx.x;
-  const int64_t g = static_cast<int64_t>(blockIdx.x) * kTile - kLeftHalo + s;
+  const int64_t g0 = static_cast<int64_t>(blockIdx.x) * kTile - kLeftHalo;
+  const int64_t g = g0 + s;
   const int64_t S = a.stride;
   const bool valid = g >= 0 && g < a.n_slots;
   const bool interior = valid && s >= kLeftHalo && s < kLeftHalo + kTile;
   const uint32_t meta = valid ? a.meta[g] : 0u;
-  const double* __restrict__ in = a.in;
-  const double* __restrict__ par = a.par;
+  // per-rod constraint data, fetched while the bulk copies are in flight
+  uint32_t rflags = 0;
+  double damper_t = 1.0, damper_r = 0.0;
+  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
+    const RodInfo* ri = a.rods + (meta >> kRodShift);
+    rflags = ri->flags;
+    damper_t = ri->damper_t;
+    damper_r = ri->damper_r;
+  }
+
+  // ---- stage the window's inputs with bulk copies
+  if (s == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (s == 0) {
+    const int64_t lo = g0 < 0 ? 0 : g0;
+    const int64_t hi = (g0 + W < S) ? g0 + W : S;
+    const uint32_t bytes = static_cast<uint32_t>((hi - lo) * sizeof(double));
+    const int off = static_cast<int>(lo - g0);
+    mbar_arrive_expect_tx(bar, bytes * static_cast<uint32_t>(kRows));
+#pragma unroll 1
+    for (int f = 0; f < kStateFields; ++f) bulk_g2s(R.row(f) + off, a.in + f * S + lo, bytes, bar);
+#pragma unroll 1
+    for (int f = 0; f < kParamFields; ++f)
+      if (M::needed(f)) bulk_g2s(R.row(M::param(f)) + off, a.par + f * S + lo, bytes, bar);
+  }
+  if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+    // a copy never completed: record it, give the copies one more bounded
+    // wait so none is left writing into this CTA's shared memory, and leave
+    if (s == 0) atomicOr(a.status, kStatusCopyTimeout);
+    (void)mbar_wait_bounded(bar, 0, kMaxPolls);
+    return;
+  }
+
   const double hdt = a.half_dt;
 
-  // ---- phase 1: load, first kinematic half step, clamp value constraint
+  // ---- phase 1: first kinematic half step and clamp value constraint,
+  // in place in shared memory
   D3 x{0.0, 0.0, 0.0}, v{0.0, 0.0, 0.0}, w{0.0, 0.0, 0.0};
   double q[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) q[k] = 0.0;
   double m = 1.0;
   if (valid) {
-    v = ld3(in + kStV * S, S, g);
-    const D3 x0 = ld3(in + kStX * S, S, g);
+    v = R.get3(rV, s);
+    const D3 x0 = R.get3(rX, s);
     x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
-    m = par[kMass * S + g];
+    m = R.at(rMass, s);
     if (meta & kElem) {
 #pragma unroll
-      for (int k = 0; k < 9; ++k) q[k] = in[(kStQ + k) * S + g];
-      w = ld3(in + kStW * S, S, g);
-      so3_update(q, hdt * w.x, hdt * w.y, hdt * w.z);
+      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
+      w = R.get3(rW, s);
+      so3(q, hdt * w.x, hdt * w.y, hdt * w.z);
     }
-    if ((a.sim_flags & kSimClamp) && (meta & kFirst)) {
+    if ((meta & kFirst) && (rflags & kRodClamp)) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
-      if (ri.flags & kRodClamp) {
-        x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+      x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
 #pragma unroll
-        for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
-      }
+      for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
     }
-  }
-  ss3(sm.x, s, x);
-  ss3(sm.v, s, v);
+    R.put3(rX, s, x);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) sm.q[k][s] = q[k];
-  sm.m[s] = m;
+    for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
+  }
   __syncthreads();
 
   // ---- phase 2: element geometry and internal stress
@@ -113,35 +207,34 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
   // and the element-local torque terms in the reference's summation order
   // (WithDiagonalLinearHyperElasticModel.hpp:341-384).  The last thread of
   // the window has no right neighbour and only supplies its position.
-  const bool elem = (meta & kElem) && s + 1 < kWindow;
-  double l = 1.0, e = 1.0;
+  const bool elem = (meta & kElem) && s + 1 < W;
+  double l = 1.0, e = 1.0, l0 = 1.0;
   D3 t{0.0, 0.0, 0.0}, sigma{0.0, 0.0, 0.0}, nl{0.0, 0.0, 0.0};
   D3 t_shear{0.0, 0.0, 0.0}, t_lag{0.0, 0.0, 0.0}, t_unst{0.0, 0.0, 0.0};
   {
     D3 f{0.0, 0.0, 0.0};
     if (elem) {
-      const D3 dx = sm3(sm.x, s + 1) - x;
+      const D3 dx = R.get3(rX, s + 1) - x;
       l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
-      t = divide(dx, l);
-      const double l0 = par[kL0 * S + g];
+      t = div3(dx, l);
+      l0 = R.at(rL0, s);
       e = l / l0;
       const D3 qt = matvec(q, t);
       sigma = {qt.x * e, qt.y * e, qt.z * e - 1.0};
-      const D3 s0 = ld3(par + kSig0 * S, S, g);
-      const D3 sh = ld3(par + kShear * S, S, g);
-      const D3 d = sigma - s0;
+      const D3 d = sigma - R.get3(rSig0, s);
+      const D3 sh = R.get3(rShear, s);
       nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
-      f = divide(mattranspvec(q, nl), e);
+      f = div3(mattranspvec(q, nl), e);
       t_shear = scale(cross(qt, nl), l0);
-      const D3 J = ld3(par + kJ * S, S, g);
-      const D3 jwe = divide(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
+      const D3 J = R.get3(rJ, s);
+      const D3 jwe = div3(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
       t_lag = cross(jwe, w);
-      const D3 dv = sm3(sm.v, s + 1) - v;
+      const D3 dv = R.get3(rV, s + 1) - v;
       const double rate = dot(t, dv) / (e * l0);
       t_unst = scale(jwe, rate);
     }
-    sm.l[s] = l;
-    ss3(sm.f, s, f);
+    R.at(rL, s) = l;
+    R.put3(rF, s, f);
   }
   __syncthreads();
 
@@ -151,34 +244,32 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
   double eps = 1.0;
   {
     D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
-    if ((meta & kVor) && s + 1 < kWindow) {
+    if ((meta & kVor) && s + 1 < W) {
       double qn[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) qn[k] = sm.q[k][s + 1];
-      const double D0 = par[kD0 * S + g];
-      kappa = inv_rotate_divide(q, qn, D0);
-      const double D = 0.5 * (l + sm.l[s + 1]);
+      for (int k = 0; k < 9; ++k) qn[k] = R.at(rQ + k, s + 1);
+      const double D0 = R.at(rD0, s);
+      kappa = curvature(q, qn, D0);
+      const double D = 0.5 * (l + R.at(rL, s + 1));
       eps = D / D0;
       const double ic = 1.0 / (eps * eps * eps);
-      const D3 k0 = ld3(par + kKap0 * S, S, g);
-      const D3 B = ld3(par + kBend * S, S, g);
-      const D3 dk = kappa - k0;
+      const D3 dk = kappa - R.get3(rKap0, s);
+      const D3 B = R.get3(rBend, s);
       tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
       gg = scale(tau, ic);
       hh = scale(cross(kappa, tau), ic * D0);
     }
-    // g and h reuse the velocity and position rows, free after phase 2
-    ss3(sm.v, s, gg);
-    ss3(sm.x, s, hh);
+    R.put3(rG, s, gg);
+    R.put3(rH, s, hh);
   }
   __syncthreads();
 
   if (!interior) return;
 
   // ---- phase 4: loads, update_acceleration (WithRodKinematics.hpp:684-714)
-  D3 F = sm3(sm.f, s) - sm3(sm.f, s - 1);
+  D3 F = R.get3(rF, s) - R.get3(rF, s - 1);
   if (kDamped) {
-    const double c = m * par[kNuF * S + g];
+    const double c = m * R.at(rNuF, s);
     F = {F.x - c * v.x, F.y - c * v.y, F.z - c * v.z};
   }
   D3 Fe{0.0, 0.0, 0.0};
@@ -187,60 +278,55 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
   const double inv_m = 1.0 / m;
   const D3 acc = {(F.x + Fe.x) * inv_m, (F.y + Fe.y) * inv_m, (F.z + Fe.z) * inv_m};
 
-  const RodInfo* ri = nullptr;
-  if (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) ri = a.rods + (meta >> kRodShift);
-
   D3 T{0.0, 0.0, 0.0}, alpha{0.0, 0.0, 0.0};
-  double jinv[3] = {0.0, 0.0, 0.0};
+  D3 jinv{0.0, 0.0, 0.0};
   if (meta & kElem) {
-    T = sm3(sm.v, s) - sm3(sm.v, s - 1);                  // two-point difference of g
-    const D3 h1 = sm3(sm.x, s), h0 = sm3(sm.x, s - 1);    // quadrature of h
+    T = R.get3(rG, s) - R.get3(rG, s - 1);                // two-point difference of g
+    const D3 h1 = R.get3(rH, s), h0 = R.get3(rH, s - 1);  // quadrature of h
     T = T + D3{0.5 * (h1.x + h0.x), 0.5 * (h1.y + h0.y), 0.5 * (h1.z + h0.z)};
     T = T + t_shear;
     T = T + t_lag;
     T = T + t_unst;
     if (kDamped) {
-      const double em = 0.5 * (m + sm.m[s + 1]);
-      const double c = em * par[kNuT * S + g];
+      const double em = 0.5 * (m + R.at(rMass, s + 1));
+      const double c = em * R.at(rNuT, s);
       T = {T.x - c * w.x, T.y - c * w.y, T.z - c * w.z};
     }
     D3 Te{0.0, 0.0, 0.0};
-    if ((a.sim_flags & kSimEndTorque) && (meta & kLastElem) && (ri->flags & kRodEndTorque)) {
-      const D3 tl = {ri->end_torque[0], ri->end_torque[1], ri->end_torque[2]};
-      Te = Te + matvec(q, tl);
+    if ((meta & kLastElem) && (rflags & kRodEndTorque)) {
+      const RodInfo& ri = a.rods[meta >> kRodShift];
+      Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
     }
-    jinv[0] = par[(kJinv + 0) * S + g];
-    jinv[1] = par[(kJinv + 1) * S + g];
-    jinv[2] = par[(kJinv + 2) * S + g];
-    alpha = {(jinv[0] * (T.x + Te.x)) * e, (jinv[1] * (T.y + Te.y)) * e, (jinv[2] * (T.z + Te.z)) * e};
+    jinv = R.get3(rJinv, s);
+    alpha = {(jinv.x * (T.x + Te.x)) * e, (jinv.y * (T.y + Te.y)) * e, (jinv.z * (T.z + Te.z)) * e};
   }
 
   // ---- dynamic step and rate constraints
   const double dt = a.dt;
   v = {v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z};
   if (meta & kElem) w = {w.x + dt * alpha.x, w.y + dt * alpha.y, w.z + dt * alpha.z};
-  if ((a.sim_flags & kSimClamp) && (meta & kFirst) && (ri->flags & kRodClamp)) {
+  if ((meta & kFirst) && (rflags & kRodClamp)) {
     v = D3{0.0, 0.0, 0.0};
     w = D3{0.0, 0.0, 0.0};
   }
-  if ((a.sim_flags & kSimDamper) && (ri->flags & kRodDamper)) {
-    const double tc = ri->damper_t;
-    v = {v.x * tc, v.y * tc, v.z * tc};
+  if (rflags & kRodDamper) {
+    v = {v.x * damper_t, v.y * damper_t, v.z * damper_t};
     if (meta & kElem) {
       // AnalyticalLinearDamper.hpp:40-75: w_k *= exp(y_k)^e with
       // y_k = -nu_r m_e J^-1_k dt.  The reference-rounding build evaluates it
-      // as written; the FMA build uses exp(e y_k) (equal up to rounding, one
+      // as written; the fast build uses exp(e y_k) (equal up to rounding, one
       // transcendental instead of two).
-      double em = 0.5 * (m + sm.m[s + 1]);
+      const double mn = R.at(rMass, s + 1);
+      double em = 0.5 * (m + mn);
       if (meta & kFirst) em += 0.5 * m;
-      if (meta & kLastElem) em += 0.5 * sm.m[s + 1];
-      const double nur = ri->damper_r;
-#ifdef EB_FMA_FP64
-      w = {w.x * exp(e * (-nur * em * jinv[0] * dt)), w.y * exp(e * (-nur * em * jinv[1] * dt)),
-           w.z * exp(e * (-nur * em * jinv[2] * dt))};
+      if (meta & kLastElem) em += 0.5 * mn;
+      const double nur = damper_r;
+#ifdef EB_FAST_FP64
+      w = {w.x * exp(e * (-nur * em * jinv.x * dt)), w.y * exp(e * (-nur * em * jinv.y * dt)),
+           w.z * exp(e * (-nur * em * jinv.z * dt))};
 #else
-      w = {w.x * pow(exp(-nur * em * jinv[0] * dt), e), w.y * pow(exp(-nur * em * jinv[1] * dt), e),
-           w.z * pow(exp(-nur * em * jinv[2] * dt), e)};
+      w = {w.x * pow(exp(-nur * em * jinv.x * dt), e), w.y * pow(exp(-nur * em * jinv.y * dt), e),
+           w.z * pow(exp(-nur * em * jinv.z * dt), e)};
 #endif
     }
   }
@@ -251,7 +337,7 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
   st3(out + kStX * S, S, g, x);
   st3(out + kStV * S, S, g, v);
   if (meta & kElem) {
-    so3_update(q, hdt * w.x, hdt * w.y, hdt * w.z);
+    so3(q, hdt * w.x, hdt * w.y, hdt * w.z);
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[(kStQ + k) * S + g] = q[k];
     st3(out + kStW * S, S, g, w);
@@ -262,14 +348,14 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
     st3(dg + kDLoads * S, S, g, F);  // InternalLoads include the damping force
     st3(dg + kDAccel * S, S, g, acc);
     if (meta & kElem) {
-      dg[kDLength * S + g] = e * par[kL0 * S + g];
+      dg[kDLength * S + g] = e * l0;
       dg[kDDil * S + g] = e;
       st3(dg + kDTangent * S, S, g, t);
       st3(dg + kDSigma * S, S, g, sigma);
       st3(dg + kDStress * S, S, g, nl);
       st3(dg + kDTorques * S, S, g, T);
       st3(dg + kDAlpha * S, S, g, alpha);
-      dg[kDDim * S + g] = sqrt(M_1_PI * par[kVol * S + g] / l);
+      dg[kDDim * S + g] = sqrt(M_1_PI * R.at(rVol, s) / l);
     }
     if (meta & kVor) {
       dg[kDVDil * S + g] = eps;
@@ -279,34 +365,61 @@ __global__ void __launch_bounds__(kWindow, kMinBlocks) rod_step_fp64_kernel(cons
   }
 }
 
+template <int W, int MinBlocks, bool kDiag, bool kDamped>
+__global__ void __launch_bounds__(W, MinBlocks) rod_step_fp64_kernel(const StepArgs a) {
+  extern __shared__ __align__(128) double smem[];
+  rod_step_window<W, kDiag, kDamped>(a, smem);
+}
+
+template <int W, int MinBlocks, bool kDiag, bool kDamped>
+cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
+  constexpr int kTile = W - 4;
+  constexpr size_t bytes = size_t(RowMap<kDamped, kDiag>::rows()) * W * sizeof(double) + 16;
+  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped>;
+  // the attribute is per device; setting it on every launch is cheap and
+  // keeps multi-device use correct
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e != cudaSuccess) return e;
+  const unsigned grid = static_cast<unsigned>((args.n_slots + kTile - 1) / kTile);
+  kern<<<grid, W, bytes, stream>>>(args);
+  return cudaGetLastError();
+}
+
+template <int W, int MinBlocks>
+cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
+  if (diag)
+    return damped ? launch_variant<W, MinBlocks, true, true>(args, stream)
+                  : launch_variant<W, MinBlocks, true, false>(args, stream);
+  return damped ? launch_variant<W, MinBlocks, false, true>(args, stream)
+                : launch_variant<W, MinBlocks, false, false>(args, stream);
+}
+
 }  // namespace
 
-// The same source is compiled twice.  The default object (built with
-// --fmad=false) rounds every product and sum separately, as the reference's
-// scalar C++ does without FMA contraction, and evaluates the damper as
-// written: it tracks the reference to transcendental-rounding level.  The
-// EB_FMA_FP64 object contracts multiply-adds into FMAs.
-#ifdef EB_FMA_FP64
-#define EB_FP64_LAUNCHER launch_rod_step_fp64_fma
-#else
+// The same source is compiled twice.  The default object (EB_FAST_FP64)
+// contracts multiply-adds into FMAs and uses the reformulations of
+// rod_math.cuh, the damper as exp(e y) and one reciprocal per repeated
+// divisor.  The reference-rounding object (built with --fmad=false) rounds
+// every product and sum separately, as the reference's scalar C++ does
+// without FMA contraction, and evaluates every expression as the reference
+// writes it.  Both stay within the same distance of the reference after many
+// steps (the rounding of any implementation is amplified alike); the second
+// matches the reference's short-horizon golden vectors at its own tolerance.
+#ifdef EB_FAST_FP64
 #define EB_FP64_LAUNCHER launch_rod_step_fp64
+#else
+#define EB_FP64_LAUNCHER launch_rod_step_fp64_reference
 #endif
 
-cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
+// window: slots per CTA (256 or 128; other values fall back to 256)
+cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream) {
   if (args.n_slots <= 0) return cudaSuccess;
-  const unsigned grid = static_cast<unsigned>((args.n_slots + kTile - 1) / kTile);
-  if (diag) {
-    if (damped)
-      rod_step_fp64_kernel<true, true><<<grid, kWindow, 0, stream>>>(args);
-    else
-      rod_step_fp64_kernel<true, false><<<grid, kWindow, 0, stream>>>(args);
-  } else {
-    if (damped)
-      rod_step_fp64_kernel<false, true><<<grid, kWindow, 0, stream>>>(args);
-    else
-      rod_step_fp64_kernel<false, false><<<grid, kWindow, 0, stream>>>(args);
-  }
-  return cudaGetLastError();
+  // every field row of a window must start on a 16-byte boundary
+  if ((args.stride & 1) || (reinterpret_cast<uintptr_t>(args.in) & 15) ||
+      (reinterpret_cast<uintptr_t>(args.par) & 15))
+    return cudaErrorMisalignedAddress;
+  if (window == 128) return launch_window<128, 4>(args, diag, damped, stream);
+  return launch_window<256, 2>(args, diag, damped, stream);
 }
 
 }  // namespace eb

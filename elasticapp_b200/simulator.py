@@ -188,12 +188,13 @@ class Simulator:
     """Owns one eb_sim (device memory and a CUDA stream)."""
 
     def __init__(self, device: int = 0, precision: str = "fp64", record_diagnostics: bool = False,
-                 fma: bool = False):
+                 reference_rounding: bool = False, window: int = 0):
         cfg = L.EbConfig()
         cfg.device = int(device)
         cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
         cfg.flags = (L.EB_FLAG_RECORD_DIAGNOSTICS if record_diagnostics else 0) | (
-            L.EB_FLAG_FMA_FP64 if fma else 0)
+            L.EB_FLAG_REFERENCE_ROUNDING if reference_rounding else 0)
+        cfg.step_window = int(window)
         h = ctypes.c_void_p()
         L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h

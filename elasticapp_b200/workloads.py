@@ -48,10 +48,10 @@ class Workload:
         return int(self.n_elements.sum())
 
     def build(self, device: int = 0, record_diagnostics: bool = False, precision: str = "fp64",
-              fma: bool = False) -> Simulator:
+              reference_rounding: bool = False, window: int = 0) -> Simulator:
         """Create the simulator through the reference-style plugin surface."""
         sim = Simulator(device=device, precision=precision, record_diagnostics=record_diagnostics,
-                        fma=fma)
+                        reference_rounding=reference_rounding, window=window)
         refs = sim.emplace_back_many(self.model, self.rods)
         if self.gravity is not None:
             sim.add_environment(GravityField(self.gravity))

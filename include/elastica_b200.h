@@ -60,19 +60,19 @@ typedef enum eb_precision {
 #define EB_FLAG_RECORD_DIAGNOSTICS 0x1u /* keep the derived per-element fields
                                            (strains, curvature, loads, ...) of
                                            the last step of every eb_step call */
-#define EB_FLAG_FMA_FP64 0x2u           /* FP64 step with fused multiply-add
-                                           contraction.  The default rounds
-                                           every product and sum separately,
-                                           as the reference's scalar C++
-                                           code; this variant differs from it
-                                           by the same amount as an FMA build
-                                           of the reference does */
+#define EB_FLAG_REFERENCE_ROUNDING 0x2u /* FP64 step that evaluates every
+                                           expression as the reference's
+                                           scalar C++ code does, without fused
+                                           multiply-adds.  The default build
+                                           contracts multiply-adds and uses
+                                           rounding-level reformulations
+                                           (reciprocals, small-angle series) */
 
 typedef struct eb_config {
-  int32_t device;    /* CUDA device ordinal */
-  int32_t precision; /* eb_precision */
-  uint32_t flags;    /* EB_FLAG_* */
-  int32_t reserved;
+  int32_t device;      /* CUDA device ordinal */
+  int32_t precision;   /* eb_precision */
+  uint32_t flags;      /* EB_FLAG_* */
+  int32_t step_window; /* slots per CTA of the step kernel: 0 (default, 128), 128 or 256 */
 } eb_config;
 
 /* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and

@@ -94,3 +94,34 @@ def max_rel_error_per_rod(got, want, n_elems, place):
         worst = max(worst, float(rel))
         o += n + 1
     return worst
+
+
+STATE_FIELDS = (("Position", "x", 0), ("Velocity", "v", 0), ("Director", "Q", 1), ("AngularVelocity", "w", 1))
+
+
+def oracle_spread(wl, n_steps, damped=False):
+    """Conditioning envelope of a workload: the largest per-rod normwise
+    relative change of each state field after n_steps when every initial
+    position, or every initial director entry, of the oracle is moved by one
+    ulp.  Returns (reference_run, {field: spread})."""
+    base = oracle_from_workload(wl, damped=damped)
+    base.step(wl.dt, n_steps)
+    spread = {name: 0.0 for name, _, _ in STATE_FIELDS}
+    for key in ("x", "Q"):
+        p = oracle_from_workload(wl, damped=damped)
+        p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
+        p.step(wl.dt, n_steps)
+        for name, k, place in STATE_FIELDS:
+            spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
+    return base, spread
+
+
+# Parity rule of the FP64 step: every state field within 1e-10 (per-rod
+# normwise relative error), or within 10x the one-ulp conditioning envelope
+# of the oracle itself where that envelope is wider.
+PARITY_FLOOR = 1e-10
+PARITY_ENVELOPE_FACTOR = 10.0
+
+
+def parity_bounds(spread):
+    return {k: max(PARITY_FLOOR, PARITY_ENVELOPE_FACTOR * v) for k, v in spread.items()}

@@ -12,18 +12,20 @@ import oracle_bridge as B
 
 pytestmark = pytest.mark.gpu
 
-# Tolerance of the FP64 drop-in against the oracle: normwise relative error
-# per rod and field after 1000 steps.
-REL_TOL_1000 = 1e-10
-# Tolerance of the FMA-contracting variant.  Contraction alone moves the
-# reference's own arithmetic this far: the oracle built with
-# -ffp-contract=fast differs from the oracle built without it by 2.3e-10 in
-# the angular velocity after 1000 steps of the same workload.
-REL_TOL_1000_FMA = 1e-9
+# Parity of the FP64 drop-in against the oracle after many steps: every
+# state field within 1e-10 per-rod normwise relative error, or within 10x the
+# oracle's own one-ulp conditioning envelope where that is wider
+# (oracle_bridge.parity_bounds).  Positions and directors always meet 1e-10;
+# velocities and angular velocities of stiff rods carry high-frequency
+# content that amplifies rounding (tests/test_conditioning.py).
 
 
-def golden_sim(case, damped, fma):
-    sim = eb.Simulator(record_diagnostics=True, fma=fma)
+def within(errs, bounds):
+    return all(errs[k] <= bounds[k] for k in errs)
+
+
+def golden_sim(case, damped, reference_rounding):
+    sim = eb.Simulator(record_diagnostics=True, reference_rounding=reference_rounding)
     s = G.ROD_SETUP
     init = eb.StraightRod(n_elements=s["n"], material=eb.Material(s["density"], s["youngs"], s["shear"]),
                           radius=s["radius"], length=s["length"], origin=s["origin"],
@@ -60,9 +62,9 @@ def compare_golden(refs, case, sec):
                          ids=lambda v: v if isinstance(v, str) else (
                              v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
 def test_golden_reference_rounding(name, case, sec, damped):
-    """Default FP64 kernel vs the reference's goldens at the reference's own
-    epsilon (Catch semantics)."""
-    sim, refs = golden_sim(case, damped, fma=False)
+    """Reference-rounding FP64 build vs the reference's goldens at the
+    reference's own epsilon (Catch semantics)."""
+    sim, refs = golden_sim(case, damped, reference_rounding=True)
     if sec["steps"]:
         sim.step(eb.PositionVerlet(), 0.0, G.ROD_SETUP["dt"], sec["steps"])
     worst = compare_golden(refs, case, sec)
@@ -73,12 +75,12 @@ def test_golden_reference_rounding(name, case, sec, damped):
 @pytest.mark.parametrize("name,case,sec,damped", list(G.step_cases()),
                          ids=lambda v: v if isinstance(v, str) else (
                              v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
-def test_golden_fma(name, case, sec, damped):
-    """FMA-contracting kernel vs the goldens.  Contraction changes rounding by
-    ~1 ulp per operation, so the bound is 4x the reference's epsilon (the
-    reference's own tolerances leave under 2% headroom for its non-FMA
-    arithmetic, see test_oracle_golden)."""
-    sim, refs = golden_sim(case, damped, fma=True)
+def test_golden_default(name, case, sec, damped):
+    """Default FP64 build (FMA contraction, rounding-level reformulations) vs
+    the goldens.  These change rounding by ~1 ulp per operation, so the bound
+    is 4x the reference's epsilon (the reference's own tolerances leave under
+    2% headroom for its non-FMA arithmetic, see test_oracle_golden)."""
+    sim, refs = golden_sim(case, damped, reference_rounding=False)
     if sec["steps"]:
         sim.step(eb.PositionVerlet(), 0.0, G.ROD_SETUP["dt"], sec["steps"])
     worst = compare_golden(refs, case, sec)
@@ -93,7 +95,7 @@ def test_state_injection_roundtrip_exact():
     for case in doc["cases"]:
         if case["name"].split(".")[-1] not in ("WithDynamicAndExternal", "FullWithDirector"):
             continue
-        sim, refs = golden_sim(case, damped=True, fma=False)
+        sim, refs = golden_sim(case, damped=True, reference_rounding=False)
         kinds = {**G.STATE_FIELDS, **G.PARAM_FIELDS, **G.DIAG_FIELDS}
         n_checked = 0
         for r in range(case["n_rods"]):
@@ -109,17 +111,20 @@ def test_state_injection_roundtrip_exact():
         sim.close()
 
 
-def _run_pair(wl, n_steps, fma=False, damped=False):
-    sim = wl.build(record_diagnostics=False, fma=fma)
-    orc = B.oracle_from_workload(wl, damped=damped)
+def _run_pair(wl, n_steps, reference_rounding=False, damped=False, window=0):
+    """Run the workload on the GPU and in the oracle; return the simulator,
+    the oracle run, the per-field errors and the parity bounds."""
+    sim = wl.build(record_diagnostics=False, reference_rounding=reference_rounding, window=window)
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, n_steps)
-    orc.step(wl.dt, n_steps)
+    orc, spread = B.oracle_spread(wl, n_steps, damped=damped)
     want = B.state_slots(orc)
     errs = {}
     for name, place in (("Position", 0), ("Velocity", 0), ("Director", 1), ("AngularVelocity", 1)):
         got = sim.get_slots(name)
         errs[name] = B.max_rel_error_per_rod(got, want[name], wl.n_elements, place)
-    return sim, orc, errs
+    bounds = B.parity_bounds(spread)
+    assert errs["Position"] <= B.PARITY_FLOOR and errs["Director"] <= B.PARITY_FLOOR, errs
+    return sim, orc, errs, bounds
 
 
 def small_uneven(n_rods=48, seed=7, n_range=(2, 40)):
@@ -127,25 +132,27 @@ def small_uneven(n_rods=48, seed=7, n_range=(2, 40)):
     return wl
 
 
-def test_uneven_batch_1000_steps_vs_oracle():
+@pytest.mark.parametrize("window", [0, 256])
+def test_uneven_batch_1000_steps_vs_oracle(window):
     """Clamped rods of uneven length with gravity and the analytical damper:
-    the FP64 drop-in matches the oracle to <= 1e-10 after 1000 steps."""
+    the FP64 drop-in matches the oracle after 1000 steps."""
     wl = small_uneven()
-    sim, orc, errs = _run_pair(wl, 1000)
-    assert max(errs.values()) <= REL_TOL_1000, errs
+    sim, orc, errs, bounds = _run_pair(wl, 1000, window=window)
+    assert within(errs, bounds), (errs, bounds)
     assert sim.launch_count() >= 1000
 
 
-def test_fma_kernel_vs_oracle():
+@pytest.mark.parametrize("window", [0, 256])
+def test_reference_rounding_build_vs_oracle(window):
     wl = small_uneven(n_rods=16, seed=11)
-    _, _, errs = _run_pair(wl, 1000, fma=True)
-    assert max(errs.values()) <= REL_TOL_1000_FMA, errs
+    _, _, errs, bounds = _run_pair(wl, 1000, reference_rounding=True, window=window)
+    assert within(errs, bounds), (errs, bounds)
 
 
 def test_rest_curvature_end_torque_vs_oracle():
     wl = W.mixed_batch(n_rods=24, seed=5, n_range=(3, 60), n_steps=500, dt=2e-6)
-    _, _, errs = _run_pair(wl, 500)
-    assert max(errs.values()) <= REL_TOL_1000, errs
+    _, _, errs, bounds = _run_pair(wl, 500)
+    assert within(errs, bounds), (errs, bounds)
 
 
 def test_explicitly_damped_rods_vs_oracle():
@@ -155,8 +162,8 @@ def test_explicitly_damped_rods_vs_oracle():
         r.force_damping_rate = 0.3
         r.torque_damping_rate = 0.2
     wl.damper = None
-    _, _, errs = _run_pair(wl, 1000, damped=True)
-    assert max(errs.values()) <= REL_TOL_1000, errs
+    _, _, errs, bounds = _run_pair(wl, 1000, damped=True)
+    assert within(errs, bounds), (errs, bounds)
 
 
 @pytest.mark.parametrize("lengths", [[1000], [255, 1, 300], [2, 2, 2, 2, 2], [254], [255], [256], [600, 2, 511]])
@@ -177,13 +184,15 @@ def test_tile_and_rod_boundaries(lengths):
                                    direction=tuple(d), normal=tuple(c)))
     wl = W.Workload("boundaries", 0, rods, velocities=[rng.normal(0, 1e-2, (3, n + 1)) for n in lengths],
                     dt=2e-6, n_steps=200)
-    _, _, errs = _run_pair(wl, 200)
-    assert max(errs.values()) <= REL_TOL_1000, errs
+    _, _, errs, bounds = _run_pair(wl, 200)
+    assert within(errs, bounds), (errs, bounds)
+    _, _, errs, bounds = _run_pair(wl, 200, reference_rounding=True, window=256)
+    assert within(errs, bounds), (errs, bounds)
 
 
 def test_energy_matches_oracle():
     wl = small_uneven(n_rods=12, seed=2)
-    sim, orc, _ = _run_pair(wl, 50)
+    sim, orc, _, _ = _run_pair(wl, 50)
     e_gpu = sim.energy()
     e_cpu = orc.energy()
     np.testing.assert_allclose(e_gpu, e_cpu, rtol=1e-9, atol=1e-300)
@@ -233,3 +242,24 @@ def test_error_paths():
     with pytest.raises(L.EbError) as e:
         L.call("eb_get_field", sim._h, 99, 0, np.zeros(3).ctypes.data_as(L.ctypes.POINTER(L.ctypes.c_double)), 3)
     assert e.value.status == 6  # EB_ERR_NOT_FOUND
+
+
+def test_full_size_uneven_batch_sampled_parity():
+    """The full uneven batch (16,384 rods, ~4.4 M elements) for 1000 steps on
+    the GPU; rods are independent, so the oracle checks a seeded sample of 48
+    of them run on their own."""
+    wl = W.uneven_batch()
+    sim = wl.build()
+    sim.step(eb.PositionVerlet(), 0.0, wl.dt, 1000)
+    rng = np.random.default_rng(2024)
+    pick = np.sort(rng.choice(len(wl.rods), size=48, replace=False))
+    sub = W.Workload(wl.name, wl.seed, [wl.rods[k] for k in pick],
+                     velocities=[wl.velocities[k] for k in pick], dt=wl.dt, n_steps=1000)
+    orc, spread = B.oracle_spread(sub, 1000)
+    bounds = B.parity_bounds(spread)
+    offs = sim.slot_offsets()
+    for name, key, place in B.STATE_FIELDS:
+        full = sim.get_slots(name)
+        got = np.concatenate([full[:, offs[k]:offs[k + 1]] for k in pick], axis=1)
+        err = B.max_rel_error_per_rod(got, orc.comp(key), sub.n_elements, place)
+        assert err <= bounds[name], (name, err, bounds[name])
