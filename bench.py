@@ -214,6 +214,10 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="uneven_batch")
     ap.add_argument("--rods", type=int, default=None, help="smaller batch (profiling captures only)")
     ap.add_argument("--e2e-cycles", type=int, default=3)
+    ap.add_argument("--batched-steps", type=int, default=256,
+                    help="steps timed on the resident (batched) kernel; 0 skips it")
+    ap.add_argument("--resident-config", type=int, default=0,
+                    help="resident configuration (1-based; 0 = chosen by timing)")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-rounding", action="store_true",
@@ -251,7 +255,8 @@ def main(argv=None) -> int:
     import elasticapp_b200 as eb
 
     wl = wl_fn(rank)
-    sim = wl.build(device=local, reference_rounding=args.reference_rounding, window=args.window)
+    sim = wl.build(device=local, reference_rounding=args.reference_rounding, window=args.window,
+                   step_mode="streaming")
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
     t = 0.0
     t = sim.step(eb.PositionVerlet(), t, wl.dt, args.warmup)
@@ -326,6 +331,35 @@ def main(argv=None) -> int:
                  if args.e2e_cycles > 0 else None)
     finite = all(np.isfinite(host[n]).all() for n in names)
 
+    # ---- the resident (batched) form of the same step on the same workload
+    batched = None
+    if args.batched_steps > 0:
+        sim.close()
+        bsim = wl.build(device=local, step_mode="resident", resident_config=args.resident_config)
+        tb = bsim.step(eb.PositionVerlet(), 0.0, wl.dt, 128)  # plan + warm-up
+        bsim.synchronize()
+        bstream = torch.cuda.ExternalStream(bsim.stream_handle(), device=torch.device("cuda", local))
+        barrier()
+        torch.cuda.synchronize()
+        l0 = bsim.launch_count()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(bstream)
+        tb = bsim.step(eb.PositionVerlet(), tb, wl.dt, args.batched_steps)
+        b1.record(bstream)
+        torch.cuda.synchronize()
+        barrier()
+        bms = torch.tensor([b0.elapsed_time(b1)], device="cuda")
+        if pg is not None:
+            pg.all_reduce(bms, op=pg.ReduceOp.MAX)
+        plan = bsim.step_plan()
+        batched = {"value": total_elems * args.batched_steps / (float(bms.item()) / 1e3), "unit": UNIT,
+                   "steps": args.batched_steps, "ms_per_step": float(bms.item()) / args.batched_steps,
+                   "launches": bsim.launch_count() - l0, "plan": plan,
+                   "kernel": "rod_block_fp64 (whole rods resident in shared memory, up to 128 steps per launch)"}
+        bsim.close()
+        sim = None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, sample = cpu_reference_rate(wl, 0, budget_s=args.cpu_budget_s, max_rods=2048)
@@ -354,9 +388,11 @@ def main(argv=None) -> int:
             "gpu_launches": launches,
             "clocks": clock_info,
             "state_finite": bool(finite),
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
+    if sim is not None:
+        sim.close()
     return 0
 
 

@@ -21,6 +21,8 @@ EB_PRECISION_FP64 = 0
 EB_PRECISION_MIXED = 1
 EB_FLAG_RECORD_DIAGNOSTICS = 0x1
 EB_FLAG_REFERENCE_ROUNDING = 0x2
+EB_FLAG_STEP_STREAMING = 0x4
+EB_FLAG_STEP_RESIDENT = 0x8
 EB_ROD_DAMPED = 0
 EB_ROD_UNDAMPED = 1
 EB_LAYOUT_PER_ROD = 0
@@ -55,7 +57,8 @@ DERIVED_FIELDS = set(FIELDS[16:])
 
 class EbConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("flags", ctypes.c_uint32), ("step_window", ctypes.c_int32)]
+                ("flags", ctypes.c_uint32), ("step_window", ctypes.c_int32),
+                ("resident_config", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class EbStraightRod(ctypes.Structure):
@@ -94,6 +97,7 @@ SIGNATURES = {
     "eb_synchronize": ([_sim], ctypes.c_int),
     "eb_energy": ([_sim, _P(ctypes.c_double), ctypes.c_int64], ctypes.c_int),
     "eb_get_stream": ([_sim, _P(ctypes.c_void_p)], ctypes.c_int),
+    "eb_step_plan": ([_sim, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_float), ctypes.c_int32], ctypes.c_int),
     "eb_launch_count": ([_sim, _P(ctypes.c_int64)], ctypes.c_int),
 }
 

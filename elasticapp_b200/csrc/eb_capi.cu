@@ -23,6 +23,10 @@ namespace eb {
 cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream);
 cudaError_t launch_rod_step_fp64_reference(const StepArgs& args, bool diag, bool damped, int window,
                                            cudaStream_t stream);
+int block_config_count();
+int block_config_capacity(int config);
+cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
+                                  int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -122,6 +126,13 @@ struct eb_sim {
   int cur = 0;
   double damper_dt = -1.0;
   int64_t launches = 0;
+  // step plan: streaming kernel (one launch per step) or the resident kernel
+  // with one of the block configurations, chosen by timing both
+  int plan_mode = 0;    // 0 undecided, 1 streaming, 2 resident
+  int plan_config = -1;
+  std::vector<int64_t*> d_cta_start;  // per block configuration (or null)
+  std::vector<int> n_ctas;
+  float plan_ms[16] = {0};
 };
 
 namespace {
@@ -278,6 +289,9 @@ void host_free(eb_sim* s) {
   if (s->d_energy) cudaFree(s->d_energy);
   if (s->d_status) cudaFree(s->d_status);
   s->d_status = nullptr;
+  for (auto* p : s->d_cta_start)
+    if (p) cudaFree(p);
+  s->d_cta_start.clear();
   s->d_state[0] = s->d_state[1] = s->d_param = s->d_diag = s->d_energy = nullptr;
   s->d_meta = nullptr;
   s->d_rods = nullptr;
@@ -318,6 +332,8 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
   if (config) cfg = *config;
   if (cfg.precision != EB_PRECISION_FP64 && cfg.precision != EB_PRECISION_MIXED)
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (cfg.resident_config < 0 || cfg.resident_config > eb::block_config_count())
+    return fail(EB_ERR_INVALID_ARGUMENT, "resident_config out of range");
   if (cfg.step_window != 0 && cfg.step_window != 128 && cfg.step_window != 256)
     return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
   if (cfg.precision == EB_PRECISION_MIXED)
@@ -657,6 +673,135 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   return EB_OK;
 }
 
+namespace {
+
+constexpr int kResidentChunk = 128;  // steps per launch of the resident kernel
+constexpr int kProbeSteps = 8;       // steps per timing probe of the planner
+
+eb::StepArgs step_args(eb_sim* s, double dt) {
+  eb::StepArgs a{};
+  a.stride = s->stride;
+  a.n_slots = s->n_slots;
+  a.par = s->d_param;
+  a.meta = s->d_meta;
+  a.rods = s->d_rods;
+  a.dt = dt;
+  a.half_dt = 0.5 * dt;
+  for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
+  a.sim_flags = s->sim_flags;
+  a.status = s->d_status;
+  return a;
+}
+
+cudaError_t launch_streaming(eb_sim* s, eb::StepArgs& a, bool rec) {
+  a.diag = rec ? s->d_diag : nullptr;
+  const int window = s->cfg.step_window ? s->cfg.step_window : 128;
+  if (s->cfg.flags & EB_FLAG_REFERENCE_ROUNDING)
+    return eb::launch_rod_step_fp64_reference(a, rec, s->any_damped, window, s->stream);
+  return eb::launch_rod_step_fp64(a, rec, s->any_damped, window, s->stream);
+}
+
+// Pack the rods, in slot order, into CTAs of at most `cap` slots (next fit).
+// Returns false when a rod is longer than the capacity.
+bool pack_rods(const eb_sim* s, int cap, std::vector<int64_t>& starts) {
+  starts.clear();
+  starts.push_back(0);
+  int64_t used = 0;
+  for (size_t r = 0; r < s->rods.size(); ++r) {
+    const int64_t w = s->rods[r].n + 1;
+    if (w > cap) return false;
+    if (used + w > cap) {
+      starts.push_back(s->offsets[r]);
+      used = 0;
+    }
+    used += w;
+  }
+  starts.push_back(s->n_slots);
+  return true;
+}
+
+eb_status build_block_worklists(eb_sim* s) {
+  if (!s->d_cta_start.empty()) return EB_OK;
+  s->d_cta_start.assign(static_cast<size_t>(eb::block_config_count()), nullptr);
+  s->n_ctas.assign(static_cast<size_t>(eb::block_config_count()), 0);
+  std::vector<int64_t> starts;
+  for (int c = 0; c < eb::block_config_count(); ++c) {
+    if (!pack_rods(s, eb::block_config_capacity(c), starts)) continue;
+    EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&s->d_cta_start[c]), starts.size() * sizeof(int64_t)));
+    EB_CUDA(cudaMemcpyAsync(s->d_cta_start[c], starts.data(), starts.size() * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, s->stream));
+    s->n_ctas[c] = static_cast<int>(starts.size() - 1);
+  }
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+// Choose between the streaming kernel and the resident configurations by
+// timing each for kProbeSteps steps from the current state into the spare
+// buffer (the current state is left untouched).
+eb_status plan_steps(eb_sim* s, double dt) {
+  const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0;
+  if (force_stream) {
+    s->plan_mode = 1;
+    return EB_OK;
+  }
+  if (eb_status st = build_block_worklists(s)) return st;
+  const int want = s->cfg.resident_config - 1;
+  if (want >= 0) {
+    if (s->d_cta_start[want]) {
+      s->plan_mode = 2;
+      s->plan_config = want;
+    } else {
+      s->plan_mode = 1;  // the rods do not fit this configuration
+    }
+    return EB_OK;
+  }
+  cudaEvent_t e0, e1;
+  EB_CUDA(cudaEventCreate(&e0));
+  EB_CUDA(cudaEventCreate(&e1));
+  eb::StepArgs a = step_args(s, dt);
+  a.in = s->d_state[s->cur];
+  a.out = s->d_state[s->cur ^ 1];
+  float best = 0.0f;
+  int best_mode = 1, best_cfg = -1;
+  const bool force_resident = (s->cfg.flags & EB_FLAG_STEP_RESIDENT) != 0;
+  for (int c = -1; c < eb::block_config_count(); ++c) {
+    if (c >= 0 && !s->d_cta_start[c]) continue;
+    if (c < 0 && force_resident) continue;
+    for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
+      EB_CUDA(cudaEventRecord(e0, s->stream));
+      if (c < 0) {
+        for (int k = 0; k < kProbeSteps; ++k) EB_CUDA(launch_streaming(s, a, false));
+      } else {
+        EB_CUDA(eb::launch_rod_block_fp64(a, s->d_cta_start[c], s->n_ctas[c], kProbeSteps, c, s->any_damped,
+                                          s->stream));
+      }
+      EB_CUDA(cudaEventRecord(e1, s->stream));
+      EB_CUDA(cudaEventSynchronize(e1));
+    }
+    float ms = 0.0f;
+    EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    s->plan_ms[c + 1] = ms;
+    if (best_cfg == -1 && best_mode == 1 && best == 0.0f) {
+      best = ms;
+      best_mode = c < 0 ? 1 : 2;
+      best_cfg = c;
+    } else if (ms < best) {
+      best = ms;
+      best_mode = c < 0 ? 1 : 2;
+      best_cfg = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_mode == 2 && best_cfg < 0) best_mode = 1;
+  s->plan_mode = best_mode;
+  s->plan_config = best_cfg;
+  return check_device_status(s);
+}
+
+}  // namespace
+
 EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
   if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "finalize before stepping");
@@ -672,36 +817,49 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     if (eb_status st = upload_rod_table(s)) return st;
     s->damper_dt = dt;
   }
-  eb::StepArgs a{};
-  a.stride = s->stride;
-  a.n_slots = s->n_slots;
-  a.par = s->d_param;
-  a.meta = s->d_meta;
-  a.rods = s->d_rods;
-  a.dt = dt;
-  a.half_dt = 0.5 * dt;
-  for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
-  a.sim_flags = s->sim_flags;
-  a.status = s->d_status;
+  if (s->plan_mode == 0)
+    if (eb_status st = plan_steps(s, dt)) return st;
+  eb::StepArgs a = step_args(s, dt);
   const bool diag = s->d_diag != nullptr;
-  for (int64_t k = 0; k < n_steps; ++k) {
+  int64_t done = 0;
+  if (s->plan_mode == 2) {
+    // resident kernel in chunks; the last step of a call that records
+    // diagnostics runs on the streaming kernel, which writes them
+    const int64_t resident_steps = diag ? n_steps - 1 : n_steps;
+    const int c = s->plan_config;
+    while (done < resident_steps) {
+      const int k = static_cast<int>(std::min<int64_t>(kResidentChunk, resident_steps - done));
+      a.in = s->d_state[s->cur];
+      a.out = s->d_state[s->cur ^ 1];
+      EB_CUDA(eb::launch_rod_block_fp64(a, s->d_cta_start[c], s->n_ctas[c], k, c, s->any_damped, s->stream));
+      s->cur ^= 1;
+      ++s->launches;
+      done += k;
+    }
+  }
+  for (; done < n_steps; ++done) {
     a.in = s->d_state[s->cur];
     a.out = s->d_state[s->cur ^ 1];
-    const bool rec = diag && (k == n_steps - 1);
-    a.diag = rec ? s->d_diag : nullptr;
-    const int window = s->cfg.step_window ? s->cfg.step_window : 128;
-    if (s->cfg.flags & EB_FLAG_REFERENCE_ROUNDING)
-      EB_CUDA(eb::launch_rod_step_fp64_reference(a, rec, s->any_damped, window, s->stream));
-    else
-      EB_CUDA(eb::launch_rod_step_fp64(a, rec, s->any_damped, window, s->stream));
+    EB_CUDA(launch_streaming(s, a, diag && done == n_steps - 1));
     s->cur ^= 1;
     ++s->launches;
-    if (time) {
+  }
+  if (time) {
+    for (int64_t k = 0; k < n_steps; ++k) {
       // two TimeUpdate substeps of dt/2 (PositionVerlet.hpp:52-58)
       *time += 0.5 * dt;
       *time += 0.5 * dt;
     }
   }
+  return EB_OK;
+}
+
+EB_API eb_status eb_step_plan(const eb_sim* s, int32_t* mode, int32_t* config, float* probe_ms, int32_t count) {
+  if (check_sim(s) || !mode || !config) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  *mode = s->plan_mode;
+  *config = s->plan_config;
+  if (probe_ms)
+    for (int i = 0; i < count && i < 16; ++i) probe_ms[i] = s->plan_ms[i];
   return EB_OK;
 }
 

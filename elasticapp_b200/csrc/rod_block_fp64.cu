@@ -1,0 +1,343 @@
+// Resident multi-step PositionVerlet kernel for batches of whole rods.
+//
+// The streaming step kernel (rod_step_fp64.cu) moves the full state through
+// HBM every step.  Rods are independent, so a CTA can instead own a group of
+// whole rods, stage their state and parameters into shared memory once, run
+// many steps entirely on chip and write the state back once: HBM traffic per
+// element-step falls by the number of steps per launch and the step becomes
+// arithmetic-bound.
+//
+// Work list: CTA c owns the consecutive slots [cta_start[c], cta_start[c+1]),
+// always a whole number of rods (the host packs rods into CTAs of at most
+// kCap slots).  Every phase loops its threads over the CTA's slots; all
+// per-slot data lives in shared-memory rows, so any thread count works.
+//
+// Step structure: the same substeps as the streaming kernel, including both
+// half drifts of every step.  (Merging the second half drift of step k with
+// the first of step k+1 into one full drift is not an identity here: the
+// reference normalises the rotation axis by theta + 1e-14, so one update by
+// dt differs from two by dt/2 by ~1e-14 per step, which the stiff rod modes
+// amplify into angular-velocity differences far above rounding.  The kernel
+// keeps a compile-time switch for it, unused by the configurations below.)
+#include <cuda_runtime.h>
+
+#include "eb_internal.h"
+#include "rod_math.cuh"
+
+namespace eb {
+namespace {
+
+using D3 = Vec3<double>;
+
+// shared-memory rows (each kCap doubles)
+enum BlockRow : int {
+  bX = 0, bV = 3, bQ = 6, bW = 15,  // state (kStateFields rows)
+  bMass = 18, bL0 = 19, bD0 = 20, bSig0 = 21, bKap0 = 24, bShear = 27, bBend = 30, bJ = 33, bJinv = 36,
+  bNuF = 39, bNuT = 40,             // explicit damping only
+  bL = 41, bE = 42, bF = 43, bG = 46, bH = 49, bTl = 52,  // per-step exchange rows
+  bRows = 55
+};
+
+template <int kCap>
+struct BRows {
+  double* base;
+  __device__ __forceinline__ double& at(int r, int s) const { return base[r * kCap + s]; }
+  __device__ __forceinline__ D3 get3(int r, int s) const {
+    return {base[r * kCap + s], base[(r + 1) * kCap + s], base[(r + 2) * kCap + s]};
+  }
+  __device__ __forceinline__ void put3(int r, int s, D3 v) const {
+    base[r * kCap + s] = v.x;
+    base[(r + 1) * kCap + s] = v.y;
+    base[(r + 2) * kCap + s] = v.z;
+  }
+};
+
+// parameter field -> shared row (the rows the resident kernel keeps)
+__device__ __forceinline__ int param_row(int f) {
+  switch (f) {
+    case kMass: return bMass;
+    case kL0: return bL0;
+    case kD0: return bD0;
+    case kNuF: return bNuF;
+    case kNuT: return bNuT;
+    default: break;
+  }
+  if (f >= kSig0 && f < kSig0 + 3) return bSig0 + (f - kSig0);
+  if (f >= kKap0 && f < kKap0 + 3) return bKap0 + (f - kKap0);
+  if (f >= kShear && f < kShear + 3) return bShear + (f - kShear);
+  if (f >= kBend && f < kBend + 3) return bBend + (f - kBend);
+  if (f >= kJ && f < kJ + 3) return bJ + (f - kJ);
+  if (f >= kJinv && f < kJinv + 3) return bJinv + (f - kJinv);
+  return -1;  // volume: only read for diagnostics, straight from global memory
+}
+
+template <int kCap, int kThreads, bool kDamped, bool kSplit>
+__global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
+                                                                    int n_steps) {
+  extern __shared__ __align__(128) double smem[];
+  const BRows<kCap> R{smem};
+  uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + bRows * kCap);
+
+  const int tid = threadIdx.x;
+  const int64_t g0 = cta_start[blockIdx.x];
+  const int count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
+  const int64_t S = a.stride;
+
+  // ---- stage state, parameters and slot metadata (coalesced loads)
+  for (int s = tid; s < count; s += kThreads) {
+    const int64_t g = g0 + s;
+    meta_s[s] = a.meta[g];
+#pragma unroll 1
+    for (int f = 0; f < kStateFields; ++f) R.at(f, s) = a.in[f * S + g];
+#pragma unroll 1
+    for (int f = 0; f < kParamFields; ++f) {
+      const int r = param_row(f);
+      if (r < 0 || (!kDamped && (f == kNuF || f == kNuT))) continue;
+      R.at(r, s) = a.par[f * S + g];
+    }
+  }
+  __syncthreads();
+
+  const double dt = a.dt, hdt = a.half_dt;
+  const bool any_rod = (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
+
+  for (int step = 0; step < n_steps; ++step) {
+    // ---- drift: half on the first step; afterwards the merged full drift,
+    // or (kSplit) the first half drift, the second half of the previous step
+    // having been applied at the end of its update phase
+    const double c = (step == 0 || kSplit) ? hdt : dt;
+    for (int s = tid; s < count; s += kThreads) {
+      const uint32_t meta = meta_s[s];
+      const D3 v = R.get3(bV, s);
+      D3 x = R.get3(bX, s);
+      x = {x.x + c * v.x, x.y + c * v.y, x.z + c * v.z};
+      double q[9];
+      if (meta & kElem) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+        const D3 w = R.get3(bW, s);
+        so3_update_fast(q, c * w.x, c * w.y, c * w.z);
+      }
+      if (any_rod && (meta & kFirst)) {
+        const RodInfo& ri = a.rods[meta >> kRodShift];
+        if (ri.flags & kRodClamp) {
+          x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+#pragma unroll
+          for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
+        }
+      }
+      R.put3(bX, s, x);
+      if (meta & kElem) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
+      }
+    }
+    __syncthreads();
+
+    // ---- element geometry, internal stress, element-local torque terms
+    for (int s = tid; s < count; s += kThreads) {
+      const uint32_t meta = meta_s[s];
+      D3 f{0.0, 0.0, 0.0}, tl{0.0, 0.0, 0.0};
+      double l = 1.0, e = 1.0;
+      if (meta & kElem) {
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+        const D3 dx = R.get3(bX, s + 1) - R.get3(bX, s);
+        l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
+        const double il = 1.0 / l;
+        const D3 t = {dx.x * il, dx.y * il, dx.z * il};
+        const double l0 = R.at(bL0, s);
+        e = l / l0;
+        const D3 qt = matvec(q, t);
+        const D3 sigma = {qt.x * e, qt.y * e, qt.z * e - 1.0};
+        const D3 d = sigma - R.get3(bSig0, s);
+        const D3 sh = R.get3(bShear, s);
+        const D3 nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
+        const double ie = 1.0 / e;
+        f = scale(mattranspvec(q, nl), ie);
+        const D3 w = R.get3(bW, s);
+        const D3 J = R.get3(bJ, s);
+        const D3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
+        const D3 dv = R.get3(bV, s + 1) - R.get3(bV, s);
+        const double rate = dot(t, dv) / (e * l0);
+        tl = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
+      }
+      R.at(bL, s) = l;
+      R.at(bE, s) = e;
+      R.put3(bF, s, f);
+      R.put3(bTl, s, tl);
+    }
+    __syncthreads();
+
+    // ---- Voronoi curvature and couple
+    for (int s = tid; s < count; s += kThreads) {
+      const uint32_t meta = meta_s[s];
+      D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
+      if (meta & kVor) {
+        double qc[9], qn[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          qc[k] = R.at(bQ + k, s);
+          qn[k] = R.at(bQ + k, s + 1);
+        }
+        const double D0 = R.at(bD0, s);
+        const D3 kappa = inv_rotate_divide_fast(qc, qn, D0);
+        const double eps = 0.5 * (R.at(bL, s) + R.at(bL, s + 1)) / D0;
+        const double ic = 1.0 / (eps * eps * eps);
+        const D3 dk = kappa - R.get3(bKap0, s);
+        const D3 B = R.get3(bBend, s);
+        const D3 tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
+        gg = scale(tau, ic);
+        hh = scale(cross(kappa, tau), ic * D0);
+      }
+      R.put3(bG, s, gg);
+      R.put3(bH, s, hh);
+    }
+    __syncthreads();
+
+    // ---- loads, torques, accelerations, kick, rate constraints
+    for (int s = tid; s < count; s += kThreads) {
+      const uint32_t meta = meta_s[s];
+      const bool first = (meta & kFirst) != 0;
+      const double m = R.at(bMass, s);
+      D3 v = R.get3(bV, s);
+      D3 F = R.get3(bF, s);
+      if (!first) F = F - R.get3(bF, s - 1);
+      if (kDamped) {
+        const double cf = m * R.at(bNuF, s);
+        F = {F.x - cf * v.x, F.y - cf * v.y, F.z - cf * v.z};
+      }
+      if (a.sim_flags & kSimGravity) F = F + D3{a.gravity[0] * m, a.gravity[1] * m, a.gravity[2] * m};
+      const double im = 1.0 / m;
+      v = {v.x + dt * (F.x * im), v.y + dt * (F.y * im), v.z + dt * (F.z * im)};
+      D3 w{0.0, 0.0, 0.0};
+      const RodInfo* ri = any_rod ? a.rods + (meta >> kRodShift) : nullptr;
+      if (meta & kElem) {
+        const double e = R.at(bE, s);
+        w = R.get3(bW, s);
+        D3 T = R.get3(bG, s);
+        D3 Q2 = R.get3(bH, s);
+        if (!first) {
+          T = T - R.get3(bG, s - 1);
+          Q2 = Q2 + R.get3(bH, s - 1);
+        }
+        T = T + scale(Q2, 0.5) + R.get3(bTl, s);
+        if (kDamped) {
+          const double ct = 0.5 * (m + R.at(bMass, s + 1)) * R.at(bNuT, s);
+          T = {T.x - ct * w.x, T.y - ct * w.y, T.z - ct * w.z};
+        }
+        if (any_rod && (meta & kLastElem) && (ri->flags & kRodEndTorque)) {
+          double q[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+          T = T + matvec(q, D3{ri->end_torque[0], ri->end_torque[1], ri->end_torque[2]});
+        }
+        const D3 ji = R.get3(bJinv, s);
+        w = {w.x + dt * (ji.x * T.x * e), w.y + dt * (ji.y * T.y * e), w.z + dt * (ji.z * T.z * e)};
+        if (any_rod && (ri->flags & kRodDamper)) {
+          const double mn = R.at(bMass, s + 1);
+          double em = 0.5 * (m + mn);
+          if (first) em += 0.5 * m;
+          if (meta & kLastElem) em += 0.5 * mn;
+          const double y = -ri->damper_r * em * dt * e;
+          w = {w.x * exp(y * ji.x), w.y * exp(y * ji.y), w.z * exp(y * ji.z)};
+        }
+      }
+      if (any_rod) {
+        if (first && (ri->flags & kRodClamp)) {
+          v = D3{0.0, 0.0, 0.0};
+          w = D3{0.0, 0.0, 0.0};
+        }
+        if (ri->flags & kRodDamper) v = scale(v, ri->damper_t);
+      }
+      R.put3(bV, s, v);
+      if (meta & kElem) R.put3(bW, s, w);
+      if (kSplit && step + 1 < n_steps) {
+        // second half drift of this step, own slot only
+        D3 x = R.get3(bX, s);
+        R.put3(bX, s, D3{x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z});
+        if (meta & kElem) {
+          double q[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+          so3_update_fast(q, hdt * w.x, hdt * w.y, hdt * w.z);
+#pragma unroll
+          for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- final half drift and write-back
+  for (int s = tid; s < count; s += kThreads) {
+    const uint32_t meta = meta_s[s];
+    const int64_t g = g0 + s;
+    const D3 v = R.get3(bV, s);
+    D3 x = R.get3(bX, s);
+    x = {x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z};
+    a.out[kStX * S + g] = x.x;
+    a.out[(kStX + 1) * S + g] = x.y;
+    a.out[(kStX + 2) * S + g] = x.z;
+    a.out[kStV * S + g] = v.x;
+    a.out[(kStV + 1) * S + g] = v.y;
+    a.out[(kStV + 2) * S + g] = v.z;
+    if (meta & kElem) {
+      double q[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+      const D3 w = R.get3(bW, s);
+      so3_update_fast(q, hdt * w.x, hdt * w.y, hdt * w.z);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a.out[(kStQ + k) * S + g] = q[k];
+      a.out[kStW * S + g] = w.x;
+      a.out[(kStW + 1) * S + g] = w.y;
+      a.out[(kStW + 2) * S + g] = w.z;
+    }
+  }
+}
+
+template <int kCap, int kThreads, bool kSplit>
+cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
+                             cudaStream_t stream) {
+  const size_t bytes = size_t(bRows) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
+  auto go = [&](auto kern) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e != cudaSuccess) return e;
+    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps);
+    return cudaGetLastError();
+  };
+  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit>)
+                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit>);
+}
+
+}  // namespace
+
+// Configurations offered to the autotuner.  The capacity bounds the longest
+// rod a configuration can hold (n + 1 slots).
+namespace {
+// {slots per CTA, threads per CTA}
+constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {256, 256}, {256, 128}};
+constexpr int kNumConfigs = 4;
+}  // namespace
+
+int block_config_count() { return kNumConfigs; }
+
+int block_config_capacity(int config) {
+  return (config >= 0 && config < kNumConfigs) ? kBlockConfigs[config][0] : 0;
+}
+
+cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
+                                  int config, bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  switch (config) {
+    case 0: return launch_block_cfg<520, 512, true>(args, cta_start, n_ctas, n_steps, damped, stream);
+    case 1: return launch_block_cfg<520, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
+    case 2: return launch_block_cfg<256, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
+    case 3: return launch_block_cfg<256, 128, true>(args, cta_start, n_ctas, n_steps, damped, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace eb

@@ -188,13 +188,16 @@ class Simulator:
     """Owns one eb_sim (device memory and a CUDA stream)."""
 
     def __init__(self, device: int = 0, precision: str = "fp64", record_diagnostics: bool = False,
-                 reference_rounding: bool = False, window: int = 0):
+                 reference_rounding: bool = False, window: int = 0, step_mode: str = "auto",
+                 resident_config: int = 0):
         cfg = L.EbConfig()
         cfg.device = int(device)
         cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
         cfg.flags = (L.EB_FLAG_RECORD_DIAGNOSTICS if record_diagnostics else 0) | (
-            L.EB_FLAG_REFERENCE_ROUNDING if reference_rounding else 0)
+            L.EB_FLAG_REFERENCE_ROUNDING if reference_rounding else 0) | {
+            "auto": 0, "streaming": L.EB_FLAG_STEP_STREAMING, "resident": L.EB_FLAG_STEP_RESIDENT}[step_mode]
         cfg.step_window = int(window)
+        cfg.resident_config = int(resident_config)
         h = ctypes.c_void_p()
         L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h
@@ -284,6 +287,14 @@ class Simulator:
         h = ctypes.c_void_p()
         L.call("eb_get_stream", self._h, ctypes.byref(h))
         return int(h.value or 0)
+
+    def step_plan(self) -> dict:
+        """The kernel plan chosen by the first step (see eb_step_plan)."""
+        mode, cfg = ctypes.c_int32(), ctypes.c_int32()
+        ms = (ctypes.c_float * 16)()
+        L.call("eb_step_plan", self._h, ctypes.byref(mode), ctypes.byref(cfg), ms, 16)
+        return {"mode": {0: "undecided", 1: "streaming", 2: "resident"}[mode.value], "config": cfg.value,
+                "probe_ms": list(ms)}
 
     def launch_count(self) -> int:
         c = ctypes.c_int64()

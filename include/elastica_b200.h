@@ -68,11 +68,22 @@ typedef enum eb_precision {
                                            rounding-level reformulations
                                            (reciprocals, small-angle series) */
 
+#define EB_FLAG_STEP_STREAMING 0x4u    /* always use the streaming step kernel
+                                           (one launch per step, state through
+                                           HBM every step) */
+#define EB_FLAG_STEP_RESIDENT 0x8u     /* always use a resident configuration
+                                           (whole rods kept on chip for up to
+                                           128 steps per launch) when the rods
+                                           fit; by default the first eb_step
+                                           times both and keeps the faster */
+
 typedef struct eb_config {
-  int32_t device;      /* CUDA device ordinal */
-  int32_t precision;   /* eb_precision */
-  uint32_t flags;      /* EB_FLAG_* */
-  int32_t step_window; /* slots per CTA of the step kernel: 0 (default, 128), 128 or 256 */
+  int32_t device;          /* CUDA device ordinal */
+  int32_t precision;       /* eb_precision */
+  uint32_t flags;          /* EB_FLAG_* */
+  int32_t step_window;     /* slots per CTA of the streaming kernel: 0 (default, 128), 128 or 256 */
+  int32_t resident_config; /* 0: chosen by timing; c > 0: resident configuration c - 1 */
+  int32_t reserved;
 } eb_config;
 
 /* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and
@@ -230,6 +241,12 @@ EB_API eb_status eb_energy(struct eb_sim* sim, double* out, int64_t count);
 /* The cudaStream_t every kernel and copy of this simulator is issued on, for
  * callers that order their own work or timing events against it. */
 EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
+
+/* The step plan chosen by the first eb_step: mode 1 = streaming kernel,
+ * 2 = resident kernel with block configuration `config`; probe_ms[0] is the
+ * streaming probe time, probe_ms[1 + c] configuration c's (up to count). */
+EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* config, float* probe_ms,
+                              int32_t count);
 
 /* Number of kernel launches this simulator has issued (diagnostic). */
 EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);

@@ -24,8 +24,9 @@ def within(errs, bounds):
     return all(errs[k] <= bounds[k] for k in errs)
 
 
-def golden_sim(case, damped, reference_rounding):
-    sim = eb.Simulator(record_diagnostics=True, reference_rounding=reference_rounding)
+def golden_sim(case, damped, reference_rounding, step_mode="streaming", resident_config=0):
+    sim = eb.Simulator(record_diagnostics=True, reference_rounding=reference_rounding, step_mode=step_mode,
+                       resident_config=resident_config)
     s = G.ROD_SETUP
     init = eb.StraightRod(n_elements=s["n"], material=eb.Material(s["density"], s["youngs"], s["shear"]),
                           radius=s["radius"], length=s["length"], origin=s["origin"],
@@ -75,6 +76,21 @@ def test_golden_reference_rounding(name, case, sec, damped):
 @pytest.mark.parametrize("name,case,sec,damped", list(G.step_cases()),
                          ids=lambda v: v if isinstance(v, str) else (
                              v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
+def test_golden_resident(name, case, sec, damped):
+    """The resident multi-step kernel vs the goldens (diagnostics of the last
+    step come from the streaming kernel, so the state after steps-1 resident
+    steps is what this checks), at 4x the reference's epsilon."""
+    sim, refs = golden_sim(case, damped, reference_rounding=False, step_mode="resident", resident_config=1)
+    if sec["steps"]:
+        sim.step(eb.PositionVerlet(), 0.0, G.ROD_SETUP["dt"], sec["steps"])
+    worst = compare_golden(refs, case, sec)
+    bad = {k: v for k, v in worst.items() if v > 4.0}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name,case,sec,damped", list(G.step_cases()),
+                         ids=lambda v: v if isinstance(v, str) else (
+                             v.get("name", "").split(".")[-1] if isinstance(v, dict) else str(v)))
 def test_golden_default(name, case, sec, damped):
     """Default FP64 build (FMA contraction, rounding-level reformulations) vs
     the goldens.  These change rounding by ~1 ulp per operation, so the bound
@@ -111,10 +127,11 @@ def test_state_injection_roundtrip_exact():
         sim.close()
 
 
-def _run_pair(wl, n_steps, reference_rounding=False, damped=False, window=0):
+def _run_pair(wl, n_steps, reference_rounding=False, damped=False, window=0, step_mode="streaming"):
     """Run the workload on the GPU and in the oracle; return the simulator,
     the oracle run, the per-field errors and the parity bounds."""
-    sim = wl.build(record_diagnostics=False, reference_rounding=reference_rounding, window=window)
+    sim = wl.build(record_diagnostics=False, reference_rounding=reference_rounding, window=window,
+                   step_mode=step_mode)
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, n_steps)
     orc, spread = B.oracle_spread(wl, n_steps, damped=damped)
     want = B.state_slots(orc)
@@ -132,14 +149,15 @@ def small_uneven(n_rods=48, seed=7, n_range=(2, 40)):
     return wl
 
 
-@pytest.mark.parametrize("window", [0, 256])
-def test_uneven_batch_1000_steps_vs_oracle(window):
+@pytest.mark.parametrize("window,step_mode", [(0, "streaming"), (256, "streaming"), (0, "resident")])
+def test_uneven_batch_1000_steps_vs_oracle(window, step_mode):
     """Clamped rods of uneven length with gravity and the analytical damper:
     the FP64 drop-in matches the oracle after 1000 steps."""
     wl = small_uneven()
-    sim, orc, errs, bounds = _run_pair(wl, 1000, window=window)
+    sim, orc, errs, bounds = _run_pair(wl, 1000, window=window, step_mode=step_mode)
     assert within(errs, bounds), (errs, bounds)
-    assert sim.launch_count() >= 1000
+    assert sim.step_plan()["mode"] == step_mode
+    assert sim.launch_count() >= (1000 if step_mode == "streaming" else 8)
 
 
 @pytest.mark.parametrize("window", [0, 256])
@@ -149,20 +167,22 @@ def test_reference_rounding_build_vs_oracle(window):
     assert within(errs, bounds), (errs, bounds)
 
 
-def test_rest_curvature_end_torque_vs_oracle():
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_rest_curvature_end_torque_vs_oracle(step_mode):
     wl = W.mixed_batch(n_rods=24, seed=5, n_range=(3, 60), n_steps=500, dt=2e-6)
-    _, _, errs, bounds = _run_pair(wl, 500)
+    _, _, errs, bounds = _run_pair(wl, 500, step_mode=step_mode)
     assert within(errs, bounds), (errs, bounds)
 
 
-def test_explicitly_damped_rods_vs_oracle():
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_explicitly_damped_rods_vs_oracle(step_mode):
     wl = small_uneven(n_rods=20, seed=3)
     wl.model = eb.CosseratRod
     for r in wl.rods:
         r.force_damping_rate = 0.3
         r.torque_damping_rate = 0.2
     wl.damper = None
-    _, _, errs, bounds = _run_pair(wl, 1000, damped=True)
+    _, _, errs, bounds = _run_pair(wl, 1000, damped=True, step_mode=step_mode)
     assert within(errs, bounds), (errs, bounds)
 
 
@@ -188,6 +208,10 @@ def test_tile_and_rod_boundaries(lengths):
     assert within(errs, bounds), (errs, bounds)
     _, _, errs, bounds = _run_pair(wl, 200, reference_rounding=True, window=256)
     assert within(errs, bounds), (errs, bounds)
+    # resident kernel where every rod fits (falls back to streaming otherwise)
+    sim, _, errs, bounds = _run_pair(wl, 200, step_mode="resident")
+    assert within(errs, bounds), (errs, bounds)
+    assert sim.step_plan()["mode"] == ("resident" if max(lengths) + 1 <= 520 else "streaming")
 
 
 def test_energy_matches_oracle():
@@ -198,10 +222,11 @@ def test_energy_matches_oracle():
     np.testing.assert_allclose(e_gpu, e_cpu, rtol=1e-9, atol=1e-300)
 
 
-def test_determinism_bitwise():
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_determinism_bitwise(step_mode):
     wl = small_uneven(n_rods=10, seed=4)
-    a = wl.build()
-    b = wl.build()
+    a = wl.build(step_mode=step_mode)
+    b = wl.build(step_mode=step_mode)
     a.step(eb.PositionVerlet(), 0.0, wl.dt, 100)
     b.step(eb.PositionVerlet(), 0.0, wl.dt, 100)
     for name in ("Position", "Velocity", "Director", "AngularVelocity"):
@@ -244,12 +269,13 @@ def test_error_paths():
     assert e.value.status == 6  # EB_ERR_NOT_FOUND
 
 
-def test_full_size_uneven_batch_sampled_parity():
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_full_size_uneven_batch_sampled_parity(step_mode):
     """The full uneven batch (16,384 rods, ~4.4 M elements) for 1000 steps on
     the GPU; rods are independent, so the oracle checks a seeded sample of 48
     of them run on their own."""
     wl = W.uneven_batch()
-    sim = wl.build()
+    sim = wl.build(step_mode=step_mode)
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, 1000)
     rng = np.random.default_rng(2024)
     pick = np.sort(rng.choice(len(wl.rods), size=48, replace=False))
@@ -263,3 +289,13 @@ def test_full_size_uneven_batch_sampled_parity():
         got = np.concatenate([full[:, offs[k]:offs[k + 1]] for k in pick], axis=1)
         err = B.max_rel_error_per_rod(got, orc.comp(key), sub.n_elements, place)
         assert err <= bounds[name], (name, err, bounds[name])
+
+
+def test_step_planner_times_every_candidate():
+    wl = small_uneven(n_rods=64, seed=12, n_range=(20, 200))
+    sim = wl.build()
+    sim.step(eb.PositionVerlet(), 0.0, wl.dt, 4)
+    plan = sim.step_plan()
+    assert plan["mode"] in ("streaming", "resident")
+    assert plan["probe_ms"][0] > 0.0  # streaming probe
+    assert any(t > 0.0 for t in plan["probe_ms"][1:])  # at least one resident probe
