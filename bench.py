@@ -205,6 +205,50 @@ def workload_config(wl, world):
             "l2": "no flush: state + parameters exceed the 126 MB L2 many times over"}
 
 
+def mixed_comparison(W, eb, torch, args, rank, local, barrier, pg):
+    wl = W.mixed_batch(n_rods=args.mixed_rods, seed=1003 + rank)
+    out = {"workload": "mixed_batch", "rods": len(wl.rods), "elements": wl.total_elements, "dt": wl.dt,
+           "steps": args.mixed_steps,
+           "dt_rule": "0.5 min(l^2 / (r c)); 1e-5 s is unstable for these rods in the FP64 reference path"}
+    res = {}
+    for label, kw in (("fp64", {"step_mode": "streaming"}), ("mixed", {"precision": "mixed"})):
+        sim = wl.build(device=local, **kw)
+        e0 = sim.energy().sum()
+        stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
+        barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(eb.PositionVerlet(), 0.0, wl.dt, args.mixed_steps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = torch.tensor([a.elapsed_time(b)], device="cuda")
+        if pg is not None:
+            pg.all_reduce(ms, op=pg.ReduceOp.MAX)
+        tips = np.stack([r.get("Position")[:, -1] for r in sim.rods])
+        e1 = sim.energy().sum()
+        res[label] = {"ms": float(ms.item()), "tips": tips, "e0": e0, "e1": e1, "plan": sim.step_plan()}
+        sim.close()
+    lengths = np.array([r.length for r in wl.rods])
+    err = np.linalg.norm(res["mixed"]["tips"] - res["fp64"]["tips"], axis=1) / lengths
+    n_el = float(wl.total_elements)
+    out.update({
+        "fp64_value": n_el * args.mixed_steps / (res["fp64"]["ms"] / 1e3),
+        "value": n_el * args.mixed_steps / (res["mixed"]["ms"] / 1e3),
+        "unit": UNIT,
+        "tip_error_max": float(np.max(err)), "tip_error_p99": float(np.percentile(err, 99)),
+        "tip_error_definition": "|tip_mixed - tip_fp64| / rod length after all steps",
+        "energy_fp64": [res["fp64"]["e0"], res["fp64"]["e1"]], "energy_mixed": [res["mixed"]["e0"], res["mixed"]["e1"]],
+        "energy_rel_diff": abs(res["mixed"]["e1"] - res["fp64"]["e1"]) / abs(res["fp64"]["e1"]),
+        "finite": bool(np.all(np.isfinite(err))),
+        "plan": res["mixed"]["plan"],
+    })
+    out["speedup_vs_fp64_dropin"] = out["value"] / out["fp64_value"]
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -218,6 +262,9 @@ def main(argv=None) -> int:
                     help="steps timed on the resident (batched) kernel; 0 skips it")
     ap.add_argument("--resident-config", type=int, default=0,
                     help="resident configuration (1-based; 0 = chosen by timing)")
+    ap.add_argument("--mixed-rods", type=int, default=65536, help="rods of the mixed-precision batch")
+    ap.add_argument("--mixed-steps", type=int, default=10000,
+                    help="steps of the FP64-vs-mixed comparison on the mixed batch; 0 skips it")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-rounding", action="store_true",
@@ -360,6 +407,12 @@ def main(argv=None) -> int:
         bsim.close()
         sim = None
 
+    # ---- mixed precision: the mixed batch on the FP64 streaming drop-in and
+    # on the mixed-precision resident kernel, tip positions compared
+    mixed = None
+    if args.mixed_steps > 0:
+        mixed = mixed_comparison(W, eb, torch, args, rank, local, barrier, pg)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, sample = cpu_reference_rate(wl, 0, budget_s=args.cpu_budget_s, max_rods=2048)
@@ -389,6 +442,7 @@ def main(argv=None) -> int:
             "clocks": clock_info,
             "state_finite": bool(finite),
             "batched": batched,
+            "mixed": mixed,
         }
         print(json.dumps(line), flush=True)
     if sim is not None:

@@ -24,6 +24,7 @@ SOURCES = [
     ("rod_step_fp64.o", "rod_step_fp64.cu", ["-DEB_FAST_FP64"]),
     ("rod_step_fp64_reference.o", "rod_step_fp64.cu", ["--fmad=false"]),
     ("rod_block_fp64.o", "rod_block_fp64.cu", []),
+    ("rod_block_mixed.o", "rod_block_mixed.cu", []),
     ("rod_energy.o", "rod_energy.cu", []),
 ]
 HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh"]

@@ -27,6 +27,8 @@ int block_config_count();
 int block_config_capacity(int config);
 cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
                                   int config, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
+                                   int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -336,8 +338,8 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
     return fail(EB_ERR_INVALID_ARGUMENT, "resident_config out of range");
   if (cfg.step_window != 0 && cfg.step_window != 128 && cfg.step_window != 256)
     return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
-  if (cfg.precision == EB_PRECISION_MIXED)
-    return fail(EB_ERR_UNSUPPORTED, "mixed precision is not built into this library yet");
+  if (cfg.precision == EB_PRECISION_MIXED && (cfg.flags & (EB_FLAG_REFERENCE_ROUNDING | EB_FLAG_STEP_STREAMING)))
+    return fail(EB_ERR_INVALID_ARGUMENT, "mixed precision runs on the resident kernels only");
   int ndev = 0;
   EB_CUDA(cudaGetDeviceCount(&ndev));
   if (cfg.device < 0 || cfg.device >= ndev) return fail(EB_ERR_INVALID_ARGUMENT, "no such CUDA device");
@@ -701,6 +703,14 @@ cudaError_t launch_streaming(eb_sim* s, eb::StepArgs& a, bool rec) {
   return eb::launch_rod_step_fp64(a, rec, s->any_damped, window, s->stream);
 }
 
+cudaError_t launch_resident(eb_sim* s, eb::StepArgs& a, int config, int steps) {
+  if (s->cfg.precision == EB_PRECISION_MIXED)
+    return eb::launch_rod_block_mixed(a, s->d_cta_start[config], s->n_ctas[config], steps, config, s->any_damped,
+                                      s->stream);
+  return eb::launch_rod_block_fp64(a, s->d_cta_start[config], s->n_ctas[config], steps, config, s->any_damped,
+                                   s->stream);
+}
+
 // Pack the rods, in slot order, into CTAs of at most `cap` slots (next fit).
 // Returns false when a rod is longer than the capacity.
 bool pack_rods(const eb_sim* s, int cap, std::vector<int64_t>& starts) {
@@ -764,7 +774,10 @@ eb_status plan_steps(eb_sim* s, double dt) {
   a.out = s->d_state[s->cur ^ 1];
   float best = 0.0f;
   int best_mode = 1, best_cfg = -1;
-  const bool force_resident = (s->cfg.flags & EB_FLAG_STEP_RESIDENT) != 0;
+  // mixed precision exists only on the resident kernels: the streaming FP64
+  // kernel is then a fallback for rods too long for any configuration
+  const bool force_resident =
+      (s->cfg.flags & EB_FLAG_STEP_RESIDENT) != 0 || s->cfg.precision == EB_PRECISION_MIXED;
   for (int c = -1; c < eb::block_config_count(); ++c) {
     if (c >= 0 && !s->d_cta_start[c]) continue;
     if (c < 0 && force_resident) continue;
@@ -773,8 +786,7 @@ eb_status plan_steps(eb_sim* s, double dt) {
       if (c < 0) {
         for (int k = 0; k < kProbeSteps; ++k) EB_CUDA(launch_streaming(s, a, false));
       } else {
-        EB_CUDA(eb::launch_rod_block_fp64(a, s->d_cta_start[c], s->n_ctas[c], kProbeSteps, c, s->any_damped,
-                                          s->stream));
+        EB_CUDA(launch_resident(s, a, c, kProbeSteps));
       }
       EB_CUDA(cudaEventRecord(e1, s->stream));
       EB_CUDA(cudaEventSynchronize(e1));
@@ -831,7 +843,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
       const int k = static_cast<int>(std::min<int64_t>(kResidentChunk, resident_steps - done));
       a.in = s->d_state[s->cur];
       a.out = s->d_state[s->cur ^ 1];
-      EB_CUDA(eb::launch_rod_block_fp64(a, s->d_cta_start[c], s->n_ctas[c], k, c, s->any_damped, s->stream));
+      EB_CUDA(launch_resident(s, a, c, k));
       s->cur ^= 1;
       ++s->launches;
       done += k;
