@@ -318,7 +318,7 @@ cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int
 // rod a configuration can hold (n + 1 slots).
 namespace {
 // {slots per CTA, threads per CTA}
-constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {264, 256}, {264, 128}};
+constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {264, 256}, {264, 288}};
 constexpr int kNumConfigs = 4;
 }  // namespace
 
@@ -335,7 +335,7 @@ cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start
     case 0: return launch_block_cfg<520, 512, true>(args, cta_start, n_ctas, n_steps, damped, stream);
     case 1: return launch_block_cfg<520, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
     case 2: return launch_block_cfg<264, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 3: return launch_block_cfg<264, 128, true>(args, cta_start, n_ctas, n_steps, damped, stream);
+    case 3: return launch_block_cfg<264, 288, true>(args, cta_start, n_ctas, n_steps, damped, stream);
     default: return cudaErrorInvalidValue;
   }
 }

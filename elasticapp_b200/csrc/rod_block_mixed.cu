@@ -1,27 +1,50 @@
 // Resident multi-step PositionVerlet kernel, mixed precision.
 //
 // Same structure as rod_block_fp64.cu (whole rods staged in shared memory,
-// many steps per launch, both half drifts per step), with the element-local
-// arithmetic in FP32 and everything whose stability needs FP64 kept in FP64:
+// many steps per launch), with the element-local arithmetic in FP32 and
+// everything whose stability needs FP64 kept in FP64:
 //
 //   FP64: positions, velocities, directors and angular velocities (state and
 //         their accumulation, including the director's exponential update,
 //         whose rounding would otherwise erode the orthonormality the
 //         curvature relies on), the position difference of an element, the
 //         shear/stretch strain sigma = Q dx / l0 - z of nearly inextensible
-//         rods (a cancellation), the curvature's skew products and trace
-//         (cancellations between neighbouring directors).
+//         rods (a cancellation), the differences of neighbouring directors
+//         from which the curvature is formed.
 //   FP32: lengths, tangents, dilatations, constitutive products, internal
 //         loads and couples, accelerations, the damping factors.
 //
+// FP32 copies of the director and angular velocity are refreshed whenever
+// the FP64 values change, so each is converted once per step, and the
+// divisions of the element math are reciprocal square roots and stored
+// reciprocals: conversions and the special-function unit, not the FP32
+// arithmetic, bound this kernel otherwise.
+//
 // Reformulations (mathematically identical; rounding differs):
 //   sigma = (Q t) e - z  =  Q dx / l0 - z         (no normalisation)
-//   rate  = (t . dv) / (e l0)  =  (t . dv) / l
+//   rate  = (t . dv) / (e l0)  =  (t . dv) / l,   1 / e = l0 / l
 //   theta = acos(c) = 2 asin(sqrt((1 - c) / 2)),  sin(theta) = sqrt((1-c)(1+c))
-// and the reference's 1e-14 guard inside sin(theta + 1e-14) is dropped (it
-// moves the curvature by less than 1e-9 relative at the smallest angle the
-// 1e-10 shift of the trace allows); theta / sin(theta) comes from its series
-// 1 + y/3 + 2y^2/15 in y = 1 - cos(theta) below y = 1e-3.
+//   the curvature's skew products and 1 - cos(theta) from the differences of
+//   neighbouring directors (see the Voronoi phase)
+//   exp(-[u]x) Q = Q + (sin t / t) [u]x Q + ((1 - cos t) / t^2)(u u^T - t^2) Q,
+//   t = |u|, with both coefficients from their Taylor series for t < 0.1
+//   (no square root or division)
+//   the damper factors exp(x) from their Taylor series for |x| < 0.01
+// The reference's 1e-14 guards (in the rotation axis and in sin(theta +
+// 1e-14)) are dropped: each moves a director by ~1e-14 per step, far below
+// this path's tolerance.  theta / sin(theta) comes from its series
+// 1 + y/3 + 2y^2/15 in y = 1 - cos(theta) below y = 1e-3.  The second half
+// drift of a step and the first half drift of the next use the same velocity
+// and angular velocity and are applied as one full drift.
+//
+// A step is two phases with one barrier after each: element and Voronoi
+// terms of a slot together (the neighbouring element's length is recomputed
+// instead of exchanged), then the kick, the constraints and the drift.
+//
+// Per-rod constraint data (clamp, damper, end torque flags and the damper's
+// constants) is copied into shared memory once per launch, so the step loop
+// reads global memory only for the clamp target and end torque of the few
+// slots that carry them.
 #include <cuda_runtime.h>
 
 #include "eb_internal.h"
@@ -34,12 +57,12 @@ using D3 = Vec3<double>;
 using F3 = Vec3<float>;
 
 // FP64 rows
-enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dRowsD = 19 };
+enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dDampT = 19, dSig0 = 20, dRowsD = 23 };
 // FP32 rows
 enum MixedRowF : int {
-  fMass = 0, fL0 = 1, fD0 = 2, fSig0 = 3, fKap0 = 6, fShear = 9, fBend = 12, fJ = 15, fJinv = 18,
-  fNuF = 21, fNuT = 22,
-  fL = 23, fE = 24, fF = 25, fG = 28, fH = 31, fTl = 34, fRowsF = 37
+  fMass = 0, fInvMass = 1, fL0 = 2, fInvL0 = 3, fD0 = 4, fInvD0 = 5, fKap0 = 6, fShear = 9, fBend = 12,
+  fJ = 15, fJinv = 18, fNuF = 21, fNuT = 22,
+  fF = 23, fP = 26, fM = 29, fE = 32, fDampR = 33, fQ = 34, fW = 43, fRowsF = 46
 };
 
 template <int kCap>
@@ -66,20 +89,76 @@ __device__ __forceinline__ F3 tof(D3 a) {
   return {static_cast<float>(a.x), static_cast<float>(a.y), static_cast<float>(a.z)};
 }
 
+// FP64 director update Q <- exp(-[u]x) Q (Rodrigues' formula of
+// Systems/States/Expressions/backends/blaze/SO3PrimitiveAddAssign/Scalar.hpp:41-95),
+// written with the unnormalised u: cos t = 1 - a2 t^2, (1 - cos t) uh uh^T =
+// a2 u u^T and sin(t) uh = a1 u for uh = u / t.
+__device__ __forceinline__ void so3_series(double q[9], double u0, double u1, double u2) {
+  const double z = u0 * u0 + u1 * u1 + u2 * u2;
+  double a1, a2;  // sin(t) / t and (1 - cos t) / t^2
+  if (z < 0.01) {
+    a1 = 1.0 + z * (-1.0 / 6.0 + z * (1.0 / 120.0 + z * (-1.0 / 5040.0 + z * (1.0 / 362880.0 - z * (1.0 / 39916800.0)))));
+    a2 = 0.5 + z * (-1.0 / 24.0 + z * (1.0 / 720.0 + z * (-1.0 / 40320.0 + z * (1.0 / 3628800.0 - z * (1.0 / 479001600.0)))));
+  } else {
+    const double t = sqrt(z);
+    double s, c;
+    sincos(t, &s, &c);
+    a1 = s / t;
+    a2 = (1.0 - c) / z;
+  }
+  double out[9];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double com = q[j] * u0 + q[3 + j] * u1 + q[6 + j] * u2;
+    out[j] = q[j] + a2 * (u0 * com - z * q[j]) + a1 * (q[3 + j] * u2 - q[6 + j] * u1);
+    out[3 + j] = q[3 + j] + a2 * (u1 * com - z * q[3 + j]) + a1 * (q[6 + j] * u0 - q[j] * u2);
+    out[6 + j] = q[6 + j] + a2 * (u2 * com - z * q[6 + j]) + a1 * (q[j] * u1 - q[3 + j] * u0);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) q[k] = out[k];
+}
+
+// exp(x), Taylor series below |x| = 0.01 (truncation below 1e-12 relative)
+__device__ __forceinline__ float exp_small(float x) {
+  if (fabsf(x) < 0.01f) return 1.f + x * (1.f + x * (0.5f + x * (1.f / 6.f + x * (1.f / 24.f))));
+  return expf(x);
+}
+
+// x += c v; Q <- exp(-c [w]x) Q for element slots; FP32 copy of Q refreshed
 template <int kCap>
-__device__ __forceinline__ void half_drift(const MRows<kCap>& R, int s, uint32_t meta, double hdt) {
-  const D3 v = R.d3(dV, s);
+__device__ __forceinline__ void drift(const MRows<kCap>& R, int s, uint32_t meta, double c, D3 v, D3 w) {
   const D3 x = R.d3(dX, s);
-  R.pd3(dX, s, D3{x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z});
+  R.pd3(dX, s, D3{x.x + c * v.x, x.y + c * v.y, x.z + c * v.z});
   if (meta & kElem) {
-    const D3 w = R.d3(dW, s);
     double q[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) q[k] = R.ad(dQ + k, s);
-    so3_update_fast(q, hdt * w.x, hdt * w.y, hdt * w.z);
+    so3_series(q, c * w.x, c * w.y, c * w.z);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = q[k];
+    for (int k = 0; k < 9; ++k) {
+      R.ad(dQ + k, s) = q[k];
+      R.af(fQ + k, s) = static_cast<float>(q[k]);
+    }
   }
+}
+
+// the clamp's value constraint on the first slot of a clamped rod
+template <int kCap>
+__device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, const RodInfo& ri) {
+  R.pd3(dX, s, D3{ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]});
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    R.ad(dQ + k, s) = ri.clamp_Q[k];
+    R.af(fQ + k, s) = static_cast<float>(ri.clamp_Q[k]);
+  }
+}
+
+// FP32 length of element s from its FP64 position difference
+template <int kCap>
+__device__ __forceinline__ float element_length(const MRows<kCap>& R, int s) {
+  const F3 dxf = tof(R.d3(dX, s + 1) - R.d3(dX, s));
+  const float l2 = dot(dxf, dxf);
+  return l2 * rsqrtf(l2);
 }
 
 __device__ __forceinline__ int mixed_param_row(int f) {
@@ -91,7 +170,6 @@ __device__ __forceinline__ int mixed_param_row(int f) {
     case kNuT: return fNuT;
     default: break;
   }
-  if (f >= kSig0 && f < kSig0 + 3) return fSig0 + (f - kSig0);
   if (f >= kKap0 && f < kKap0 + 3) return fKap0 + (f - kKap0);
   if (f >= kShear && f < kShear + 3) return fShear + (f - kShear);
   if (f >= kBend && f < kBend + 3) return fBend + (f - kBend);
@@ -106,56 +184,81 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   extern __shared__ __align__(128) double smem[];
   const MRows<kCap> R{smem, reinterpret_cast<float*>(smem + dRowsD * kCap)};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + fRowsF * kCap);
+  uint32_t* rflag_s = meta_s + kCap;
 
   const int tid = threadIdx.x;
   const int64_t g0 = cta_start[blockIdx.x];
   const int count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
   const int64_t S = a.stride;
 
+  // ---- stage state, parameters, reciprocals, FP32 copies and rod data
+  const bool any_rod = (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
   for (int s = tid; s < count; s += kThreads) {
     const int64_t g = g0 + s;
-    meta_s[s] = a.meta[g];
+    const uint32_t meta = a.meta[g];
+    meta_s[s] = meta;
+    uint32_t rf = 0;
+    double dtc = 1.0;
+    float dr = 0.f;
+    if (any_rod) {
+      const RodInfo& ri = a.rods[meta >> kRodShift];
+      rf = ri.flags;
+      dtc = ri.damper_t;
+      dr = static_cast<float>(ri.damper_r);
+    }
+    rflag_s[s] = rf;
+    R.ad(dDampT, s) = dtc;
+    R.af(fDampR, s) = dr;
 #pragma unroll 1
     for (int f = 0; f < kStateFields; ++f) R.ad(f, s) = a.in[f * S + g];
-    const double l0 = a.par[kL0 * S + g];
-    R.ad(dInvL0, s) = 1.0 / l0;
+#pragma unroll 1
+    for (int k = 0; k < 9; ++k) R.af(fQ + k, s) = static_cast<float>(R.ad(dQ + k, s));
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) R.af(fW + k, s) = static_cast<float>(R.ad(dW + k, s));
+    const double il0 = 1.0 / a.par[kL0 * S + g];
+    R.ad(dInvL0, s) = il0;
+    R.af(fInvL0, s) = static_cast<float>(il0);
+    // the rest strain, with the unit axial strain of sigma = Q dx / l0 - z folded in
+    R.ad(dSig0, s) = a.par[kSig0 * S + g];
+    R.ad(dSig0 + 1, s) = a.par[(kSig0 + 1) * S + g];
+    R.ad(dSig0 + 2, s) = a.par[(kSig0 + 2) * S + g] + 1.0;
 #pragma unroll 1
     for (int f = 0; f < kParamFields; ++f) {
       const int r = mixed_param_row(f);
       if (r < 0 || (!kDamped && (f == kNuF || f == kNuT))) continue;
       R.af(r, s) = static_cast<float>(a.par[f * S + g]);
     }
+    R.af(fInvMass, s) = static_cast<float>(1.0 / a.par[kMass * S + g]);
+    R.af(fInvD0, s) = static_cast<float>(1.0 / a.par[kD0 * S + g]);
   }
   __syncthreads();
 
   const double dt = a.dt, hdt = a.half_dt;
   const float dtf = static_cast<float>(dt);
-  const bool any_rod = (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
   const F3 grav = {static_cast<float>(a.gravity[0]), static_cast<float>(a.gravity[1]),
                    static_cast<float>(a.gravity[2])};
 
-  for (int step = 0; step < n_steps; ++step) {
-    // ---- first half drift (the second one of the previous step was applied
-    // at the end of its update phase) and clamp value constraint
-    for (int s = tid; s < count; s += kThreads) {
-      const uint32_t meta = meta_s[s];
-      half_drift(R, s, meta, hdt);
-      if (any_rod && (meta & kFirst)) {
-        const RodInfo& ri = a.rods[meta >> kRodShift];
-        if (ri.flags & kRodClamp) {
-          R.pd3(dX, s, D3{ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]});
-#pragma unroll
-          for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = ri.clamp_Q[k];
-        }
-      }
-    }
-    __syncthreads();
+  // ---- first half drift of the first step and the clamp's value constraint
+  for (int s = tid; s < count; s += kThreads) {
+    const uint32_t meta = meta_s[s];
+    drift(R, s, meta, hdt, R.d3(dV, s), R.d3(dW, s));
+    if ((meta & kFirst) && (rflag_s[s] & kRodClamp)) clamp_value(R, s, a.rods[meta >> kRodShift]);
+  }
+  __syncthreads();
 
-    // ---- element geometry, internal stress, element-local torque terms
+  // Two phases per step, one barrier after each.  Phase A: element s (strain,
+  // internal load, element-local torque terms) and Voronoi s (curvature and
+  // couple, with the length of element s + 1 recomputed rather than shared).
+  // Phase B: loads, torques, kick, rate constraints, then the merged drift
+  // (second half of this step and first half of the next; half on the last
+  // step), the value constraint and, on the last step, the write-back.
+  for (int step = 0; step < n_steps; ++step) {
+    const bool last = step == n_steps - 1;
+
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
-      F3 f{0.f, 0.f, 0.f}, tl{0.f, 0.f, 0.f};
-      float l = 1.f, e = 1.f;
+      F3 f{0.f, 0.f, 0.f}, p{0.f, 0.f, 0.f}, mm{0.f, 0.f, 0.f};
+      float e = 1.f;
       if (meta & kElem) {
         const D3 dx = R.d3(dX, s + 1) - R.d3(dX, s);
         double qd[3];
@@ -163,80 +266,79 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         for (int k = 0; k < 3; ++k)
           qd[k] = R.ad(dQ + 3 * k, s) * dx.x + R.ad(dQ + 3 * k + 1, s) * dx.y + R.ad(dQ + 3 * k + 2, s) * dx.z;
         const double il0 = R.ad(dInvL0, s);
-        const F3 s0 = R.f3(fSig0, s);
-        const F3 d = {static_cast<float>(qd[0] * il0 - static_cast<double>(s0.x)),
-                      static_cast<float>(qd[1] * il0 - static_cast<double>(s0.y)),
-                      static_cast<float>((qd[2] * il0 - 1.0) - static_cast<double>(s0.z))};
-        l = sqrtf(static_cast<float>(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z));
-        const float il = 1.f / l;
-        const F3 t = scale(tof(dx), il);
-        e = l * static_cast<float>(il0);
+        const F3 d = {static_cast<float>(qd[0] * il0 - R.ad(dSig0, s)),
+                      static_cast<float>(qd[1] * il0 - R.ad(dSig0 + 1, s)),
+                      static_cast<float>(qd[2] * il0 - R.ad(dSig0 + 2, s))};
+        const F3 dxf = tof(dx);
+        const float l2 = dot(dxf, dxf);
+        const float il = rsqrtf(l2);
+        const float l = l2 * il;
+        const F3 t = scale(dxf, il);
+        const float l0 = R.af(fL0, s);
+        e = l * R.af(fInvL0, s);
+        const float ie = l0 * il;
         const F3 sh = R.f3(fShear, s);
         const F3 nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
         float qf[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
-        const float ie = 1.f / e;
+        for (int k = 0; k < 9; ++k) qf[k] = R.af(fQ + k, s);
         f = scale(mattranspvec(qf, nl), ie);
         const F3 qt = matvec(qf, t);
-        const F3 w = tof(R.d3(dW, s));
+        const F3 w = R.f3(fW, s);
         const F3 J = R.f3(fJ, s);
         const F3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
         const F3 dv = tof(R.d3(dV, s + 1) - R.d3(dV, s));
         const float rate = dot(t, dv) * il;
-        tl = scale(cross(qt, nl), R.af(fL0, s)) + cross(jwe, w) + scale(jwe, rate);
+        p = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
+
+        if (meta & kVor) {
+          // With d_k the director rows of element s and dd_k = d_k(s+1) - d_k(s)
+          // (FP64 differences), the reference's skew terms are exactly
+          //   d3.d2' - d2.d3' = d3.dd2 - d2.dd3 (and cyclic), since d3.d2 = d2.d3,
+          // and 1 - cos(theta) = 1.5 - tr/2 = |dd|^2/4 for unit rows (their
+          // norms stay within 1e-14 of one, below the reference's 1e-10 shift);
+          // both forms are free of the cancellation of the original products.
+          float dd[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) dd[k] = static_cast<float>(R.ad(dQ + k, s + 1) - R.ad(dQ + k, s));
+          float sq = 0.f;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) sq += dd[k] * dd[k];
+          const float y = 0.25f * sq + 1e-10f;
+          float ratio;  // theta / sin(theta)
+          if (y < 1e-3f) {
+            ratio = 1.f + y * (1.f / 3.f + y * (2.f / 15.f));
+          } else {
+            ratio = 2.f * asinf(sqrtf(0.5f * y)) * rsqrtf(y * (2.f - y));
+          }
+          const float D0 = R.af(fD0, s);
+          const float st = 0.5f * ratio * R.af(fInvD0, s);
+          const F3 d1{qf[0], qf[1], qf[2]}, d2{qf[3], qf[4], qf[5]}, d3{qf[6], qf[7], qf[8]};
+          const F3 e1{dd[0], dd[1], dd[2]}, e2{dd[3], dd[4], dd[5]}, e3{dd[6], dd[7], dd[8]};
+          const F3 skew = {dot(d3, e2) - dot(d2, e3), dot(d1, e3) - dot(d3, e1), dot(d2, e1) - dot(d1, e2)};
+          const F3 kappa = scale(skew, st);
+          // 1 / eps^3 with eps = D / D0, D the mean length of elements s, s + 1
+          const float ieps = __fdividef(D0, 0.5f * (l + element_length(R, s + 1)));
+          const float ic = ieps * ieps * ieps;
+          const F3 dk = kappa - R.f3(fKap0, s);
+          const F3 B = R.f3(fBend, s);
+          const F3 tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
+          // the couple's two parts: G = tau / eps^3 (differenced) and
+          // H = (kappa x tau) D0 / eps^3 (averaged) enter torque s as
+          // (G_s + H_s / 2) - (G_{s-1} - H_{s-1} / 2)
+          const F3 gg = scale(tau, ic);
+          const F3 hh = scale(cross(kappa, tau), 0.5f * ic * D0);
+          p = p + gg + hh;
+          mm = gg - hh;
+        }
       }
-      R.af(fL, s) = l;
       R.af(fE, s) = e;
       R.pf3(fF, s, f);
-      R.pf3(fTl, s, tl);
+      R.pf3(fP, s, p);
+      R.pf3(fM, s, mm);
     }
     __syncthreads();
 
-    // ---- Voronoi curvature and couple
-    for (int s = tid; s < count; s += kThreads) {
-      const uint32_t meta = meta_s[s];
-      F3 gg{0.f, 0.f, 0.f}, hh{0.f, 0.f, 0.f};
-      if (meta & kVor) {
-        double qc[9], qn[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          qc[k] = R.ad(dQ + k, s);
-          qn[k] = R.ad(dQ + k, s + 1);
-        }
-        const double tr = qc[0] * qn[0] + qc[1] * qn[1] + qc[2] * qn[2] + qc[3] * qn[3] + qc[4] * qn[4] +
-                          qc[5] * qn[5] + qc[6] * qn[6] + qc[7] * qn[7] + qc[8] * qn[8];
-        // 1 - cos(theta) with the reference's 1e-10 shift
-        const float y = fmaxf(static_cast<float>((1.5 + 1e-10) - 0.5 * tr), 0.f);
-        float ratio;  // theta / sin(theta)
-        if (y < 1e-3f) {
-          ratio = 1.f + y * (1.f / 3.f + y * (2.f / 15.f));
-        } else {
-          ratio = 2.f * asinf(sqrtf(0.5f * y)) / sqrtf(y * (2.f - y));
-        }
-        const float D0 = R.af(fD0, s);
-        const float st = 0.5f * ratio / D0;
-        const F3 skew = {static_cast<float>(-qc[3] * qn[6] - qc[4] * qn[7] - qc[5] * qn[8] + qc[6] * qn[3] +
-                                            qc[7] * qn[4] + qc[8] * qn[5]),
-                         static_cast<float>(qc[0] * qn[6] + qc[1] * qn[7] + qc[2] * qn[8] - qc[6] * qn[0] -
-                                            qc[7] * qn[1] - qc[8] * qn[2]),
-                         static_cast<float>(-qc[0] * qn[3] - qc[1] * qn[4] - qc[2] * qn[5] + qc[3] * qn[0] +
-                                            qc[4] * qn[1] + qc[5] * qn[2])};
-        const F3 kappa = scale(skew, st);
-        const float eps = 0.5f * (R.af(fL, s) + R.af(fL, s + 1)) / D0;
-        const float ic = 1.f / (eps * eps * eps);
-        const F3 dk = kappa - R.f3(fKap0, s);
-        const F3 B = R.f3(fBend, s);
-        const F3 tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
-        gg = scale(tau, ic);
-        hh = scale(cross(kappa, tau), ic * D0);
-      }
-      R.pf3(fG, s, gg);
-      R.pf3(fH, s, hh);
-    }
-    __syncthreads();
-
-    // ---- loads, torques, accelerations, kick, rate constraints, second half drift
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       const bool first = (meta & kFirst) != 0;
@@ -250,70 +352,66 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         F = {F.x - cf * vf.x, F.y - cf * vf.y, F.z - cf * vf.z};
       }
       if (a.sim_flags & kSimGravity) F = F + F3{grav.x * m, grav.y * m, grav.z * m};
-      const float im = 1.f / m;
+      const float im = R.af(fInvMass, s);
       v = {v.x + dt * static_cast<double>(F.x * im), v.y + dt * static_cast<double>(F.y * im),
            v.z + dt * static_cast<double>(F.z * im)};
       D3 w{0.0, 0.0, 0.0};
-      const RodInfo* ri = any_rod ? a.rods + (meta >> kRodShift) : nullptr;
+      const uint32_t rf = rflag_s[s];
       if (meta & kElem) {
         const float e = R.af(fE, s);
         w = R.d3(dW, s);
-        F3 T = R.f3(fG, s);
-        F3 Q2 = R.f3(fH, s);
-        if (!first) {
-          T = T - R.f3(fG, s - 1);
-          Q2 = Q2 + R.f3(fH, s - 1);
-        }
-        T = T + scale(Q2, 0.5f) + R.f3(fTl, s);
+        F3 T = R.f3(fP, s);
+        if (!first) T = T - R.f3(fM, s - 1);
         if (kDamped) {
           const float ct = 0.5f * (m + R.af(fMass, s + 1)) * R.af(fNuT, s);
-          const F3 wf = tof(w);
+          const F3 wf = R.f3(fW, s);
           T = {T.x - ct * wf.x, T.y - ct * wf.y, T.z - ct * wf.z};
         }
-        if (any_rod && (meta & kLastElem) && (ri->flags & kRodEndTorque)) {
+        if ((meta & kLastElem) && (rf & kRodEndTorque)) {
+          const RodInfo& ri = a.rods[meta >> kRodShift];
           float qf[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
-          T = T + matvec(qf, F3{static_cast<float>(ri->end_torque[0]), static_cast<float>(ri->end_torque[1]),
-                                static_cast<float>(ri->end_torque[2])});
+          for (int k = 0; k < 9; ++k) qf[k] = R.af(fQ + k, s);
+          T = T + matvec(qf, F3{static_cast<float>(ri.end_torque[0]), static_cast<float>(ri.end_torque[1]),
+                                static_cast<float>(ri.end_torque[2])});
         }
         const F3 ji = R.f3(fJinv, s);
         w = {w.x + dt * static_cast<double>(ji.x * T.x * e), w.y + dt * static_cast<double>(ji.y * T.y * e),
              w.z + dt * static_cast<double>(ji.z * T.z * e)};
-        if (any_rod && (ri->flags & kRodDamper)) {
+        if (rf & kRodDamper) {
           const float mn = R.af(fMass, s + 1);
           float em = 0.5f * (m + mn);
           if (first) em += 0.5f * m;
           if (meta & kLastElem) em += 0.5f * mn;
-          const float y = -static_cast<float>(ri->damper_r) * em * dtf * e;
-          w = {w.x * static_cast<double>(expf(y * ji.x)), w.y * static_cast<double>(expf(y * ji.y)),
-               w.z * static_cast<double>(expf(y * ji.z))};
+          const float y = -R.af(fDampR, s) * em * dtf * e;
+          w = {w.x * static_cast<double>(exp_small(y * ji.x)), w.y * static_cast<double>(exp_small(y * ji.y)),
+               w.z * static_cast<double>(exp_small(y * ji.z))};
         }
       }
-      if (any_rod) {
-        if (first && (ri->flags & kRodClamp)) {
-          v = D3{0.0, 0.0, 0.0};
-          w = D3{0.0, 0.0, 0.0};
-        }
-        if (ri->flags & kRodDamper) v = scale(v, ri->damper_t);
+      const bool clamped = first && (rf & kRodClamp);
+      if (clamped) {
+        v = D3{0.0, 0.0, 0.0};
+        w = D3{0.0, 0.0, 0.0};
       }
+      if (rf & kRodDamper) v = scale(v, R.ad(dDampT, s));
       R.pd3(dV, s, v);
-      if (meta & kElem) R.pd3(dW, s, w);
-      half_drift(R, s, meta, hdt);
+      if (meta & kElem) {
+        R.pd3(dW, s, w);
+        R.pf3(fW, s, tof(w));
+      }
+      drift(R, s, meta, last ? hdt : dt, v, w);
+      if (clamped) clamp_value(R, s, a.rods[meta >> kRodShift]);
+      if (last) {
+        const int64_t g = g0 + s;
+#pragma unroll
+        for (int fld = 0; fld < 6; ++fld) a.out[fld * S + g] = R.ad(fld, s);
+        if (meta & kElem) {
+#pragma unroll
+          for (int fld = 6; fld < kStateFields; ++fld) a.out[fld * S + g] = R.ad(fld, s);
+        }
+      }
     }
     __syncthreads();
-  }
-
-  // ---- write-back (the last step's second half drift is already applied)
-  for (int s = tid; s < count; s += kThreads) {
-    const uint32_t meta = meta_s[s];
-    const int64_t g = g0 + s;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) a.out[f * S + g] = R.ad(f, s);
-    if (meta & kElem) {
-#pragma unroll
-      for (int f = 6; f < kStateFields; ++f) a.out[f * S + g] = R.ad(f, s);
-    }
   }
 }
 
@@ -321,7 +419,7 @@ template <int kCap, int kThreads, int kMinBlocks>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream) {
   const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(fRowsF) * kCap * sizeof(float) +
-                       size_t(kCap) * sizeof(uint32_t);
+                       2 * size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
@@ -338,12 +436,13 @@ cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_star
                                    int config, bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
   // the same capacities as the FP64 resident configurations (0/1: 520 slots,
-  // 2/3: 264 slots); the smaller footprint allows two CTAs per SM at 264
+  // 2/3: 264 slots); 376 B of shared memory per slot allows two CTAs per SM
+  // at 264 slots
   switch (config) {
     case 0: return launch_mixed_cfg<520, 512, 1>(args, cta_start, n_ctas, n_steps, damped, stream);
     case 1: return launch_mixed_cfg<520, 256, 1>(args, cta_start, n_ctas, n_steps, damped, stream);
     case 2: return launch_mixed_cfg<264, 256, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 3: return launch_mixed_cfg<264, 128, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
+    case 3: return launch_mixed_cfg<264, 288, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
     default: return cudaErrorInvalidValue;
   }
 }
