@@ -5,10 +5,10 @@ The compute path is libelastica_b200.so (hand-written sm_100a kernels); it is
 built in-tree by ``python -m elasticapp_b200.build`` and there is no CPU
 fallback.
 """
-from .simulator import (AnalyticalLinearDamper, Clamp, CosseratRod, CosseratRodWithoutDamping,
-                        EndTorque, GravityField, Material, PositionVerlet, RodRef, Simulator,
-                        StraightRod)
+from .simulator import (AnalyticalLinearDamper, Clamp, CollisionSystem, ContactMaterial, CosseratRod,
+                        CosseratRodWithoutDamping, EndTorque, GravityField, Material, PositionVerlet, RodRef,
+                        Simulator, StraightRod)
 from . import _lib
 
-__all__ = ["AnalyticalLinearDamper", "Clamp", "CosseratRod", "CosseratRodWithoutDamping", "EndTorque",
+__all__ = ["AnalyticalLinearDamper", "Clamp", "CollisionSystem", "ContactMaterial", "CosseratRod", "CosseratRodWithoutDamping", "EndTorque",
            "GravityField", "Material", "PositionVerlet", "RodRef", "Simulator", "StraightRod", "_lib"]

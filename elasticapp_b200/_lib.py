@@ -36,7 +36,7 @@ FIELDS = [
     "InvMassSecondMomentOfInertia", "ForceDampingRate", "TorqueDampingRate", "ElementLength",
     "ElementDilatation", "Tangent", "VoronoiDilatation", "ShearStretchStrain", "Curvature",
     "InternalStress", "InternalCouple", "InternalLoads", "InternalTorques", "Acceleration",
-    "AngularAcceleration", "ElementDimension",
+    "AngularAcceleration", "ElementDimension", "ContactForce", "ContactTorque",
 ]
 FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
 # (place, ncomp): place 0 = nodes (n+1), 1 = elements (n), 2 = Voronoi (n-1)
@@ -51,8 +51,10 @@ FIELD_SHAPE = {
     "ShearStretchStrain": (1, 3), "Curvature": (2, 3), "InternalStress": (1, 3),
     "InternalCouple": (2, 3), "InternalLoads": (0, 3), "InternalTorques": (1, 3),
     "Acceleration": (0, 3), "AngularAcceleration": (1, 3), "ElementDimension": (1, 1),
+    "ContactForce": (1, 3), "ContactTorque": (1, 3),
 }
-DERIVED_FIELDS = set(FIELDS[16:])
+DERIVED_FIELDS = set(FIELDS[16:29])
+CONTACT_FIELDS = {"ContactForce", "ContactTorque"}
 
 
 class EbConfig(ctypes.Structure):
@@ -68,6 +70,12 @@ class EbStraightRod(ctypes.Structure):
                 ("length", ctypes.c_double), ("origin", ctypes.c_double * 3),
                 ("direction", ctypes.c_double * 3), ("normal", ctypes.c_double * 3),
                 ("force_damping_rate", ctypes.c_double), ("torque_damping_rate", ctypes.c_double)]
+
+
+class EbContactMaterial(ctypes.Structure):
+    _fields_ = [("stiffness", ctypes.c_double), ("normal_damping", ctypes.c_double),
+                ("tangential_damping", ctypes.c_double), ("static_friction", ctypes.c_double),
+                ("dynamic_friction", ctypes.c_double)]
 
 
 # every entry point of include/elastica_b200.h with its ctypes signature
@@ -92,6 +100,10 @@ SIGNATURES = {
     "eb_add_gravity": ([_sim, _P(ctypes.c_double)], ctypes.c_int),
     "eb_add_end_torque": ([_sim, ctypes.c_int64, _P(ctypes.c_double)], ctypes.c_int),
     "eb_add_analytical_damper": ([_sim, ctypes.c_int64, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+    "eb_add_contact_material": ([_sim, _P(EbContactMaterial), _P(ctypes.c_int32)], ctypes.c_int),
+    "eb_add_rod_contact": ([_sim, ctypes.c_int64, ctypes.c_int32], ctypes.c_int),
+    "eb_add_contact_plane": ([_sim, _P(ctypes.c_double), _P(ctypes.c_double), ctypes.c_int32], ctypes.c_int),
+    "eb_contact_pairs": ([_sim, _P(ctypes.c_int64), ctypes.c_int64, _P(ctypes.c_int64)], ctypes.c_int),
     "eb_finalize": ([_sim], ctypes.c_int),
     "eb_step": ([_sim, _P(ctypes.c_double), ctypes.c_double, ctypes.c_int64], ctypes.c_int),
     "eb_synchronize": ([_sim], ctypes.c_int),

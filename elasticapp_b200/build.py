@@ -26,8 +26,11 @@ SOURCES = [
     ("rod_block_fp64.o", "rod_block_fp64.cu", []),
     ("rod_block_mixed.o", "rod_block_mixed.cu", []),
     ("rod_energy.o", "rod_energy.cu", []),
+    # rounded as written (no contracted multiply-adds): capsules, boxes and
+    # candidate pairs bit-identical to a scalar FP64 evaluation
+    ("contact.o", "contact.cu", ["--fmad=false"]),
 ]
-HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh"]
+HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,622 @@
+// Collision system for rods: capsules, candidate pairs, contact loads.
+//
+// Every element of a participating rod is a capsule (Systems/Customization/
+// CosseratRods/Transfer/Common.hpp:57-93): centre = mid-point of the element's
+// nodes, length = dilatation * rest length, radius = the element dimension
+// sqrt(V / (pi l)), rotation from the tangent (Utilities/Math/Orthogonal.cpp:
+// 118-129), mass-weighted node velocity and the element's angular velocity.
+// One evaluation per step, at the state after the first half drift, in
+// five stages:
+//
+//   1. capsule_kernel: capsules and their axis-aligned bounding boxes
+//      (Primitives/detail/CapsulePrimitiveBase.cpp:163-180), and the largest
+//      box extent (block max, one atomic per CTA).
+//   2. cell_kernel + scan + scatter_kernel: a uniform grid with the cell edge
+//      just above the largest extent, hashed into a power-of-two table; every
+//      capsule is filed under the cell of its box's lower corner (a counting
+//      sort by bucket).
+//   3. pairs_kernel<false> + scan + pairs_kernel<true>: every capsule tests
+//      the capsules filed in its 27 neighbouring cells, then every plane;
+//      counts first, then each capsule writes its partner list into its own
+//      segment and sorts it.  Two boxes that overlap have lower corners less
+//      than one cell apart on each axis, so the candidate set equals the
+//      exhaustive search's (Detection/Coarse/ExhaustiveSearch.hpp:322-435,
+//      closed intervals of BoundingBox.hpp:532-540), which the reference's
+//      hash grids reproduce (tests/.../Test_HashGrids.cpp).
+//   4. force_kernel: each capsule evaluates the narrow phase with every
+//      partner in ascending id order (RodCapsuleRodCapsule.hpp:70-186,
+//      CapsulePlane.hpp:60-113), the pair always oriented with the smaller id
+//      as the first body, and sums the spring-dashpot loads
+//      (LinearSpringDashpot.cpp:32-85) that act on itself.  Each pair is
+//      evaluated by both of its capsules; no atomics, so the loads are
+//      deterministic.
+//   5. the step kernel adds half the capsule force to each node and the
+//      torque, recast as Q tau, to the element (Transfer/Common.hpp:32-55).
+//
+// This file is compiled without contraction of multiply-adds, so every
+// product and sum is rounded as written; the capsules, boxes and candidate
+// pairs are then bit-identical to a scalar FP64 evaluation of the same
+// expressions.
+#include <cuda_runtime.h>
+
+#include "contact.h"
+#include "rod_math.cuh"
+
+namespace eb {
+namespace {
+
+using D3 = Vec3<double>;
+
+constexpr double kContactThreshold = 1e-8;   // Utilities/Thresholds.hpp:138
+constexpr double kParallelThreshold = 1e-8;  // Utilities/Thresholds.hpp:159
+constexpr double kFrictionThreshold = 1e-8;  // Utilities/Thresholds.hpp:149
+constexpr double kZeroLength = 1e-8;         // is_zero_length bound (Utilities/Math/Zero.hpp:46-49)
+constexpr double kCellMargin = 1.0 + 1.0 / 1048576.0;
+constexpr double kCellClamp = 1073741824.0;  // 2^30 cells from the origin
+
+constexpr int kThreads = 256;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+__device__ __forceinline__ D3 ld3(const double* p, int64_t S, int64_t s) { return {p[s], p[S + s], p[2 * S + s]}; }
+__device__ __forceinline__ void st3(double* p, int64_t S, int64_t s, D3 a) {
+  p[s] = a.x;
+  p[S + s] = a.y;
+  p[2 * S + s] = a.z;
+}
+__device__ __forceinline__ D3 mul3(double k, D3 a) { return {k * a.x, k * a.y, k * a.z}; }
+__device__ __forceinline__ D3 neg3(D3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ double norm3(D3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+// blaze::normalize: a * (1 / |a|), a zero vector stays zero
+__device__ __forceinline__ D3 normalize3(D3 a) {
+  const double len = norm3(a);
+  const double il = len != 0.0 ? 1.0 / len : 0.0;
+  return {a.x * il, a.y * il, a.z * il};
+}
+
+struct Capsule {
+  D3 c, u, vel, ww;
+  double L, r;
+};
+
+__device__ __forceinline__ Capsule load_capsule(const double* cap, int64_t S, int64_t s) {
+  Capsule k;
+  k.c = ld3(cap + kCapC * S, S, s);
+  k.L = cap[kCapL * S + s];
+  k.r = cap[kCapR * S + s];
+  k.u = ld3(cap + kCapU * S, S, s);
+  k.vel = ld3(cap + kCapVel * S, S, s);
+  k.ww = ld3(cap + kCapW * S, S, s);
+  return k;
+}
+
+__device__ __forceinline__ bool overlaps(const double alo[3], const double ahi[3], const double blo[3],
+                                         const double bhi[3]) {
+  return !(blo[0] > ahi[0] || blo[1] > ahi[1] || blo[2] > ahi[2] || bhi[0] < alo[0] || bhi[1] < alo[1] ||
+           bhi[2] < alo[2]);
+}
+
+__device__ __forceinline__ uint32_t cell_hash(int32_t cx, int32_t cy, int32_t cz) {
+  uint64_t h = static_cast<uint64_t>(static_cast<uint32_t>(cx)) * 0x9E3779B97F4A7C15ull ^
+               static_cast<uint64_t>(static_cast<uint32_t>(cy)) * 0xC2B2AE3D27D4EB4Full ^
+               static_cast<uint64_t>(static_cast<uint32_t>(cz)) * 0x165667B19E3779F9ull;
+  h ^= h >> 29;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 32;
+  return static_cast<uint32_t>(h);
+}
+
+// ---- stage 1: capsules and boxes ------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) capsule_kernel(const ContactArgs a) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  const int64_t S = a.stride;
+  double ext = 0.0;
+  bool bad = false;
+  if (s < a.n_slots && a.cap_material[s] >= 0) {
+    const double* x = a.state + kStX * S;
+    const double* v = a.state + kStV * S;
+    const double* w = a.state + kStW * S;
+    const double c = a.half_dt;
+    // positions after the first half drift (PositionVerlet.hpp:60-69) and
+    // the clamp's value constraint
+    D3 x0 = {x[s] + c * v[s], x[S + s] + c * v[S + s], x[2 * S + s] + c * v[2 * S + s]};
+    const D3 x1 = {x[s + 1] + c * v[s + 1], x[S + s + 1] + c * v[S + s + 1], x[2 * S + s + 1] + c * v[2 * S + s + 1]};
+    const uint32_t meta = a.meta[s];
+    if ((meta & kFirst) && (a.sim_flags & kSimClamp)) {
+      const RodInfo& ri = a.rods[meta >> kRodShift];
+      if (ri.flags & kRodClamp) x0 = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+    }
+    const D3 dx = x1 - x0;
+    const double l = norm3(dx);
+    const D3 t = {dx.x / l, dx.y / l, dx.z / l};
+    const double l0 = a.par[kL0 * S + s];
+    const double e = l / l0;
+    const double L = e * l0;
+    const double r = sqrt(M_1_PI * a.par[kVol * S + s] / l);
+    const D3 cen = {0.5 * (x0.x + x1.x), 0.5 * (x0.y + x1.y), 0.5 * (x0.z + x1.z)};
+    // Orthogonal.cpp:32-55 with the tangent as the third row
+    const D3 v1 = normalize3(t);
+    D3 v2 = {0.8, 0.6, 0.0};
+    D3 v3 = cross(v1, v2);
+    v2 = cross(v3, v1);
+    if (dot(v2, v2) < kZeroLength) {
+      v2 = {0.6, -0.8, 0.0};
+      v3 = normalize3(cross(v1, v2));
+      v2 = cross(v3, v1);
+    }
+    const D3 r0 = normalize3(v2), r1 = normalize3(v3), r2 = v1;
+    const double m0 = a.par[kMass * S + s], m1 = a.par[kMass * S + s + 1];
+    const D3 va = ld3(v, S, s), vb = ld3(v, S, s + 1);
+    const D3 num = mul3(m0, va) + mul3(m1, vb);
+    const double den = m0 + m1;
+    const D3 vel = {num.x / den, num.y / den, num.z / den};
+    const D3 om = ld3(w, S, s);
+    const D3 ww = {r0.x * om.x + r1.x * om.y + r2.x * om.z, r0.y * om.x + r1.y * om.y + r2.y * om.z,
+                   r0.z * om.x + r1.z * om.y + r2.z * om.z};
+    double* cap = a.cap;
+    st3(cap + kCapC * S, S, s, cen);
+    cap[kCapL * S + s] = L;
+    cap[kCapR * S + s] = r;
+    st3(cap + kCapU * S, S, s, r2);
+    st3(cap + kCapVel * S, S, s, vel);
+    st3(cap + kCapW * S, S, s, ww);
+    const double ua[3] = {r2.x, r2.y, r2.z}, ca[3] = {cen.x, cen.y, cen.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double len = fabs(ua[d] * L) * 0.5 + r + kContactThreshold;
+      const double lo = ca[d] - len, hi = ca[d] + len;
+      cap[(kCapLo + d) * S + s] = lo;
+      cap[(kCapHi + d) * S + s] = hi;
+      const double xt = hi - lo;
+      if (!(xt >= 0.0 && xt < 1e300)) bad = true;  // NaN or infinite box
+      else ext = fmax(ext, xt);
+    }
+  }
+  // block max of the extents, one atomic per CTA (non-negative doubles order
+  // like their bit patterns)
+  for (int o = 16; o > 0; o >>= 1) ext = fmax(ext, __shfl_xor_sync(0xffffffffu, ext, o));
+  __shared__ double wmax[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = ext;
+  if (bad) atomicOr(a.status, kStatusContactNonFinite);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < kThreads / 32; ++i) m = fmax(m, wmax[i]);
+    if (m > 0.0) atomicMax(a.extent_bits, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+// ---- stage 2: grid cells, counting sort by bucket --------------------------
+
+__device__ __forceinline__ double inverse_cell(const ContactArgs& a) {
+  double h = __longlong_as_double(static_cast<long long>(*a.extent_bits)) * kCellMargin;
+  if (!(h > 0.0)) h = 1.0;
+  return 1.0 / h;
+}
+
+__global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (s >= a.n_slots || a.cap_material[s] < 0) return;
+  const int64_t S = a.stride;
+  const double ih = inverse_cell(a);
+  int32_t c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double f = floor(a.cap[(kCapLo + d) * S + s] * ih);
+    f = fmin(fmax(f, -kCellClamp), kCellClamp);  // a NaN becomes -2^30 (and is flagged)
+    c[d] = static_cast<int32_t>(f);
+    a.cell[d * S + s] = c[d];
+  }
+  const uint32_t b = cell_hash(c[0], c[1], c[2]) & a.table_mask;
+  a.bucket[s] = b;
+  atomicAdd(a.bucket_count + b, 1);
+}
+
+__global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (s >= a.n_slots || a.cap_material[s] < 0) return;
+  const int64_t S = a.stride;
+  const uint32_t b = a.bucket[s];
+  // bucket_count was zeroed by the scan and now serves as the fill cursor
+  const int32_t pos = a.bucket_start[b] + atomicAdd(a.bucket_count + b, 1);
+  if (pos < 0 || pos >= a.n_caps) {  // cannot happen with consistent counts; never write out of range
+    atomicOr(a.status, kStatusContactIndex);
+    return;
+  }
+  a.sorted_id[pos] = static_cast<int32_t>(s);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    a.sorted_cell[3 * pos + d] = a.cell[d * S + s];
+    a.sorted_box[6 * pos + d] = a.cap[(kCapLo + d) * S + s];
+    a.sorted_box[6 * pos + 3 + d] = a.cap[(kCapHi + d) * S + s];
+  }
+}
+
+// ---- stage 3: candidate pairs ----------------------------------------------
+
+template <bool kWrite>
+__global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps) {
+  const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (e >= n_caps) return;
+  const int32_t id = a.sorted_id[e];
+  const int32_t cx = a.sorted_cell[3 * e], cy = a.sorted_cell[3 * e + 1], cz = a.sorted_cell[3 * e + 2];
+  double lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = a.sorted_box[6 * e + d];
+    hi[d] = a.sorted_box[6 * e + 3 + d];
+  }
+  int32_t* out = nullptr;
+  if (kWrite) {
+    const int64_t total = a.pair_offset[a.n_slots];
+    if (total > a.capacity) {
+      if (e == 0) {
+        atomicOr(a.status, kStatusPairOverflow);
+        atomicMax(a.required, static_cast<unsigned long long>(total));
+      }
+      return;
+    }
+    out = a.partners + a.pair_offset[id];  // within [0, capacity)
+  }
+  int32_t cnt = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int32_t nx = cx + dx, ny = cy + dy, nz = cz + dz;
+        const uint32_t b = cell_hash(nx, ny, nz) & a.table_mask;
+        const int32_t k0 = max(a.bucket_start[b], 0), k1 = min(a.bucket_start[b + 1], n_caps);
+        for (int32_t k = k0; k < k1; ++k) {
+          if (a.sorted_cell[3 * k] != nx || a.sorted_cell[3 * k + 1] != ny || a.sorted_cell[3 * k + 2] != nz) continue;
+          const int32_t other = a.sorted_id[k];
+          if (other == id) continue;
+          const double* bx = a.sorted_box + 6 * k;
+          if (!overlaps(lo, hi, bx, bx + 3)) continue;
+          if (kWrite) out[cnt] = other;
+          ++cnt;
+        }
+      }
+  for (int32_t p = 0; p < a.n_planes; ++p) {
+    if (!overlaps(lo, hi, a.planes[p].lo, a.planes[p].hi)) continue;
+    if (kWrite) out[cnt] = static_cast<int32_t>(a.n_slots) + p;
+    ++cnt;
+  }
+  if (!kWrite) {
+    a.pair_count[id] = cnt;
+  } else {
+    // ascending partner order (insertion sort of this capsule's segment)
+    for (int32_t i = 1; i < cnt; ++i) {
+      const int32_t v = out[i];
+      int32_t j = i - 1;
+      while (j >= 0 && out[j] > v) {
+        out[j + 1] = out[j];
+        --j;
+      }
+      out[j + 1] = v;
+    }
+  }
+}
+
+// ---- exclusive scan of int32 counts (out[n] = total), accumulated in Acc ----
+
+template <typename Acc>
+__device__ __forceinline__ Acc block_exclusive_scan(Acc v, Acc* total) {
+  __shared__ Acc warp_sums[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Acc x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const Acc y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    Acc ws = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const Acc y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  const Acc prefix = (wid > 0 ? warp_sums[wid - 1] : Acc(0)) + x - v;
+  *total = warp_sums[kScanThreads / 32 - 1];
+  __syncthreads();
+  return prefix;
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kScanThreads) scan_partial(int32_t* in, Acc* out, int64_t n, Acc* block_sums,
+                                                             bool zero_in) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kScanBlock + static_cast<int64_t>(threadIdx.x) * kScanItems;
+  Acc v[kScanItems];
+  Acc sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = base + i < n ? static_cast<Acc>(in[base + i]) : Acc(0);
+    sum += v[i];
+  }
+  Acc total;
+  Acc run = block_exclusive_scan<Acc>(sum, &total);
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) {
+      out[base + i] = run;
+      if (zero_in) in[base + i] = 0;
+    }
+    run += v[i];
+  }
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kScanThreads) scan_top(Acc* block_sums, int64_t nb, Acc* out, int64_t n) {
+  Acc carry = 0;
+  for (int64_t base = 0; base < nb; base += kScanThreads) {
+    const int64_t i = base + threadIdx.x;
+    const Acc v = i < nb ? block_sums[i] : Acc(0);
+    Acc total;
+    const Acc pre = block_exclusive_scan<Acc>(v, &total);
+    if (i < nb) block_sums[i] = carry + pre;
+    carry += total;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kScanThreads) scan_add(Acc* out, int64_t n, const Acc* block_sums) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kScanBlock + static_cast<int64_t>(threadIdx.x) * kScanItems;
+  const Acc add = block_sums[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < n) out[base + i] += add;
+}
+
+template <typename Acc>
+cudaError_t exclusive_scan(int32_t* in, Acc* out, int64_t n, Acc* block_sums, bool zero_in, cudaStream_t stream,
+                           int64_t* launches) {
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if (nb > 0)
+    scan_partial<Acc><<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(in, out, n, block_sums, zero_in);
+  scan_top<Acc><<<1, kScanThreads, 0, stream>>>(block_sums, nb, out, n);
+  if (nb > 0) scan_add<Acc><<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(out, n, block_sums);
+  *launches += nb > 0 ? 3 : 1;
+  return cudaGetLastError();
+}
+
+// ---- stage 4: narrow phase and spring-dashpot loads ------------------------
+
+struct ContactPoint {
+  D3 pos, n;
+  double dist;
+};
+
+// Utilities/Geometry/GetClosestLineSegmentPoints.cpp, branch for branch
+__device__ void closest_segment_points(D3 a1, D3 a2, D3 b1, D3 b2, D3& cp1, D3& cp2) {
+  const D3 a1a2 = a2 - a1, b1b2 = b2 - b1, a1b1 = b1 - a1;
+  const double da1 = dot(a1a2, a1b1), db1 = dot(b1b2, a1b1);
+  if (da1 <= 0.0 && db1 >= 0.0) {
+    cp1 = a1;
+    cp2 = b1;
+    return;
+  }
+  const D3 a1b2 = b2 - a1;
+  const double da2 = dot(a1a2, a1b2), db2 = dot(b1b2, a1b2);
+  if (da2 <= 0.0 && db2 <= 0.0) {
+    cp1 = a1;
+    cp2 = b2;
+    return;
+  }
+  const D3 a2b1 = b1 - a2;
+  const double da3 = dot(a1a2, a2b1), db3 = dot(b1b2, a2b1);
+  if (da3 >= 0.0 && db3 >= 0.0) {
+    cp1 = a2;
+    cp2 = b1;
+    return;
+  }
+  const D3 a2b2 = b2 - a2;
+  const double da4 = dot(a1a2, a2b2), db4 = dot(b1b2, a2b2);
+  if (da4 >= 0.0 && db4 <= 0.0) {
+    cp1 = a2;
+    cp2 = b2;
+    return;
+  }
+  const double la = dot(a1a2, a1a2);
+  if (da1 >= -kParallelThreshold && da3 <= kParallelThreshold) {
+    const D3 k = mul3(da1 / la, a1a2);
+    const D3 n = a1b1 - k;
+    if (dot(b1b2, n) >= -kParallelThreshold) {
+      cp1 = a1 + k;
+      cp2 = b1;
+      return;
+    }
+  }
+  if (da2 >= -kParallelThreshold && da4 <= kParallelThreshold) {
+    const D3 k = mul3(da2 / la, a1a2);
+    const D3 n = a1b2 - k;
+    if (dot(b1b2, n) <= kParallelThreshold) {
+      cp1 = a1 + k;
+      cp2 = b2;
+      return;
+    }
+  }
+  const double lb = dot(b1b2, b1b2);
+  if (db1 <= kParallelThreshold && db2 >= -kParallelThreshold) {
+    const D3 k = mul3(-db1 / lb, b1b2);
+    const D3 n = neg3(a1b1) - k;
+    if (dot(a1a2, n) >= -kParallelThreshold) {
+      cp1 = a1;
+      cp2 = b1 + k;
+      return;
+    }
+  }
+  if (db3 <= kParallelThreshold && db4 >= -kParallelThreshold) {
+    const D3 k = mul3(-db3 / lb, b1b2);
+    const D3 n = neg3(a2b1) - k;
+    if (dot(a1a2, n) <= kParallelThreshold) {
+      cp1 = a2;
+      cp2 = b1 + k;
+      return;
+    }
+  }
+  const double sc = dot(a1a2, b1b2);
+  double div = la * lb - sc * sc;
+  div = 1.0 / div;
+  const double sp = (lb * da1 - sc * db1) * div;
+  const double tp = (sc * da1 - la * db1) * div;
+  cp1 = a1 + mul3(sp, a1a2);
+  cp2 = b1 + mul3(tp, b1b2);
+}
+
+// RodCapsuleRodCapsule.hpp:70-186 (c1 has the smaller id)
+__device__ int rod_capsule_contacts(const Capsule& c1, const Capsule& c2, ContactPoint out[2]) {
+  const D3 up1 = mul3(0.5 * c1.L, c1.u), up2 = mul3(0.5 * c2.L, c2.u);
+  D3 cp1, cp2;
+  closest_segment_points(c1.c + up1, c1.c - up1, c2.c + up2, c2.c - up2, cp1, cp2);
+  D3 nrm = cp1 - cp2;
+  const double ln = norm3(nrm);
+  if (ln < kContactThreshold) return 0;
+  const double dist = ln - c1.r - c2.r;
+  if (!(dist < kContactThreshold)) return 0;
+  nrm = normalize3(nrm);
+  const double c2x = dot(c1.u, c2.c - c1.c);
+  if ((fabs(dot(c1.u, c2.u)) - 1.0) > -kParallelThreshold && fabs(c2x) < c1.L) {
+    const double hl1 = 0.5 * c1.L, hl2 = 0.5 * c2.L;
+    if (hl1 < c2x + hl2) {
+      const double k = c1.r + 0.5 * dist;
+      out[0] = {(c1.c + up1) - mul3(k, nrm), nrm, dist};
+    } else {
+      const double k = c2.r + 0.5 * dist;
+      out[0] = {(c2.c + mul3(hl2, c1.u)) + mul3(k, nrm), nrm, dist};
+    }
+    if (-hl1 > c2x - hl2) {
+      const double k = c1.r + 0.5 * dist;
+      out[1] = {(c1.c - up1) - mul3(k, nrm), nrm, dist};
+    } else {
+      const double k = c2.r + 0.5 * dist;
+      out[1] = {(c2.c - mul3(hl2, c1.u)) + mul3(k, nrm), nrm, dist};
+    }
+    return 2;
+  }
+  const double k = c2.r + 0.5 * dist;
+  out[0] = {cp2 + mul3(k, nrm), nrm, dist};
+  return 1;
+}
+
+// CapsulePlane.hpp:60-113
+__device__ int capsule_plane_contacts(const Capsule& c, const ContactPlane& p, ContactPoint out[2]) {
+  const D3 up = mul3(0.5 * c.L, c.u);
+  const D3 pu = c.c + up, pl = c.c - up;
+  const D3 pp = {p.p[0], p.p[1], p.p[2]}, n = {p.n[0], p.n[1], p.n[2]};
+  const double du = fabs(dot(n, pu - pp)) - c.r;
+  const double dl = fabs(dot(n, pl - pp)) - c.r;
+  int k = 0;
+  if (du < kContactThreshold) out[k++] = {pu - mul3(c.r + du, n), n, du};
+  if (dl < kContactThreshold) out[k++] = {pl - mul3(c.r + dl, n), n, dl};
+  return k;
+}
+
+__device__ __forceinline__ D3 point_velocity(const Capsule& k, D3 pos) { return k.vel + cross(k.ww, pos - k.c); }
+
+// Contact.cpp:150-215 and LinearSpringDashpot.cpp:32-85; false: separated
+__device__ bool spring_dashpot(const ContactPoint& ct, D3 rvel, const ContactPair& pm, D3& net) {
+  if (!(ct.dist < -kContactThreshold)) return false;
+  const D3 n = ct.n;
+  const double rvn = dot(n, rvel);
+  const double rvt = dot(n, rvel - mul3(rvn, n));
+  const double mu = fabs(rvt) > kFrictionThreshold ? pm.mu_d : pm.mu_s;
+  const double delta = -ct.dist;
+  const double relvn = -dot(n, rvel);
+  const D3 relvt = neg3(rvel) - mul3(relvn, n);
+  const double fn = fmax(0.0, pm.k * delta + pm.cn * relvn);
+  const double ft = fmin(pm.ct * norm3(relvt), mu * fn);
+  net = mul3(fn, n) + mul3(ft, normalize3(relvt));
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads) force_kernel(const ContactArgs a) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (s >= a.n_slots) return;
+  const int32_t mat = a.cap_material[s];
+  if (mat < 0) return;
+  const int64_t S = a.stride;
+  D3 F = {0.0, 0.0, 0.0}, T = {0.0, 0.0, 0.0};
+  const int64_t total = a.pair_offset[a.n_slots];
+  if (total <= a.capacity) {
+    const Capsule me = load_capsule(a.cap, S, s);
+    const int64_t k0 = a.pair_offset[s], k1 = a.pair_offset[s + 1];
+    ContactPoint pts[2];
+    for (int64_t k = k0; k < k1; ++k) {
+      const int64_t o = a.partners[k];
+      if (o >= 0 && o < a.n_slots) {
+        const int32_t om = a.cap_material[o];
+        if (om < 0) continue;
+        const bool first = s < o;
+        const Capsule other = load_capsule(a.cap, S, o);
+        const Capsule& c1 = first ? me : other;
+        const Capsule& c2 = first ? other : me;
+        const ContactPair pm = a.pair_table[(first ? mat : om) * a.n_materials + (first ? om : mat)];
+        const int np = rod_capsule_contacts(c1, c2, pts);
+        for (int i = 0; i < np; ++i) {
+          const D3 rvel = point_velocity(c1, pts[i].pos) - point_velocity(c2, pts[i].pos);
+          D3 net;
+          if (!spring_dashpot(pts[i], rvel, pm, net)) continue;
+          // RigidBodyPrimitive.hpp:500-504 add_force_at_position
+          const D3 f = first ? net : neg3(net);
+          F = F + f;
+          T = T + cross(pts[i].pos - me.c, f);
+        }
+      } else if (o >= a.n_slots && o < a.n_slots + a.n_planes) {
+        const ContactPlane& P = a.planes[o - a.n_slots];
+        const ContactPair pm = a.pair_table[mat * a.n_materials + P.material];
+        const int np = capsule_plane_contacts(me, P, pts);
+        for (int i = 0; i < np; ++i) {
+          const D3 rvel = point_velocity(me, pts[i].pos) - D3{0.0, 0.0, 0.0};  // the plane is fixed
+          D3 net;
+          if (!spring_dashpot(pts[i], rvel, pm, net)) continue;
+          F = F + net;
+          T = T + cross(pts[i].pos - me.c, net);
+        }
+      }
+    }
+  }
+  st3(a.cf, S, s, F);
+  st3(a.ct, S, s, T);
+}
+
+}  // namespace
+
+int64_t contact_scan_blocks(int64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* launches) {
+  if (a.n_slots <= 0) return cudaSuccess;
+  const unsigned gs = static_cast<unsigned>((a.n_slots + kThreads - 1) / kThreads);
+  cudaError_t e = cudaMemsetAsync(a.extent_bits, 0, sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return e;
+  // the bucket counts: the scatter of the previous evaluation left them at
+  // the bucket sizes
+  const int64_t table = static_cast<int64_t>(a.table_mask) + 1;
+  e = cudaMemsetAsync(a.bucket_count, 0, static_cast<size_t>(table) * sizeof(int32_t), stream);
+  if (e != cudaSuccess) return e;
+  capsule_kernel<<<gs, kThreads, 0, stream>>>(a);
+  cell_kernel<<<gs, kThreads, 0, stream>>>(a);
+  *launches += 2;
+  e = exclusive_scan<int32_t>(a.bucket_count, a.bucket_start, table, reinterpret_cast<int32_t*>(a.scan_blocks), true,
+                             stream, launches);
+  if (e != cudaSuccess) return e;
+  scatter_kernel<<<gs, kThreads, 0, stream>>>(a);
+  const unsigned ge = static_cast<unsigned>((a.n_caps + kThreads - 1) / kThreads);
+  if (ge > 0) pairs_kernel<false><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
+  *launches += 2;
+  e = exclusive_scan<int64_t>(a.pair_count, a.pair_offset, a.n_slots, a.scan_blocks, false, stream, launches);
+  if (e != cudaSuccess) return e;
+  if (ge > 0) pairs_kernel<true><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
+  force_kernel<<<gs, kThreads, 0, stream>>>(a);
+  *launches += 2;
+  return cudaGetLastError();
+}
+
+}  // namespace eb

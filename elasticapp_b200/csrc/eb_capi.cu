@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/elastica_b200.h"
+#include "contact.h"
 #include "eb_internal.h"
 
 namespace eb {
@@ -51,7 +52,7 @@ eb_status fail(eb_status s, const std::string& msg) {
   } while (0)
 
 enum Place { kNode = 0, kElement = 1, kVoronoi = 2 };
-enum Kind { kState = 0, kParam = 1, kDiag = 2 };
+enum Kind { kState = 0, kParam = 1, kDiag = 2, kContactLoad = 3 };
 
 struct FieldInfo {
   Place place;
@@ -90,6 +91,8 @@ const FieldInfo kFields[EB_FIELD_COUNT] = {
     {kNode, 3, kDiag, eb::kDAccel},         // EB_ACCELERATION
     {kElement, 3, kDiag, eb::kDAlpha},      // EB_ANGULAR_ACCELERATION
     {kElement, 1, kDiag, eb::kDDim},        // EB_ELEMENT_DIMENSION
+    {kElement, 3, kContactLoad, 0},         // EB_CONTACT_FORCE
+    {kElement, 3, kContactLoad, 3},         // EB_CONTACT_TORQUE
 };
 
 int64_t place_count(Place p, int64_t n) { return p == kNode ? n + 1 : (p == kElement ? n : n - 1); }
@@ -101,6 +104,35 @@ struct RodHost {
   std::vector<double> state, param, diag;
   eb::RodInfo info{};
   double damper_nu_t = 0.0;
+  int32_t contact_material = -1;  // collision-system material, -1: no contact
+};
+
+// device side of the collision system
+struct ContactDevice {
+  bool on = false;
+  int32_t n_caps = 0;
+  uint32_t table_mask = 0;
+  int64_t capacity = 0;
+  double* cap = nullptr;
+  int32_t* cap_material = nullptr;
+  unsigned long long* extent = nullptr;
+  int32_t* cell = nullptr;
+  uint32_t* bucket = nullptr;
+  int32_t* bucket_count = nullptr;
+  int32_t* bucket_start = nullptr;
+  int32_t* sorted_id = nullptr;
+  int32_t* sorted_cell = nullptr;
+  double* sorted_box = nullptr;
+  int32_t* pair_count = nullptr;
+  int64_t* pair_offset = nullptr;
+  int32_t* partners = nullptr;
+  unsigned long long* required = nullptr;
+  eb::ContactPlane* planes = nullptr;
+  eb::ContactPair* pair_table = nullptr;
+  double* loads = nullptr;  // 6 x stride: force rows 0-2, torque rows 3-5
+  int64_t* scan_blocks = nullptr;
+  double* backup = nullptr;  // state at the start of a step chunk
+  bool evaluated = false;
 };
 
 }  // namespace
@@ -135,6 +167,10 @@ struct eb_sim {
   std::vector<int64_t*> d_cta_start;  // per block configuration (or null)
   std::vector<int> n_ctas;
   float plan_ms[16] = {0};
+  // collision system
+  std::vector<eb_contact_material> materials;
+  std::vector<eb::ContactPlane> planes;
+  ContactDevice contact;
 };
 
 namespace {
@@ -276,6 +312,8 @@ eb_status rod_field_check(const eb_sim* s, int64_t rod, int32_t field, int64_t c
 }
 
 double* device_base(eb_sim* s, const FieldInfo& f) {
+  if (f.kind == kContactLoad)
+    return s->contact.loads ? s->contact.loads + static_cast<int64_t>(f.offset) * s->stride : nullptr;
   double* base = f.kind == kState ? s->d_state[s->cur] : (f.kind == kParam ? s->d_param : s->d_diag);
   return base ? base + static_cast<int64_t>(f.offset) * s->stride : nullptr;
 }
@@ -294,6 +332,13 @@ void host_free(eb_sim* s) {
   for (auto* p : s->d_cta_start)
     if (p) cudaFree(p);
   s->d_cta_start.clear();
+  ContactDevice& c = s->contact;
+  void* cptrs[] = {c.cap, c.cap_material, c.extent, c.cell, c.bucket, c.bucket_count, c.bucket_start,
+                   c.sorted_id, c.sorted_cell, c.sorted_box, c.pair_count, c.pair_offset, c.partners,
+                   c.required, c.planes, c.pair_table, c.loads, c.scan_blocks, c.backup};
+  for (void* p : cptrs)
+    if (p) cudaFree(p);
+  c = ContactDevice{};
   s->d_state[0] = s->d_state[1] = s->d_param = s->d_diag = s->d_energy = nullptr;
   s->d_meta = nullptr;
   s->d_rods = nullptr;
@@ -308,6 +353,10 @@ eb_status check_device_status(eb_sim* s) {
   EB_CUDA(cudaStreamSynchronize(s->stream));
   if (st & eb::kStatusCopyTimeout)
     return fail(EB_ERR_CUDA, "a step kernel gave up waiting for its bulk copies (bounded wait expired)");
+  if (st & eb::kStatusContactNonFinite)
+    return fail(EB_ERR_NUMERICAL, "a capsule's bounding box was not finite: the state has diverged");
+  if (st & eb::kStatusContactIndex)
+    return fail(EB_ERR_CUDA, "the contact grid produced an out-of-range index (skipped)");
   return EB_OK;
 }
 
@@ -315,6 +364,120 @@ eb_status upload_rod_table(eb_sim* s) {
   std::vector<eb::RodInfo> info(s->rods.size());
   for (size_t r = 0; r < s->rods.size(); ++r) info[r] = s->rods[r].info;
   EB_CUDA(cudaMemcpyAsync(s->d_rods, info.data(), info.size() * sizeof(eb::RodInfo),
+                          cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+// ---- collision system set-up ------------------------------------------------
+
+struct H3 {
+  double x, y, z;
+};
+H3 h_cross(H3 a, H3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+double h_dot(H3 a, H3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// blaze::normalize: a * (1 / |a|), a zero vector stays zero
+H3 h_normalize(H3 a) {
+  const double len = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  const double il = len != 0.0 ? 1.0 / len : 0.0;
+  return {a.x * il, a.y * il, a.z * il};
+}
+
+// PlanePrimitive from a normal (PlanePrimitive.cpp:60-130): rotation rows
+// from make_orthogonal_bases_from_normal (Utilities/Math/Orthogonal.cpp:32-55,
+// 85-96) and the bounding box of the default 1e40 spans (PlanePrimitive.cpp:179-236)
+eb::ContactPlane make_plane(const double point[3], const double normal[3], int32_t material) {
+  const H3 v1 = h_normalize({normal[0], normal[1], normal[2]});
+  H3 v2 = {0.8, 0.6, 0.0};
+  H3 v3 = h_cross(v1, v2);
+  v2 = h_cross(v3, v1);
+  if (h_dot(v2, v2) < 1e-8) {  // is_zero_length with blaze::accuracy
+    v2 = {0.6, -0.8, 0.0};
+    v3 = h_normalize(h_cross(v1, v2));
+    v2 = h_cross(v3, v1);
+  }
+  const H3 b = h_normalize(v2), t = h_normalize(v3);
+  eb::ContactPlane P{};
+  const double bb[3] = {b.x, b.y, b.z}, tt[3] = {t.x, t.y, t.z};
+  const double n[3] = {v1.x, v1.y, v1.z};
+  for (int d = 0; d < 3; ++d) {
+    P.p[d] = point[d];
+    P.n[d] = n[d];
+    const double len = 0.5 * (std::fabs(bb[d] * 1e40) + std::fabs(tt[d] * 1e40)) + 1e-8;
+    P.lo[d] = point[d] - len;
+    P.hi[d] = point[d] + len;
+  }
+  P.material = material;
+  return P;
+}
+
+eb_status setup_contact(eb_sim* s) {
+  ContactDevice& c = s->contact;
+  const int64_t S = s->stride, nr = static_cast<int64_t>(s->rods.size());
+  std::vector<int32_t> cap_mat(static_cast<size_t>(S), -1);
+  int64_t n_caps = 0;
+  for (int64_t r = 0; r < nr; ++r) {
+    const RodHost& R = s->rods[r];
+    if (R.contact_material < 0) continue;
+    for (int64_t i = 0; i < R.n; ++i) cap_mat[static_cast<size_t>(s->offsets[r] + i)] = R.contact_material;
+    n_caps += R.n;
+  }
+  if (n_caps == 0) return EB_OK;
+  if (s->cfg.precision == EB_PRECISION_MIXED)
+    return fail(EB_ERR_UNSUPPORTED, "the collision system runs on the FP64 streaming step only");
+  if (s->n_slots + static_cast<int64_t>(s->planes.size()) >= (int64_t(1) << 31) - 1)
+    return fail(EB_ERR_UNSUPPORTED, "too many slots for the collision system's 32-bit ids");
+  c.on = true;
+  c.n_caps = static_cast<int32_t>(n_caps);
+  int64_t table = 1024;
+  while (table < 2 * n_caps) table <<= 1;
+  c.table_mask = static_cast<uint32_t>(table - 1);
+  c.capacity = std::max<int64_t>(int64_t(1) << 16, 24 * n_caps);
+  const size_t nm = s->materials.size();
+  std::vector<eb::ContactPair> pairs(nm * nm);
+  for (size_t i = 0; i < nm; ++i)
+    for (size_t j = 0; j < nm; ++j) {
+      const eb_contact_material& a = s->materials[i];
+      const eb_contact_material& b = s->materials[j];
+      pairs[i * nm + j] = {1.0 / (1.0 / a.stiffness + 1.0 / b.stiffness),
+                           1.0 / (1.0 / a.normal_damping + 1.0 / b.normal_damping),
+                           1.0 / (1.0 / a.tangential_damping + 1.0 / b.tangential_damping),
+                           a.static_friction + b.static_friction, a.dynamic_friction + b.dynamic_friction};
+    }
+  const int64_t scan_blocks = eb::contact_scan_blocks(std::max<int64_t>(table, s->n_slots + 1));
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](auto** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s->stream);
+  };
+  alloc(&c.cap, static_cast<size_t>(eb::kCapRows * S) * sizeof(double));
+  alloc(&c.cap_material, static_cast<size_t>(S) * sizeof(int32_t));
+  alloc(&c.extent, sizeof(unsigned long long));
+  alloc(&c.cell, static_cast<size_t>(3 * S) * sizeof(int32_t));
+  alloc(&c.bucket, static_cast<size_t>(S) * sizeof(uint32_t));
+  alloc(&c.bucket_count, static_cast<size_t>(table) * sizeof(int32_t));
+  alloc(&c.bucket_start, static_cast<size_t>(table + 1) * sizeof(int32_t));
+  alloc(&c.sorted_id, static_cast<size_t>(n_caps) * sizeof(int32_t));
+  alloc(&c.sorted_cell, static_cast<size_t>(3 * n_caps) * sizeof(int32_t));
+  alloc(&c.sorted_box, static_cast<size_t>(6 * n_caps) * sizeof(double));
+  alloc(&c.pair_count, static_cast<size_t>(S) * sizeof(int32_t));
+  alloc(&c.pair_offset, static_cast<size_t>(s->n_slots + 1) * sizeof(int64_t));
+  alloc(&c.partners, static_cast<size_t>(c.capacity) * sizeof(int32_t));
+  alloc(&c.required, sizeof(unsigned long long));
+  alloc(&c.planes, std::max<size_t>(1, s->planes.size()) * sizeof(eb::ContactPlane));
+  alloc(&c.pair_table, std::max<size_t>(1, pairs.size()) * sizeof(eb::ContactPair));
+  alloc(&c.loads, static_cast<size_t>(6 * S) * sizeof(double));
+  alloc(&c.scan_blocks, static_cast<size_t>(scan_blocks) * sizeof(int64_t));
+  alloc(&c.backup, static_cast<size_t>(eb::kStateFields * S) * sizeof(double));
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA,
+                std::string("collision system allocation: ") + cudaGetErrorString(e));
+  EB_CUDA(cudaMemcpyAsync(c.cap_material, cap_mat.data(), cap_mat.size() * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s->stream));
+  if (!s->planes.empty())
+    EB_CUDA(cudaMemcpyAsync(c.planes, s->planes.data(), s->planes.size() * sizeof(eb::ContactPlane),
+                            cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(c.pair_table, pairs.data(), pairs.size() * sizeof(eb::ContactPair),
                           cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
   return EB_OK;
@@ -436,6 +599,7 @@ EB_API eb_status eb_set_field(eb_sim* s, int64_t rod, int32_t field, const doubl
   if (eb_status st = rod_field_check(s, rod, field, count, &fi, &expected)) return st;
   RodHost& r = s->rods[rod];
   const int64_t per = place_count(fi->place, r.n);
+  if (fi->kind == kContactLoad) return fail(EB_ERR_UNSUPPORTED, "contact loads are read only");
   if (!s->finalized) {
     std::vector<double>& buf = fi->kind == kState ? r.state : (fi->kind == kParam ? r.param : r.diag);
     for (int c = 0; c < fi->ncomp; ++c)
@@ -467,6 +631,8 @@ EB_API eb_status eb_get_field(eb_sim* s, int64_t rod, int32_t field, double* val
   if (eb_status st = rod_field_check(s, rod, field, count, &fi, &expected)) return st;
   const RodHost& r = s->rods[rod];
   const int64_t per = place_count(fi->place, r.n);
+  if (fi->kind == kContactLoad && !s->finalized)
+    return fail(EB_ERR_INVALID_STATE, "contact loads exist after eb_finalize");
   if (!s->finalized) {
     const std::vector<double>& buf = fi->kind == kState ? r.state : (fi->kind == kParam ? r.param : r.diag);
     for (int c = 0; c < fi->ncomp; ++c)
@@ -476,7 +642,9 @@ EB_API eb_status eb_get_field(eb_sim* s, int64_t rod, int32_t field, double* val
   }
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, *fi);
-  if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  if (!base)
+    return fail(EB_ERR_UNSUPPORTED, fi->kind == kContactLoad ? "no rod takes part in contact"
+                                                              : "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
   EB_CUDA(cudaMemcpy2DAsync(values, per * sizeof(double), base + s->offsets[rod],
                             s->stride * sizeof(double), per * sizeof(double), fi->ncomp,
                             cudaMemcpyDeviceToHost, s->stream));
@@ -490,6 +658,7 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
   if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "batch access needs a finalized simulator");
   if (field < 0 || field >= EB_FIELD_COUNT) return fail(EB_ERR_INVALID_ARGUMENT, "unknown field");
   const FieldInfo& fi = kFields[field];
+  if (fi.kind == kContactLoad && to_device) return fail(EB_ERR_UNSUPPORTED, "contact loads are read only");
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, fi);
   if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
@@ -603,6 +772,49 @@ EB_API eb_status eb_add_analytical_damper(eb_sim* s, int64_t rod, double transla
   return EB_OK;
 }
 
+EB_API eb_status eb_add_contact_material(eb_sim* s, const eb_contact_material* m, int32_t* material_id) {
+  if (check_sim(s) || !m) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add materials after finalize");
+  // Materials.cpp:237-283 argument checks
+  if (!(m->stiffness > 0.0) || !std::isfinite(m->stiffness)) return fail(EB_ERR_INVALID_ARGUMENT, "Invalid stiffness");
+  if (!(m->normal_damping >= 0.0) || !(m->tangential_damping >= 0.0) || !std::isfinite(m->normal_damping) ||
+      !std::isfinite(m->tangential_damping))
+    return fail(EB_ERR_INVALID_ARGUMENT, "Invalid damping coefficients");
+  if (!(m->static_friction >= 0.0) || !(m->dynamic_friction >= 0.0) || !std::isfinite(m->static_friction) ||
+      !std::isfinite(m->dynamic_friction))
+    return fail(EB_ERR_INVALID_ARGUMENT, "Invalid coefficient of friction");
+  if (s->materials.size() >= 4096) return fail(EB_ERR_UNSUPPORTED, "too many contact materials");
+  s->materials.push_back(*m);
+  if (material_id) *material_id = static_cast<int32_t>(s->materials.size() - 1);
+  return EB_OK;
+}
+
+EB_API eb_status eb_add_rod_contact(eb_sim* s, int64_t rod, int32_t material_id) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add contact after finalize");
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  if (material_id < 0 || material_id >= static_cast<int32_t>(s->materials.size()))
+    return fail(EB_ERR_NOT_FOUND, "unknown contact material");
+  s->rods[rod].contact_material = material_id;
+  return EB_OK;
+}
+
+EB_API eb_status eb_add_contact_plane(eb_sim* s, const double point[3], const double normal[3],
+                                      int32_t material_id) {
+  if (check_sim(s) || !point || !normal) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add planes after finalize");
+  if (material_id < 0 || material_id >= static_cast<int32_t>(s->materials.size()))
+    return fail(EB_ERR_NOT_FOUND, "unknown contact material");
+  for (int d = 0; d < 3; ++d)
+    if (!std::isfinite(point[d]) || !std::isfinite(normal[d]))
+      return fail(EB_ERR_INVALID_ARGUMENT, "plane point and normal must be finite");
+  if (normal[0] == 0.0 && normal[1] == 0.0 && normal[2] == 0.0)
+    return fail(EB_ERR_INVALID_ARGUMENT, "zero plane normal");
+  if (s->planes.size() >= 4096) return fail(EB_ERR_UNSUPPORTED, "too many planes");
+  s->planes.push_back(make_plane(point, normal, material_id));
+  return EB_OK;
+}
+
 EB_API eb_status eb_finalize(eb_sim* s) {
   if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
   if (s->finalized) return fail(EB_ERR_INVALID_STATE, "already finalized");
@@ -669,6 +881,10 @@ EB_API eb_status eb_finalize(eb_sim* s) {
                           cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(uint32_t), s->stream));
   s->cur = 0;
+  if (eb_status st = setup_contact(s)) {
+    host_free(s);
+    return st;
+  }
   s->finalized = true;
   if (eb_status st = upload_rod_table(s)) return st;
   EB_CUDA(cudaStreamSynchronize(s->stream));
@@ -750,7 +966,9 @@ eb_status build_block_worklists(eb_sim* s) {
 // timing each for kProbeSteps steps from the current state into the spare
 // buffer (the current state is left untouched).
 eb_status plan_steps(eb_sim* s, double dt) {
-  const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0;
+  // contact needs a global exchange every step: the streaming kernel
+  const bool force_stream =
+      (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 || s->contact.on;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -812,6 +1030,100 @@ eb_status plan_steps(eb_sim* s, double dt) {
   return check_device_status(s);
 }
 
+constexpr int64_t kContactChunk = 32;  // steps between checks of the pair buffer
+
+eb::ContactArgs contact_args(eb_sim* s, double dt) {
+  ContactDevice& c = s->contact;
+  eb::ContactArgs a{};
+  a.stride = s->stride;
+  a.n_slots = s->n_slots;
+  a.par = s->d_param;
+  a.meta = s->d_meta;
+  a.rods = s->d_rods;
+  a.cap_material = c.cap_material;
+  a.half_dt = 0.5 * dt;
+  a.sim_flags = s->sim_flags;
+  a.cap = c.cap;
+  a.extent_bits = c.extent;
+  a.cell = c.cell;
+  a.bucket = c.bucket;
+  a.table_mask = c.table_mask;
+  a.bucket_count = c.bucket_count;
+  a.bucket_start = c.bucket_start;
+  a.sorted_id = c.sorted_id;
+  a.sorted_cell = c.sorted_cell;
+  a.sorted_box = c.sorted_box;
+  a.pair_count = c.pair_count;
+  a.pair_offset = c.pair_offset;
+  a.partners = c.partners;
+  a.capacity = c.capacity;
+  a.required = c.required;
+  a.planes = c.planes;
+  a.n_planes = static_cast<int32_t>(s->planes.size());
+  a.n_materials = static_cast<int32_t>(s->materials.size());
+  a.pair_table = c.pair_table;
+  a.cf = c.loads;
+  a.ct = c.loads + 3 * s->stride;
+  a.n_caps = c.n_caps;
+  a.scan_blocks = c.scan_blocks;
+  a.status = s->d_status;
+  return a;
+}
+
+// Steps with the collision system, in chunks: the chunk's starting state is
+// kept, and a chunk whose candidate pairs overflowed the partner buffer is
+// run again from it with a larger buffer.
+eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
+  ContactDevice& c = s->contact;
+  const size_t state_bytes = static_cast<size_t>(eb::kStateFields * s->stride) * sizeof(double);
+  eb::StepArgs a = step_args(s, dt);
+  a.contact_force = c.loads;
+  a.contact_torque = c.loads + 3 * s->stride;
+  int64_t done = 0;
+  int regrowths = 0;
+  while (done < n_steps) {
+    const int64_t k = std::min<int64_t>(kContactChunk, n_steps - done);
+    const int c0 = s->cur;
+    EB_CUDA(cudaMemcpyAsync(c.backup, s->d_state[c0], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+    eb::ContactArgs ca = contact_args(s, dt);
+    for (int64_t i = 0; i < k; ++i) {
+      ca.state = s->d_state[s->cur];
+      EB_CUDA(eb::launch_contact(ca, s->stream, &s->launches));
+      a.in = s->d_state[s->cur];
+      a.out = s->d_state[s->cur ^ 1];
+      EB_CUDA(launch_streaming(s, a, diag && done + i == n_steps - 1));
+      s->cur ^= 1;
+      ++s->launches;
+    }
+    uint32_t st = 0;
+    unsigned long long req = 0;
+    EB_CUDA(cudaMemcpyAsync(&st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    EB_CUDA(cudaMemcpyAsync(&req, c.required, sizeof(req), cudaMemcpyDeviceToHost, s->stream));
+    EB_CUDA(cudaStreamSynchronize(s->stream));
+    if (st & eb::kStatusPairOverflow) {
+      if (++regrowths > 8) return fail(EB_ERR_OUT_OF_MEMORY, "candidate pair buffer keeps overflowing");
+      const int64_t want = std::max<int64_t>(2 * c.capacity, static_cast<int64_t>(req) + req / 2);
+      if (want >= (int64_t(1) << 31)) return fail(EB_ERR_UNSUPPORTED, "more than 2^31 candidate pairs");
+      EB_CUDA(cudaFree(c.partners));
+      c.partners = nullptr;
+      EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.partners), static_cast<size_t>(want) * sizeof(int32_t)));
+      EB_CUDA(cudaMemsetAsync(c.partners, 0, static_cast<size_t>(want) * sizeof(int32_t), s->stream));
+      c.capacity = want;
+      const uint32_t cleared = st & ~static_cast<uint32_t>(eb::kStatusPairOverflow);
+      EB_CUDA(cudaMemcpyAsync(s->d_status, &cleared, sizeof(cleared), cudaMemcpyHostToDevice, s->stream));
+      EB_CUDA(cudaMemsetAsync(c.required, 0, sizeof(unsigned long long), s->stream));
+      EB_CUDA(cudaMemcpyAsync(s->d_state[c0], c.backup, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+      EB_CUDA(cudaStreamSynchronize(s->stream));
+      s->cur = c0;
+      continue;
+    }
+    c.evaluated = true;
+    if (st) return check_device_status(s);
+    done += k;
+  }
+  return EB_OK;
+}
+
 }  // namespace
 
 EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
@@ -831,8 +1143,17 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   }
   if (s->plan_mode == 0)
     if (eb_status st = plan_steps(s, dt)) return st;
-  eb::StepArgs a = step_args(s, dt);
   const bool diag = s->d_diag != nullptr;
+  if (s->contact.on) {
+    if (eb_status st = step_with_contact(s, dt, n_steps, diag)) return st;
+    if (time)
+      for (int64_t k = 0; k < n_steps; ++k) {
+        *time += 0.5 * dt;
+        *time += 0.5 * dt;
+      }
+    return EB_OK;
+  }
+  eb::StepArgs a = step_args(s, dt);
   int64_t done = 0;
   if (s->plan_mode == 2) {
     // resident kernel in chunks; the last step of a call that records
@@ -864,6 +1185,39 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     }
   }
   return EB_OK;
+}
+
+EB_API eb_status eb_contact_pairs(eb_sim* s, int64_t* pairs, int64_t capacity, int64_t* count) {
+  if (check_sim(s) || !count) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (capacity > 0 && !pairs) return fail(EB_ERR_INVALID_ARGUMENT, "null pair buffer");
+  const ContactDevice& c = s->contact;
+  if (!c.on) return fail(EB_ERR_UNSUPPORTED, "no rod takes part in contact");
+  if (!c.evaluated) return fail(EB_ERR_INVALID_STATE, "no contact evaluation yet: step first");
+  if (eb_status st = set_device(s)) return st;
+  std::vector<int64_t> off(static_cast<size_t>(s->n_slots + 1));
+  EB_CUDA(cudaMemcpyAsync(off.data(), c.pair_offset, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  const int64_t total = off[static_cast<size_t>(s->n_slots)];
+  if (total > c.capacity) return fail(EB_ERR_INVALID_STATE, "the last evaluation overflowed the pair buffer");
+  std::vector<int32_t> part(static_cast<size_t>(std::max<int64_t>(total, 1)));
+  if (total > 0)
+    EB_CUDA(cudaMemcpyAsync(part.data(), c.partners, static_cast<size_t>(total) * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  int64_t n = 0;
+  for (int64_t a = 0; a < s->n_slots; ++a)
+    for (int64_t k = off[static_cast<size_t>(a)]; k < off[static_cast<size_t>(a + 1)]; ++k) {
+      const int64_t b = part[static_cast<size_t>(k)];
+      if (b <= a) continue;
+      if (n < capacity) {
+        pairs[2 * n] = a;
+        pairs[2 * n + 1] = b;
+      }
+      ++n;
+    }
+  *count = n;
+  return check_device_status(s);
 }
 
 EB_API eb_status eb_step_plan(const eb_sim* s, int32_t* mode, int32_t* config, float* probe_ms, int32_t count) {

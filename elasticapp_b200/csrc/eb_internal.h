@@ -99,10 +99,19 @@ struct StepArgs {
   double half_dt;
   double gravity[3];
   uint32_t sim_flags;   // kSim* below
+  // capsule contact loads of this step (lab frame, 3 x stride each, per
+  // element slot), or nullptr without a collision system
+  const double* contact_force;
+  const double* contact_torque;
 };
 
 // device status bits reported back to the host
-enum StatusBits : uint32_t { kStatusCopyTimeout = 1u };
+enum StatusBits : uint32_t {
+  kStatusCopyTimeout = 1u,
+  kStatusPairOverflow = 2u,     // the candidate pair list did not fit its buffer
+  kStatusContactNonFinite = 4u, // a capsule had a non-finite bounding box
+  kStatusContactIndex = 8u      // a grid index fell outside its table (never expected)
+};
 
 enum SimFlags : uint32_t { kSimGravity = 1u, kSimDamper = 2u, kSimEndTorque = 4u, kSimClamp = 8u };
 

@@ -106,7 +106,7 @@ __device__ __forceinline__ D3 div3(D3 a, double d) {
 #endif
 }
 
-template <int W, bool kDiag, bool kDamped>
+template <int W, bool kDiag, bool kDamped, bool kContact>
 __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem) {
   using M = RowMap<kDamped, kDiag>;
   constexpr int kTile = W - 4;  // interior slots stored per CTA (even)
@@ -275,6 +275,14 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   D3 Fe{0.0, 0.0, 0.0};
   if (a.sim_flags & kSimGravity)
     Fe = {0.0 + a.gravity[0] * m, 0.0 + a.gravity[1] * m, 0.0 + a.gravity[2] * m};
+  if (kContact) {
+    // collision system after gravity: the element before the node, then the
+    // element at the node, each adding half its capsule force
+    // (Systems/Customization/CosseratRods/Transfer/Common.hpp:32-55)
+    const double* __restrict__ cf = a.contact_force;
+    if (!(meta & kFirst)) Fe = {Fe.x + 0.5 * cf[g - 1], Fe.y + 0.5 * cf[S + g - 1], Fe.z + 0.5 * cf[2 * S + g - 1]};
+    if (meta & kElem) Fe = {Fe.x + 0.5 * cf[g], Fe.y + 0.5 * cf[S + g], Fe.z + 0.5 * cf[2 * S + g]};
+  }
   const double inv_m = 1.0 / m;
   const D3 acc = {(F.x + Fe.x) * inv_m, (F.y + Fe.y) * inv_m, (F.z + Fe.z) * inv_m};
 
@@ -293,6 +301,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       T = {T.x - c * w.x, T.y - c * w.y, T.z - c * w.z};
     }
     D3 Te{0.0, 0.0, 0.0};
+    if (kContact) {
+      // the capsule torque recast into the material frame: Q tau
+      const double* __restrict__ ct = a.contact_torque;
+      Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
+    }
     if ((meta & kLastElem) && (rflags & kRodEndTorque)) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
       Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
@@ -365,17 +378,17 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
 }
 
-template <int W, int MinBlocks, bool kDiag, bool kDamped>
+template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
 __global__ void __launch_bounds__(W, MinBlocks) rod_step_fp64_kernel(const StepArgs a) {
   extern __shared__ __align__(128) double smem[];
-  rod_step_window<W, kDiag, kDamped>(a, smem);
+  rod_step_window<W, kDiag, kDamped, kContact>(a, smem);
 }
 
-template <int W, int MinBlocks, bool kDiag, bool kDamped>
+template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
 cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   constexpr int kTile = W - 4;
   constexpr size_t bytes = size_t(RowMap<kDamped, kDiag>::rows()) * W * sizeof(double) + 16;
-  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped>;
+  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped, kContact>;
   // the attribute is per device; setting it on every launch is cheap and
   // keeps multi-device use correct
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -385,13 +398,20 @@ cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <int W, int MinBlocks, bool kContact>
+cudaError_t launch_window_c(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
+  if (diag)
+    return damped ? launch_variant<W, MinBlocks, true, true, kContact>(args, stream)
+                  : launch_variant<W, MinBlocks, true, false, kContact>(args, stream);
+  return damped ? launch_variant<W, MinBlocks, false, true, kContact>(args, stream)
+                : launch_variant<W, MinBlocks, false, false, kContact>(args, stream);
+}
+
 template <int W, int MinBlocks>
 cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if (diag)
-    return damped ? launch_variant<W, MinBlocks, true, true>(args, stream)
-                  : launch_variant<W, MinBlocks, true, false>(args, stream);
-  return damped ? launch_variant<W, MinBlocks, false, true>(args, stream)
-                : launch_variant<W, MinBlocks, false, false>(args, stream);
+  if (args.contact_force && args.contact_torque)
+    return launch_window_c<W, MinBlocks, true>(args, diag, damped, stream);
+  return launch_window_c<W, MinBlocks, false>(args, diag, damped, stream);
 }
 
 }  // namespace

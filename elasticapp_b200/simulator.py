@@ -120,6 +120,26 @@ class GravityField:
 
 
 @dataclass
+class ContactMaterial:
+    """Contact parameters of elastica::create_material (Simulator/Materials/
+    Materials.cpp:237-372); a material pair uses 1/(1/a + 1/b) for stiffness
+    and dampings and a + b for the friction coefficients."""
+
+    stiffness: float
+    normal_damping: float
+    tangential_damping: float
+    static_friction: float
+    dynamic_friction: float
+
+
+@dataclass
+class CollisionSystem:
+    """The collision-system environment (Environments/CollisionSystem/
+    DEMSolver.hpp:701-727).  Rods take part through Simulator.add_contact;
+    planes through Simulator.emplace_plane."""
+
+
+@dataclass
 class PositionVerlet:
     """Time/SymplecticSteppers/Algorithms/PositionVerlet.hpp:49-88."""
 
@@ -245,8 +265,40 @@ class Simulator:
         if isinstance(env, GravityField):
             g = np.asarray(env.gravity, dtype=np.float64)
             L.call("eb_add_gravity", self._h, _dptr(g))
+        elif isinstance(env, CollisionSystem):
+            pass  # active once a rod takes part (add_contact)
         else:
             raise TypeError(f"unsupported environment {env!r}")
+
+    # -- collision system ---------------------------------------------------------
+    def create_material(self, material: ContactMaterial) -> int:
+        m = L.EbContactMaterial(float(material.stiffness), float(material.normal_damping),
+                                float(material.tangential_damping), float(material.static_friction),
+                                float(material.dynamic_friction))
+        mid = ctypes.c_int32()
+        L.call("eb_add_contact_material", self._h, ctypes.byref(m), ctypes.byref(mid))
+        return mid.value
+
+    def add_contact(self, rod: RodRef, material: int) -> None:
+        """The rod's elements become capsules of the collision system."""
+        L.call("eb_add_rod_contact", self._h, rod.id, int(material))
+
+    def emplace_plane(self, point, normal, material: int) -> None:
+        """Infinite fixed plane (PlanePrimitive.cpp:60-130)."""
+        p = np.ascontiguousarray(point, dtype=np.float64)
+        n = np.ascontiguousarray(normal, dtype=np.float64)
+        L.call("eb_add_contact_plane", self._h, _dptr(p), _dptr(n), int(material))
+
+    def contact_pairs(self) -> np.ndarray:
+        """Sorted candidate pairs (k, 2) of the last step: capsule id = element
+        slot, plane p = n_slots + p."""
+        count = ctypes.c_int64()
+        L.call("eb_contact_pairs", self._h, None, 0, ctypes.byref(count))
+        out = np.zeros(2 * max(count.value, 1), dtype=np.int64)
+        n2 = ctypes.c_int64()
+        L.call("eb_contact_pairs", self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), count.value,
+               ctypes.byref(n2))
+        return out[:2 * n2.value].reshape(n2.value, 2)
 
     def _attach(self, kind, rod, index, item):
         if kind == "constrain" and isinstance(item, Clamp):

@@ -19,6 +19,14 @@ with the seed recorded in the workload.
   reference algorithm itself (the FP64 oracle's angular velocities grow and
   turn non-finite within 8,000 steps), because the fattest elements have a
   radius up to 25 times their length.
+* ``contact_batch`` — 8,192 free rods, n = 64, L 0.2 m, r 0.002 m, E 1e6,
+  G = E/3, rho 1000, centres uniform in the unit cube, random directions,
+  node velocities N(0, 0.05^2), gravity -9.81 z, six wall planes of the cube
+  with inward normals, contact stiffness 1e4 N/m, dashpot 10 N s/m and
+  friction 0.3 for every pair (per material 2e4, 20 and 0.15 under the pair
+  rules), no damping, dt 1e-5.  With 4 r > l every capsule also overlaps the
+  capsules two elements along its own rod; the reference's collision system
+  applies contact there too.
 """
 from __future__ import annotations
 
@@ -26,8 +34,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .simulator import (AnalyticalLinearDamper, Clamp, CosseratRodWithoutDamping, EndTorque,
-                        GravityField, Material, Simulator, StraightRod)
+from .simulator import (AnalyticalLinearDamper, Clamp, CollisionSystem, ContactMaterial,
+                        CosseratRodWithoutDamping, EndTorque, GravityField, Material, Simulator, StraightRod)
 
 
 @dataclass
@@ -44,6 +52,9 @@ class Workload:
     rest_curvature: list | None = None        # per rod (3, n - 1)
     dt: float = 1e-5
     n_steps: int = 1000
+    contact_materials: list | None = None     # ContactMaterial per material id
+    contact_rod_material: list | None = None  # per rod material id (-1: none)
+    planes: list | None = None                # (point, normal, material id)
 
     @property
     def n_elements(self) -> np.ndarray:
@@ -74,6 +85,15 @@ class Workload:
                 sim.constrain(ref).using(AnalyticalLinearDamper(*self.damper))
             if self.end_torque is not None:
                 sim.force(ref).at(ref.n_elements - 1).using(EndTorque(self.end_torque[k]))
+        if self.contact_materials:
+            sim.add_environment(CollisionSystem())
+            ids = [sim.create_material(m) for m in self.contact_materials]
+            for k, ref in enumerate(refs):
+                mat = self.contact_rod_material[k] if self.contact_rod_material is not None else 0
+                if mat >= 0:
+                    sim.add_contact(ref, ids[mat])
+            for point, normal, mat in (self.planes or []):
+                sim.emplace_plane(point, normal, ids[mat])
         sim.finalize()
         return sim
 
@@ -146,4 +166,31 @@ def mixed_batch(n_rods: int = 65536, seed: int = 1003, n_range=(64, 256), n_step
                     end_torque=torque, dt=dt, n_steps=n_steps)
 
 
-CONFIGS = {"cantilever": cantilever, "uneven_batch": uneven_batch, "mixed_batch": mixed_batch}
+def unit_cube_walls(size: float = 1.0, material: int = 0) -> list:
+    """The six walls of [0, size]^3 with inward normals."""
+    h = 0.5 * size
+    return [((0.0, h, h), (1.0, 0.0, 0.0), material), ((size, h, h), (-1.0, 0.0, 0.0), material),
+            ((h, 0.0, h), (0.0, 1.0, 0.0), material), ((h, size, h), (0.0, -1.0, 0.0), material),
+            ((h, h, 0.0), (0.0, 0.0, 1.0), material), ((h, h, size), (0.0, 0.0, -1.0), material)]
+
+
+def contact_batch(n_rods: int = 8192, seed: int = 1004, n_elements: int = 64, box: float = 1.0,
+                  dt: float = 1e-5, n_steps: int = 10_000, length: float = 0.2) -> Workload:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    radius, E = 0.002, 1e6
+    d = _unit_vectors(rng, n_rods)
+    nv = _normals(rng, d)
+    centres = rng.uniform(0.0, box, size=(n_rods, 3))
+    rods = [StraightRod(n_elements=n_elements, material=Material(1000.0, E, E / 3.0), radius=radius,
+                        length=length, origin=tuple(centres[k] - 0.5 * length * d[k]), direction=tuple(d[k]),
+                        normal=tuple(nv[k])) for k in range(n_rods)]
+    vel = [rng.normal(0.0, 0.05, size=(3, n_elements + 1)) for _ in range(n_rods)]
+    mat = ContactMaterial(stiffness=2e4, normal_damping=20.0, tangential_damping=20.0, static_friction=0.15,
+                          dynamic_friction=0.15)
+    return Workload("contact_batch", seed, rods, clamp=False, damper=None, velocities=vel, dt=dt,
+                    n_steps=n_steps, contact_materials=[mat], contact_rod_material=[0] * n_rods,
+                    planes=unit_cube_walls(box))
+
+
+CONFIGS = {"cantilever": cantilever, "uneven_batch": uneven_batch, "mixed_batch": mixed_batch,
+           "contact_batch": contact_batch}

@@ -150,7 +150,11 @@ typedef enum eb_field {
   EB_ACCELERATION = 26,          /* 3 x N */
   EB_ANGULAR_ACCELERATION = 27,  /* 3 x E */
   EB_ELEMENT_DIMENSION = 28,     /* E */
-  EB_FIELD_COUNT = 29
+  /* collision system (after eb_add_rod_contact), read only: the capsule
+   * loads of the last step's contact evaluation, lab frame, per element */
+  EB_CONTACT_FORCE = 29,         /* 3 x E */
+  EB_CONTACT_TORQUE = 30,        /* 3 x E */
+  EB_FIELD_COUNT = 31
 } eb_field;
 
 /* Layout of the batch accessors. */
@@ -220,6 +224,48 @@ EB_API eb_status eb_add_end_torque(struct eb_sim* sim, int64_t rod, const double
  * 15-76): v *= exp(-nu_t dt); w_k *= exp(-nu_r m_e J^-1_k dt)^e. */
 EB_API eb_status eb_add_analytical_damper(struct eb_sim* sim, int64_t rod,
                                           double translational_rate, double rotational_rate);
+
+/* --- environments: the collision system (elastica/Simulator/Environments/
+ * CollisionSystem, resolved once per dynamic substep, DEMSolver.hpp:701-727).
+ * Every element of a participating rod is a capsule (Systems/Customization/
+ * CosseratRods/Transfer/Common.hpp:57-93); candidate pairs are the capsule
+ * pairs and capsule-plane pairs whose closed bounding boxes overlap
+ * (Detection/Coarse/HashGrids.hpp, ExhaustiveSearch.hpp:322-435); the narrow
+ * phase is RodCapsuleRodCapsule.hpp:70-186 and CapsulePlane.hpp:60-113; the
+ * response is the linear spring-dashpot (Response/DEMForces/
+ * LinearSpringDashpot.cpp:32-85); the capsule loads go back to the nodes
+ * (half each) and, recast as Q tau, to the element (Transfer/Common.hpp:
+ * 32-55), after gravity.  Contact runs on the FP64 streaming step only. */
+
+/* Contact parameters of one material (elastica::create_material,
+ * Simulator/Materials/Materials.cpp:237-372).  A pair of materials uses
+ * 1 / (1 / a + 1 / b) for stiffness and both dampings and a + b for the
+ * friction coefficients (Materials.hpp:1131-1137). */
+typedef struct eb_contact_material {
+  double stiffness;           /* > 0 */
+  double normal_damping;      /* >= 0 */
+  double tangential_damping;  /* >= 0 */
+  double static_friction;     /* >= 0 */
+  double dynamic_friction;    /* >= 0 */
+} eb_contact_material;
+
+/* create_material: returns the material id (0, 1, 2, ... in order). */
+EB_API eb_status eb_add_contact_material(struct eb_sim* sim, const eb_contact_material* material,
+                                         int32_t* material_id);
+/* The rod takes part in the collision system with this material (the
+ * RodInitializer::Material of the reference's rods). */
+EB_API eb_status eb_add_rod_contact(struct eb_sim* sim, int64_t rod, int32_t material_id);
+/* An infinite, fixed, double-sided plane through `point` with `normal`
+ * (PlanePrimitive, Simulator/Environments/Primitives/PlanePrimitive.cpp:60-130). */
+EB_API eb_status eb_add_contact_plane(struct eb_sim* sim, const double point[3], const double normal[3],
+                                      int32_t material_id);
+/* Candidate pairs of the last step's contact evaluation: pairs[2 k], pairs[2 k + 1]
+ * = (a, b), a < b, sorted; a capsule's id is its element slot (rod r's element
+ * i is eb_slot_offsets()[r] + i) and plane p is eb_slot_count() + p.  Writes
+ * up to `capacity` pairs and sets *count to the total (the set the
+ * reference's coarse detection produces, Detection/Coarse/ExhaustiveSearch.hpp:
+ * 322-435).  EB_ERR_INVALID_STATE before the first step. */
+EB_API eb_status eb_contact_pairs(struct eb_sim* sim, int64_t* pairs, int64_t capacity, int64_t* count);
 
 /* --- simulator->finalize() (Simulator.hpp:538-578): allocates device
  * memory and uploads the rods.  No rods or constraints may be added after. */

@@ -42,6 +42,24 @@ class _OrcRods(ctypes.Structure):
     ]
 
 
+class _OrcContactMaterial(ctypes.Structure):
+    _fields_ = [("stiffness", ctypes.c_double), ("normal_damping", ctypes.c_double),
+                ("tangential_damping", ctypes.c_double), ("static_friction", ctypes.c_double),
+                ("dynamic_friction", ctypes.c_double)]
+
+
+class _OrcContact(ctypes.Structure):
+    _fields_ = [
+        ("n_materials", ctypes.c_int32),
+        ("materials", ctypes.POINTER(_OrcContactMaterial)),
+        ("rod_material", ctypes.POINTER(ctypes.c_int32)),
+        ("n_planes", ctypes.c_int32),
+        ("plane_point", _P), ("plane_normal", _P),
+        ("plane_material", ctypes.POINTER(ctypes.c_int32)),
+        ("capsule_force", _P), ("capsule_torque", _P),
+    ]
+
+
 _lib = None
 
 
@@ -65,6 +83,16 @@ def lib():
         _lib.orc_energy.argtypes = [ctypes.POINTER(_OrcRods), _P, ctypes.c_int]
         _lib.orc_straight_rod.argtypes = [ctypes.c_int64, _P, _P, _P, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double] + [_P] * 11
+        _lib.orc_step_contact.argtypes = [ctypes.POINTER(_OrcRods), ctypes.POINTER(_OrcContact), ctypes.c_double,
+                                          ctypes.c_int64, ctypes.c_int]
+        _lib.orc_contact_capsules.argtypes = [ctypes.POINTER(_OrcRods), ctypes.POINTER(_OrcContact),
+                                              ctypes.c_double, _P]
+        _lib.orc_contact_pairs.argtypes = [ctypes.POINTER(_OrcRods), ctypes.POINTER(_OrcContact), ctypes.c_double,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.c_int64]
+        _lib.orc_contact_pairs.restype = ctypes.c_int64
+        for name in ("orc_fine_capsule_capsule", "orc_fine_capsule_plane"):
+            getattr(_lib, name).argtypes = [_P, _P, _P]
+        _lib.orc_fine_pair_loads.argtypes = [_P, _P, _P, _P]
     return _lib
 
 
@@ -200,3 +228,116 @@ class RodArrays:
             setattr(c, k, getattr(self, k).copy())
         c.diag = None if self.diag is None else {k: a.copy() for k, a in self.diag.items()}
         return c
+
+
+class ContactSpec:
+    """Collision-system description for the oracle: per-material contact
+    parameters (stiffness, normal damping, tangential damping, static and
+    dynamic friction), the material of each rod (-1: no contact) and planes
+    (point, normal, material)."""
+
+    def __init__(self, materials, rod_material, planes=()):
+        self.materials = np.asarray(materials, dtype=np.float64).reshape(-1, 5)
+        self.rod_material = np.ascontiguousarray(rod_material, dtype=np.int32)
+        self.planes = list(planes)
+        self.plane_point = np.array([p[0] for p in self.planes], dtype=np.float64).reshape(-1)
+        self.plane_normal = np.array([p[1] for p in self.planes], dtype=np.float64).reshape(-1)
+        self.plane_material = np.array([p[2] for p in self.planes], dtype=np.int32)
+        if self.plane_point.size == 0:
+            self.plane_point = np.zeros(3)
+            self.plane_normal = np.zeros(3)
+            self.plane_material = np.zeros(1, dtype=np.int32)
+        self._mats = (_OrcContactMaterial * max(1, len(self.materials)))()
+        for i, m in enumerate(self.materials):
+            self._mats[i] = _OrcContactMaterial(*[float(v) for v in m])
+        self.capsule_force = None
+        self.capsule_torque = None
+
+    def _struct(self, n_slots):
+        c = _OrcContact()
+        c.n_materials = len(self.materials)
+        c.materials = ctypes.cast(self._mats, ctypes.POINTER(_OrcContactMaterial))
+        c.rod_material = self.rod_material.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        c.n_planes = len(self.planes)
+        c.plane_point = self.plane_point.ctypes.data_as(_P)
+        c.plane_normal = self.plane_normal.ctypes.data_as(_P)
+        c.plane_material = self.plane_material.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        if self.capsule_force is None or self.capsule_force.size != 3 * n_slots:
+            self.capsule_force = np.zeros(3 * n_slots)
+            self.capsule_torque = np.zeros(3 * n_slots)
+        c.capsule_force = self.capsule_force.ctypes.data_as(_P)
+        c.capsule_torque = self.capsule_torque.ctypes.data_as(_P)
+        return c
+
+
+def contact_step(rods: RodArrays, spec: ContactSpec, dt, n_steps=1, n_threads=0):
+    """PositionVerlet steps with the collision system (orc_step_contact)."""
+    s = rods._struct()
+    c = spec._struct(rods.n_slots)
+    if lib().orc_step_contact(ctypes.byref(s), ctypes.byref(c), float(dt), int(n_steps), int(n_threads)) != 0:
+        raise RuntimeError("orc_step_contact failed")
+
+
+def contact_capsules(rods: RodArrays, spec: ContactSpec, half_dt=0.0):
+    """(14, n_slots) capsule table after a drift of half_dt: centre(3),
+    length, radius, axis(3), AABB min(3), AABB max(3); NaN where no capsule."""
+    out = np.full(14 * rods.n_slots, np.nan)
+    s = rods._struct()
+    c = spec._struct(rods.n_slots)
+    if lib().orc_contact_capsules(ctypes.byref(s), ctypes.byref(c), float(half_dt), out.ctypes.data_as(_P)) != 0:
+        raise RuntimeError("orc_contact_capsules failed")
+    return out.reshape(14, rods.n_slots)
+
+
+def contact_pairs(rods: RodArrays, spec: ContactSpec, half_dt=0.0, exhaustive=True):
+    """Sorted candidate pairs (k, 2) int64 of the capsules after a drift of
+    half_dt; plane p appears as n_slots + p."""
+    s = rods._struct()
+    c = spec._struct(rods.n_slots)
+    n = lib().orc_contact_pairs(ctypes.byref(s), ctypes.byref(c), float(half_dt), int(bool(exhaustive)), None, 0)
+    if n < 0:
+        raise RuntimeError("orc_contact_pairs failed")
+    out = np.zeros(2 * max(n, 1), dtype=np.int64)
+    n2 = lib().orc_contact_pairs(ctypes.byref(s), ctypes.byref(c), float(half_dt), int(bool(exhaustive)),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), int(n))
+    assert n2 == n
+    return out[:2 * n].reshape(n, 2)
+
+
+def _capsule_desc(c):
+    d = np.zeros(14)
+    d[0:3] = c["centre"]
+    d[3:6] = c["axis"]
+    d[6] = c["radius"]
+    d[7] = c["length"]
+    d[8:11] = c.get("velocity", (0.0, 0.0, 0.0))
+    d[11:14] = c.get("omega", (0.0, 0.0, 0.0))
+    return d
+
+
+def fine_capsule_capsule(a, b):
+    """Contacts [(position, normal, distance)] of two rod capsules (dicts with
+    centre, axis, radius, length[, velocity, omega]), a being the first body."""
+    out = np.zeros(14)
+    da, db = _capsule_desc(a), _capsule_desc(b)
+    n = lib().orc_fine_capsule_capsule(da.ctypes.data_as(_P), db.ctypes.data_as(_P), out.ctypes.data_as(_P))
+    return [(out[7 * i:7 * i + 3].copy(), out[7 * i + 3:7 * i + 6].copy(), float(out[7 * i + 6])) for i in range(n)]
+
+
+def fine_capsule_plane(c, point, normal):
+    out = np.zeros(14)
+    dc = _capsule_desc(c)
+    pl = np.concatenate([np.asarray(point, float), np.asarray(normal, float)])
+    n = lib().orc_fine_capsule_plane(dc.ctypes.data_as(_P), pl.ctypes.data_as(_P), out.ctypes.data_as(_P))
+    return [(out[7 * i:7 * i + 3].copy(), out[7 * i + 3:7 * i + 6].copy(), float(out[7 * i + 6])) for i in range(n)]
+
+
+def fine_pair_loads(a, b, pair_material):
+    """(force1, torque1, force2, torque2) of the spring-dashpot over all
+    contacts of the capsule pair; pair_material = (k, c_n, c_t, mu_s, mu_d)."""
+    out = np.zeros(12)
+    da, db = _capsule_desc(a), _capsule_desc(b)
+    pm = np.asarray(pair_material, dtype=np.float64)
+    lib().orc_fine_pair_loads(da.ctypes.data_as(_P), db.ctypes.data_as(_P), pm.ctypes.data_as(_P),
+                              out.ctypes.data_as(_P))
+    return out.reshape(4, 3)

@@ -13,8 +13,11 @@
 // values (zeroed dummy vectors, zeroed curvature ghosts) make the two equal.
 #include "rod_oracle.h"
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 #ifdef _OPENMP
@@ -178,7 +181,11 @@ void clamp_values(const OrcRods& R, int64_t r) {
 // Internal forces and torques of one rod (ElasticityInterface.hpp:360-365),
 // then external loads and update_acceleration.  Fills sc.fl (loads, nodes)
 // and sc.tq (torques, elements) and the per-element dilatation sc.dil.
-void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, double* alpha) {
+// cf, ct: capsule contact force and torque (lab frame, per element slot,
+// 3*S) transferred to the rod as in
+// Systems/Customization/CosseratRods/Transfer/Common.hpp:32-55, or NULL.
+void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, double* alpha,
+                      const double* cf = nullptr, const double* ct = nullptr) {
   const int64_t S = R.n_slots, o = R.offset[r], n = R.offset[r + 1] - o - 1;
   const Field x{R.x, S}, v{R.v, S}, w{R.w, S};
   sc.resize(n);
@@ -322,7 +329,12 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
   for (int64_t j = 0; j <= n; ++j) {
     const int64_t s = o + j;
     const double m = R.mass[s];
-    const V3 fe = {0.0 + R.gravity[0] * m, 0.0 + R.gravity[1] * m, 0.0 + R.gravity[2] * m};
+    V3 fe = {0.0 + R.gravity[0] * m, 0.0 + R.gravity[1] * m, 0.0 + R.gravity[2] * m};
+    if (cf) {
+      // element j-1 adds half its force to node j first, then element j
+      if (j > 0) fe = {fe.x + 0.5 * cf[s - 1], fe.y + 0.5 * cf[S + s - 1], fe.z + 0.5 * cf[2 * S + s - 1]};
+      if (j < n) fe = {fe.x + 0.5 * cf[s], fe.y + 0.5 * cf[S + s], fe.z + 0.5 * cf[2 * S + s]};
+    }
     const V3 f = getv(sc.fl, j);
     const double im = 1.0 / m;  // InvMass, WithRodKinematics.hpp:411-424
     const V3 a = {(f.x + fe.x) * im, (f.y + fe.y) * im, (f.z + fe.z) * im};
@@ -333,6 +345,13 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
   for (int64_t i = 0; i < n; ++i) {
     const int64_t s = o + i;
     V3 te = {0.0, 0.0, 0.0};
+    if (ct) {
+      // the capsule torque recast into the material frame: Q tau
+      double q[9];
+      load_q(R.Q, S, s, q);
+      const V3 tc = matvec(q, {ct[s], ct[S + s], ct[2 * S + s]});
+      te = {te.x + tc.x, te.y + tc.y, te.z + tc.z};
+    }
     if (i == n - 1) te = {te.x + tend.x, te.y + tend.y, te.z + tend.z};
     const V3 T = getv(sc.tq, i);
     const double e = sc.dil[i];
@@ -417,6 +436,523 @@ int check(const OrcRods* R) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Collision system (Simulator/Environments/CollisionSystem): every element of
+// a participating rod becomes a capsule, candidate pairs are the capsule
+// pairs (and capsule-plane pairs) whose closed axis-aligned bounding boxes
+// overlap, the narrow phase generates contact points, a linear
+// spring-dashpot turns them into forces and torques on the capsules, and the
+// capsule loads are transferred back to the rods' external loads.
+
+constexpr double kContactThreshold = 1e-8;   // Utilities/Thresholds.hpp:138
+constexpr double kParallelThreshold = 1e-8;  // Utilities/Thresholds.hpp:159
+constexpr double kFrictionThreshold = 1e-8;  // Utilities/Thresholds.hpp:149
+// blaze::accuracy for double (Blaze's Limits<double>::accuracy()), the bound
+// of is_zero_length (Utilities/Math/Zero.hpp:46-49)
+constexpr double kZeroLength = 1e-8;
+// default plane spans (Simulator/Environments/Primitives/PlanePrimitive.cpp:63-66)
+constexpr double kPlaneSpan = 1e40;
+
+inline double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 add3(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 mul3(double k, V3 a) { return {k * a.x, k * a.y, k * a.z}; }
+inline V3 neg3(V3 a) { return {-a.x, -a.y, -a.z}; }
+// blaze::normalize: a * (1 / |a|); a zero vector stays zero
+inline V3 normalize3(V3 a) {
+  const double len = norm(a);
+  const double il = len != 0.0 ? 1.0 / len : 0.0;
+  return {a.x * il, a.y * il, a.z * il};
+}
+
+struct Basis {
+  V3 r0, r1, r2;  // rows of the rotation matrix
+};
+
+// Utilities/Math/Orthogonal.cpp:32-55 (make_orthogonal_bases_impl): returns
+// {v1, normalize(v2), normalize(v3)} for the normalised input v1.
+inline void orthogonal_bases(V3 vec, V3& v1, V3& v2n, V3& v3n) {
+  v1 = normalize3(vec);
+  V3 v2 = {0.8, 0.6, 0.0};
+  V3 v3 = cross(v1, v2);
+  v2 = cross(v3, v1);
+  if (dot3(v2, v2) < kZeroLength) {
+    v2 = {0.6, -0.8, 0.0};
+    v3 = normalize3(cross(v1, v2));
+    v2 = cross(v3, v1);
+  }
+  v2n = normalize3(v2);
+  v3n = normalize3(v3);
+}
+
+// Orthogonal.cpp:118-129 make_orthogonal_bases_from_tangent: rows permuted
+// {1, 2, 0}, so the tangent is the third row.
+inline Basis bases_from_tangent(V3 t) {
+  V3 a, b, c;
+  orthogonal_bases(t, a, b, c);
+  return {b, c, a};
+}
+
+// Orthogonal.cpp:85-96 make_orthogonal_bases_from_normal: rows in order.
+inline Basis bases_from_normal(V3 n) {
+  V3 a, b, c;
+  orthogonal_bases(n, a, b, c);
+  return {a, b, c};
+}
+
+struct Capsule {
+  V3 c;       // centre
+  double L;   // length
+  double r;   // radius
+  V3 u;       // axis (third row of the rotation)
+  V3 vel;     // translational velocity
+  V3 ww;      // angular velocity taken to the world frame, trans(R) w
+  double lo[3], hi[3];
+  int32_t material;
+};
+
+struct Plane {
+  V3 p, n;
+  double lo[3], hi[3];
+  int32_t material;
+};
+
+// Rod -> capsule transfer (Systems/Customization/CosseratRods/Transfer/
+// Common.hpp:57-93, CapsuleFromRodPrimitive::transfer) and the capsule
+// bounding box (Primitives/detail/CapsulePrimitiveBase.cpp:163-180).  x0, x1
+// are the (drifted) nodes of the element at slot s.
+Capsule make_capsule(const OrcRods& R, int64_t s, V3 x0, V3 x1, int32_t material) {
+  const int64_t S = R.n_slots;
+  Capsule k;
+  const V3 dx = sub(x1, x0);
+  const double l = norm(dx);
+  const V3 t = {dx.x / l, dx.y / l, dx.z / l};
+  const double l0 = R.rest_length[s];
+  const double e = l / l0;
+  k.L = e * l0;  // element_length = dilatation * rest length after the torques
+  k.r = std::sqrt(M_1_PI * R.volume[s] / l);
+  k.c = {0.5 * (x0.x + x1.x), 0.5 * (x0.y + x1.y), 0.5 * (x0.z + x1.z)};
+  const Basis B = bases_from_tangent(t);
+  k.u = B.r2;
+  const double m0 = R.mass[s], m1 = R.mass[s + 1];
+  const V3 v0 = {R.v[s], R.v[S + s], R.v[2 * S + s]};
+  const V3 v1 = {R.v[s + 1], R.v[S + s + 1], R.v[2 * S + s + 1]};
+  const V3 num = add3(mul3(m0, v0), mul3(m1, v1));
+  const double den = m0 + m1;
+  k.vel = {num.x / den, num.y / den, num.z / den};
+  const V3 w = {R.w[s], R.w[S + s], R.w[2 * S + s]};
+  // RigidBodyPrimitive.hpp:382-393 from_body_FOR_to_world_FOR: trans(Q) * w
+  k.ww = {B.r0.x * w.x + B.r1.x * w.y + B.r2.x * w.z, B.r0.y * w.x + B.r1.y * w.y + B.r2.y * w.z,
+          B.r0.z * w.x + B.r1.z * w.y + B.r2.z * w.z};
+  const double ua[3] = {k.u.x, k.u.y, k.u.z}, ca[3] = {k.c.x, k.c.y, k.c.z};
+  for (int d = 0; d < 3; ++d) {
+    const double len = std::fabs(ua[d] * k.L) * 0.5 + k.r + kContactThreshold;
+    k.lo[d] = ca[d] - len;
+    k.hi[d] = ca[d] + len;
+  }
+  k.material = material;
+  return k;
+}
+
+// PlanePrimitive.cpp:88-130 (rotation from the normal) and :179-236 (its
+// bounding box with the default spans).
+Plane make_plane(V3 point, V3 normal, int32_t material) {
+  Plane P;
+  const Basis B = bases_from_normal(normal);
+  P.p = point;
+  P.n = B.r0;
+  const double b[3] = {B.r1.x, B.r1.y, B.r1.z}, t[3] = {B.r2.x, B.r2.y, B.r2.z};
+  const double pa[3] = {point.x, point.y, point.z};
+  for (int d = 0; d < 3; ++d) {
+    const double len = 0.5 * (std::fabs(b[d] * kPlaneSpan) + std::fabs(t[d] * kPlaneSpan)) + kContactThreshold;
+    P.lo[d] = pa[d] - len;
+    P.hi[d] = pa[d] + len;
+  }
+  P.material = material;
+  return P;
+}
+
+// Detection/Coarse/BoundingBox.hpp:532-540 (closed intervals)
+inline bool overlaps(const double alo[3], const double ahi[3], const double blo[3], const double bhi[3]) {
+  return !(blo[0] > ahi[0] || blo[1] > ahi[1] || blo[2] > ahi[2] || bhi[0] < alo[0] || bhi[1] < alo[1] ||
+           bhi[2] < alo[2]);
+}
+
+// Utilities/Geometry/GetClosestLineSegmentPoints.cpp (closest points of the
+// segments a1-a2 and b1-b2), branch for branch.
+void closest_segment_points(V3 a1, V3 a2, V3 b1, V3 b2, V3& cp1, V3& cp2) {
+  const V3 a1a2 = sub(a2, a1), b1b2 = sub(b2, b1), a1b1 = sub(b1, a1);
+  const double da1 = dot3(a1a2, a1b1), db1 = dot3(b1b2, a1b1);
+  if (da1 <= 0.0 && db1 >= 0.0) {
+    cp1 = a1;
+    cp2 = b1;
+    return;
+  }
+  const V3 a1b2 = sub(b2, a1);
+  const double da2 = dot3(a1a2, a1b2), db2 = dot3(b1b2, a1b2);
+  if (da2 <= 0.0 && db2 <= 0.0) {
+    cp1 = a1;
+    cp2 = b2;
+    return;
+  }
+  const V3 a2b1 = sub(b1, a2);
+  const double da3 = dot3(a1a2, a2b1), db3 = dot3(b1b2, a2b1);
+  if (da3 >= 0.0 && db3 >= 0.0) {
+    cp1 = a2;
+    cp2 = b1;
+    return;
+  }
+  const V3 a2b2 = sub(b2, a2);
+  const double da4 = dot3(a1a2, a2b2), db4 = dot3(b1b2, a2b2);
+  if (da4 >= 0.0 && db4 <= 0.0) {
+    cp1 = a2;
+    cp2 = b2;
+    return;
+  }
+  const double la = dot3(a1a2, a1a2);
+  if (da1 >= -kParallelThreshold && da3 <= kParallelThreshold) {
+    const V3 k = mul3(da1 / la, a1a2);
+    const V3 n = sub(a1b1, k);
+    if (dot3(b1b2, n) >= -kParallelThreshold) {
+      cp1 = add3(a1, k);
+      cp2 = b1;
+      return;
+    }
+  }
+  if (da2 >= -kParallelThreshold && da4 <= kParallelThreshold) {
+    const V3 k = mul3(da2 / la, a1a2);
+    const V3 n = sub(a1b2, k);
+    if (dot3(b1b2, n) <= kParallelThreshold) {
+      cp1 = add3(a1, k);
+      cp2 = b2;
+      return;
+    }
+  }
+  const double lb = dot3(b1b2, b1b2);
+  if (db1 <= kParallelThreshold && db2 >= -kParallelThreshold) {
+    const V3 k = mul3(-db1 / lb, b1b2);
+    const V3 n = sub(neg3(a1b1), k);
+    if (dot3(a1a2, n) >= -kParallelThreshold) {
+      cp1 = a1;
+      cp2 = add3(b1, k);
+      return;
+    }
+  }
+  if (db3 <= kParallelThreshold && db4 >= -kParallelThreshold) {
+    const V3 k = mul3(-db3 / lb, b1b2);
+    const V3 n = sub(neg3(a2b1), k);
+    if (dot3(a1a2, n) <= kParallelThreshold) {
+      cp1 = a2;
+      cp2 = add3(b1, k);
+      return;
+    }
+  }
+  const double scale = dot3(a1a2, b1b2);
+  double div = la * lb - scale * scale;
+  div = 1.0 / div;
+  const double sp = (lb * da1 - scale * db1) * div;
+  const double tp = (scale * da1 - la * db1) * div;
+  cp1 = add3(a1, mul3(sp, a1a2));
+  cp2 = add3(b1, mul3(tp, b1b2));
+}
+
+struct ContactPoint {
+  V3 pos, n;
+  double dist;
+};
+
+// Detection/Fine/Kernels/RodCapsuleRodCapsule.hpp:70-186; c1 is the capsule
+// with the smaller id.  Returns the number of contact points (0, 1 or 2).
+int rod_capsule_contacts(const Capsule& c1, const Capsule& c2, ContactPoint out[2]) {
+  const V3 up1 = mul3(0.5 * c1.L, c1.u), up2 = mul3(0.5 * c2.L, c2.u);
+  V3 cp1, cp2;
+  closest_segment_points(add3(c1.c, up1), sub(c1.c, up1), add3(c2.c, up2), sub(c2.c, up2), cp1, cp2);
+  V3 nrm = sub(cp1, cp2);
+  const double ln = norm(nrm);
+  if (ln < kContactThreshold) return 0;
+  const double dist = ln - c1.r - c2.r;
+  if (!(dist < kContactThreshold)) return 0;
+  nrm = normalize3(nrm);
+  const double c2x = dot3(c1.u, sub(c2.c, c1.c));
+  if ((std::fabs(dot3(c1.u, c2.u)) - 1.0) > -kParallelThreshold && std::fabs(c2x) < c1.L) {
+    const double hl1 = 0.5 * c1.L, hl2 = 0.5 * c2.L;
+    if (hl1 < c2x + hl2) {
+      const double k = c1.r + 0.5 * dist;
+      out[0] = {sub(add3(c1.c, up1), mul3(k, nrm)), nrm, dist};
+    } else {
+      const double k = c2.r + 0.5 * dist;
+      out[0] = {add3(add3(c2.c, mul3(hl2, c1.u)), mul3(k, nrm)), nrm, dist};
+    }
+    if (-hl1 > c2x - hl2) {
+      const double k = c1.r + 0.5 * dist;
+      out[1] = {sub(sub(c1.c, up1), mul3(k, nrm)), nrm, dist};
+    } else {
+      const double k = c2.r + 0.5 * dist;
+      out[1] = {add3(sub(c2.c, mul3(hl2, c1.u)), mul3(k, nrm)), nrm, dist};
+    }
+    return 2;
+  }
+  const double k = c2.r + 0.5 * dist;
+  out[0] = {add3(cp2, mul3(k, nrm)), nrm, dist};
+  return 1;
+}
+
+// Detection/Fine/Kernels/CapsulePlane.hpp:60-113
+int capsule_plane_contacts(const Capsule& c, const Plane& p, ContactPoint out[2]) {
+  const V3 up = mul3(0.5 * c.L, c.u);
+  const V3 pu = add3(c.c, up), pl = sub(c.c, up);
+  const double du = std::fabs(dot3(p.n, sub(pu, p.p))) - c.r;
+  const double dl = std::fabs(dot3(p.n, sub(pl, p.p))) - c.r;
+  int k = 0;
+  if (du < kContactThreshold) out[k++] = {sub(pu, mul3(c.r + du, p.n)), p.n, du};
+  if (dl < kContactThreshold) out[k++] = {sub(pl, mul3(c.r + dl, p.n)), p.n, dl};
+  return k;
+}
+
+struct PairMaterial {
+  double k, cn, ct, mu_s, mu_d;
+};
+
+// Simulator/Materials/Materials.hpp:1131-1137 and the damping analogues
+// (series rule), Materials.cpp:346-372 (pair friction = sum of the two)
+PairMaterial pair_material(const OrcContact& C, int32_t m1, int32_t m2) {
+  const OrcContactMaterial& a = C.materials[m1];
+  const OrcContactMaterial& b = C.materials[m2];
+  PairMaterial pm;
+  pm.k = 1.0 / (1.0 / a.stiffness + 1.0 / b.stiffness);
+  pm.cn = 1.0 / (1.0 / a.normal_damping + 1.0 / b.normal_damping);
+  pm.ct = 1.0 / (1.0 / a.tangential_damping + 1.0 / b.tangential_damping);
+  pm.mu_s = a.static_friction + b.static_friction;
+  pm.mu_d = a.dynamic_friction + b.dynamic_friction;
+  return pm;
+}
+
+// velocity of a capsule's material point at pos (RigidBodyPrimitive.hpp:451-465)
+inline V3 point_velocity(const Capsule& k, V3 pos) { return add3(k.vel, cross(k.ww, sub(pos, k.c))); }
+
+// Contact.cpp:150-215 (relative velocity, friction coefficient choice) and
+// Response/DEMForces/LinearSpringDashpot.cpp:32-85.  rvel is the relative
+// velocity of body 1 against body 2 at the contact point.  Returns false for
+// a separated contact (no force).
+bool spring_dashpot(const ContactPoint& ct, V3 rvel, const PairMaterial& pm, V3& net) {
+  if (!(ct.dist < -kContactThreshold)) return false;
+  const V3 n = ct.n;
+  const double rvn = dot3(n, rvel);
+  const double rvt = dot3(n, sub(rvel, mul3(rvn, n)));
+  const double mu = std::fabs(rvt) > kFrictionThreshold ? pm.mu_d : pm.mu_s;
+  const double delta = -ct.dist;
+  const double relvn = -dot3(n, rvel);
+  const V3 relv = neg3(rvel);
+  const V3 relvt = sub(relv, mul3(relvn, n));
+  const double fn = std::max(0.0, pm.k * delta + pm.cn * relvn);
+  const V3 fN = mul3(fn, n);
+  const double ft = std::min(pm.ct * norm(relvt), mu * fn);
+  const V3 fT = mul3(ft, normalize3(relvt));
+  net = add3(fN, fT);
+  return true;
+}
+
+struct ContactWorld {
+  std::vector<Capsule> caps;      // by slot (only element slots of participating rods used)
+  std::vector<uint8_t> is_cap;    // by slot
+  std::vector<int64_t> cap_ids;   // participating element slots, ascending
+  std::vector<Plane> planes;
+};
+
+// capsules of the current R.x (already drifted) for every participating rod
+void build_capsules(const OrcRods& R, const OrcContact& C, ContactWorld& W, const double* x) {
+  const int64_t S = R.n_slots;
+  W.caps.resize(S);
+  W.is_cap.assign(S, 0);
+  W.cap_ids.clear();
+  for (int64_t r = 0; r < R.n_rods; ++r) {
+    const int32_t mat = C.rod_material ? C.rod_material[r] : -1;
+    if (mat < 0) continue;
+    const int64_t o = R.offset[r], n = R.offset[r + 1] - o - 1;
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t s = o + i;
+      const V3 x0 = {x[s], x[S + s], x[2 * S + s]};
+      const V3 x1 = {x[s + 1], x[S + s + 1], x[2 * S + s + 1]};
+      W.caps[s] = make_capsule(R, s, x0, x1, mat);
+      W.is_cap[s] = 1;
+      W.cap_ids.push_back(s);
+    }
+  }
+  W.planes.clear();
+  for (int32_t p = 0; p < C.n_planes; ++p)
+    W.planes.push_back(make_plane({C.plane_point[3 * p], C.plane_point[3 * p + 1], C.plane_point[3 * p + 2]},
+                                  {C.plane_normal[3 * p], C.plane_normal[3 * p + 1], C.plane_normal[3 * p + 2]},
+                                  C.plane_material[p]));
+}
+
+// Exhaustive search (Detection/Coarse/ExhaustiveSearch.hpp:322-435) over the
+// capsules in id order, then every capsule against every plane.
+void pairs_exhaustive(const OrcRods& R, const ContactWorld& W, std::vector<int64_t>& pairs) {
+  pairs.clear();
+  const size_t N = W.cap_ids.size();
+  for (size_t i = 0; i < N; ++i) {
+    const Capsule& a = W.caps[W.cap_ids[i]];
+    for (size_t j = i + 1; j < N; ++j) {
+      const Capsule& b = W.caps[W.cap_ids[j]];
+      if (overlaps(a.lo, a.hi, b.lo, b.hi)) {
+        pairs.push_back(W.cap_ids[i]);
+        pairs.push_back(W.cap_ids[j]);
+      }
+    }
+    for (size_t p = 0; p < W.planes.size(); ++p)
+      if (overlaps(a.lo, a.hi, W.planes[p].lo, W.planes[p].hi)) {
+        pairs.push_back(W.cap_ids[i]);
+        pairs.push_back(R.n_slots + static_cast<int64_t>(p));
+      }
+  }
+}
+
+// The same pair set from a uniform grid: cell edge above the largest box
+// extent, each capsule filed under the cell of its box's lower corner, every
+// capsule tested against the capsules of its 27 neighbouring cells.  Two
+// overlapping boxes have lower corners less than one cell apart on every
+// axis, so the set equals the exhaustive one (the property the reference
+// tests for its hash grids, Test_HashGrids.cpp).
+void pairs_grid(const OrcRods& R, const ContactWorld& W, std::vector<int64_t>& pairs) {
+  pairs.clear();
+  const size_t N = W.cap_ids.size();
+  double h = 0.0;
+  for (int64_t s : W.cap_ids)
+    for (int d = 0; d < 3; ++d) h = std::max(h, W.caps[s].hi[d] - W.caps[s].lo[d]);
+  h = h * (1.0 + 1.0 / 1048576.0);
+  if (!(h > 0.0)) h = 1.0;
+  const double ih = 1.0 / h;
+  auto cell = [&](const Capsule& k, int d) {
+    double c = std::floor(k.lo[d] * ih);
+    c = std::min(std::max(c, -1073741824.0), 1073741824.0);
+    return static_cast<int64_t>(c);
+  };
+  auto key = [](int64_t a, int64_t b, int64_t c) {
+    return (static_cast<uint64_t>(a + (1ll << 31)) << 42) ^ (static_cast<uint64_t>(b + (1ll << 31)) << 21) ^
+           static_cast<uint64_t>(c + (1ll << 31));
+  };
+  std::vector<std::array<int64_t, 3>> cells(N);
+  std::unordered_map<uint64_t, std::vector<int64_t>> grid;
+  grid.reserve(2 * N + 1);
+  for (size_t i = 0; i < N; ++i) {
+    const Capsule& k = W.caps[W.cap_ids[i]];
+    cells[i] = {cell(k, 0), cell(k, 1), cell(k, 2)};
+  }
+  for (size_t i = 0; i < N; ++i) grid[key(cells[i][0], cells[i][1], cells[i][2])].push_back(static_cast<int64_t>(i));
+  std::vector<int64_t> found;
+  for (size_t i = 0; i < N; ++i) {
+    const Capsule& a = W.caps[W.cap_ids[i]];
+    found.clear();
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int64_t cx = cells[i][0] + dx, cy = cells[i][1] + dy, cz = cells[i][2] + dz;
+          auto it = grid.find(key(cx, cy, cz));
+          if (it == grid.end()) continue;
+          for (int64_t j : it->second) {
+            if (static_cast<size_t>(j) <= i) continue;
+            if (cells[j][0] != cx || cells[j][1] != cy || cells[j][2] != cz) continue;
+            const Capsule& b = W.caps[W.cap_ids[j]];
+            if (overlaps(a.lo, a.hi, b.lo, b.hi)) found.push_back(W.cap_ids[j]);
+          }
+        }
+    std::sort(found.begin(), found.end());
+    for (int64_t b : found) {
+      pairs.push_back(W.cap_ids[i]);
+      pairs.push_back(b);
+    }
+    for (size_t p = 0; p < W.planes.size(); ++p)
+      if (overlaps(a.lo, a.hi, W.planes[p].lo, W.planes[p].hi)) {
+        pairs.push_back(W.cap_ids[i]);
+        pairs.push_back(R.n_slots + static_cast<int64_t>(p));
+      }
+  }
+}
+
+// Narrow phase and response for every capsule over its partners in
+// ascending id order (capsules, then planes), each pair evaluated with the
+// smaller id as the first body; then the loads per capsule (lab frame).
+void contact_loads(const OrcRods& R, const OrcContact& C, const ContactWorld& W, const std::vector<int64_t>& pairs,
+                   double* cf, double* ct, int nt) {
+  const int64_t S = R.n_slots;
+  std::vector<std::vector<int64_t>> adj(S);
+  for (size_t k = 0; k < pairs.size(); k += 2) {
+    adj[pairs[k]].push_back(pairs[k + 1]);
+    if (pairs[k + 1] < S) adj[pairs[k + 1]].push_back(pairs[k]);
+  }
+  for (int64_t s = 0; s < S; ++s) std::sort(adj[s].begin(), adj[s].end());
+  const int64_t nc = static_cast<int64_t>(W.cap_ids.size());
+  (void)nt;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
+#endif
+  for (int64_t q = 0; q < nc; ++q) {
+    const int64_t s = W.cap_ids[q];
+    const Capsule& me = W.caps[s];
+    V3 F = {0.0, 0.0, 0.0}, T = {0.0, 0.0, 0.0};
+    ContactPoint pts[2];
+    for (int64_t o : adj[s]) {
+      if (o < S) {
+        const bool first = s < o;
+        const Capsule& c1 = first ? me : W.caps[o];
+        const Capsule& c2 = first ? W.caps[o] : me;
+        const PairMaterial pm = pair_material(C, c1.material, c2.material);
+        const int np = rod_capsule_contacts(c1, c2, pts);
+        for (int k = 0; k < np; ++k) {
+          const V3 rvel = sub(point_velocity(c1, pts[k].pos), point_velocity(c2, pts[k].pos));
+          V3 net;
+          if (!spring_dashpot(pts[k], rvel, pm, net)) continue;
+          // Primitives/RigidBodyPrimitive.hpp:500-504 add_force_at_position
+          const V3 f = first ? net : neg3(net);
+          F = add3(F, f);
+          T = add3(T, cross(sub(pts[k].pos, me.c), f));
+        }
+      } else {
+        const Plane& P = W.planes[o - S];
+        const PairMaterial pm = pair_material(C, me.material, P.material);
+        const int np = capsule_plane_contacts(me, P, pts);
+        for (int k = 0; k < np; ++k) {
+          // the plane is fixed: zero velocity
+          const V3 rvel = sub(point_velocity(me, pts[k].pos), V3{0.0, 0.0, 0.0});
+          V3 net;
+          if (!spring_dashpot(pts[k], rvel, pm, net)) continue;
+          F = add3(F, net);
+          T = add3(T, cross(sub(pts[k].pos, me.c), net));
+        }
+      }
+    }
+    cf[s] = F.x;
+    cf[S + s] = F.y;
+    cf[2 * S + s] = F.z;
+    ct[s] = T.x;
+    ct[S + s] = T.y;
+    ct[2 * S + s] = T.z;
+  }
+}
+
+int check_contact(const OrcRods& R, const OrcContact* C) {
+  if (!C) return -1;
+  if (C->n_materials < 0 || (C->n_materials > 0 && !C->materials)) return -1;
+  if (C->n_planes < 0 || (C->n_planes > 0 && (!C->plane_point || !C->plane_normal || !C->plane_material)))
+    return -1;
+  for (int64_t r = 0; r < R.n_rods; ++r)
+    if (C->rod_material && C->rod_material[r] >= C->n_materials) return -1;
+  for (int32_t p = 0; p < C->n_planes; ++p)
+    if (C->plane_material[p] < 0 || C->plane_material[p] >= C->n_materials) return -1;
+  return 0;
+}
+
+// positions after a drift of c and the clamp's value constraint (a copy)
+std::vector<double> drifted_positions(const OrcRods& R, double c) {
+  const int64_t S = R.n_slots;
+  std::vector<double> x(R.x, R.x + 3 * S);
+  for (int64_t i = 0; i < 3 * S; ++i) x[i] = x[i] + c * R.v[i];
+  if (R.clamp)
+    for (int64_t r = 0; r < R.n_rods; ++r)
+      if (R.clamp[r])
+        for (int d = 0; d < 3; ++d) x[d * S + R.offset[r]] = R.clamp_x[3 * r + d];
+  return x;
+}
+
 }  // namespace
 
 extern "C" int orc_step(const OrcRods* rods, double dt, int64_t n_steps, int n_threads) {
@@ -450,6 +986,162 @@ extern "C" int orc_step(const OrcRods* rods, double dt, int64_t n_steps, int n_t
   }
   (void)n_threads;
   return 0;
+}
+
+extern "C" int orc_step_contact(const OrcRods* rods, const OrcContact* contact, double dt, int64_t n_steps,
+                                int n_threads) {
+  if (check(rods) != 0) return -1;
+  const OrcRods& R = *rods;
+  if (check_contact(R, contact) != 0) return -1;
+  const OrcContact& C = *contact;
+#ifdef _OPENMP
+  const int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#else
+  const int nt = 1;
+#endif
+  const int64_t S = R.n_slots;
+  std::vector<double> cf(3 * S, 0.0), ct(3 * S, 0.0);
+  ContactWorld W;
+  std::vector<int64_t> pairs;
+  for (int64_t step = 0; step < n_steps; ++step) {
+    // kinematic half step and value constraints of every rod first: the
+    // collision system sees all rods at the drifted state
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt)
+#endif
+    for (int64_t r = 0; r < R.n_rods; ++r) {
+      kinematic_half(R, r, dt);
+      clamp_values(R, r);
+    }
+    build_capsules(R, C, W, R.x);
+    pairs_grid(R, W, pairs);
+    contact_loads(R, C, W, pairs, cf.data(), ct.data(), nt);
+    if (step == n_steps - 1 && C.capsule_force && C.capsule_torque) {
+      std::copy(cf.begin(), cf.end(), C.capsule_force);
+      std::copy(ct.begin(), ct.end(), C.capsule_torque);
+    }
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt)
+#endif
+    {
+      Scratch sc;
+      std::vector<double> acc, alpha;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 16)
+#endif
+      for (int64_t r = 0; r < R.n_rods; ++r) {
+        const int64_t n = R.offset[r + 1] - R.offset[r] - 1;
+        acc.assign(3 * (n + 1), 0.0);
+        alpha.assign(3 * (n + 1), 0.0);
+        compute_dynamics(R, r, sc, acc.data(), alpha.data(), cf.data(), ct.data());
+        if (step == n_steps - 1) write_diagnostics(R, r, sc, acc.data(), alpha.data());
+        dynamic_update(R, r, dt, sc, acc.data(), alpha.data());
+        kinematic_half(R, r, dt);
+      }
+    }
+  }
+  return 0;
+}
+
+extern "C" int orc_contact_capsules(const OrcRods* rods, const OrcContact* contact, double half_dt, double* out) {
+  if (check(rods) != 0 || !out) return -1;
+  const OrcRods& R = *rods;
+  if (check_contact(R, contact) != 0) return -1;
+  const int64_t S = R.n_slots;
+  const std::vector<double> x = drifted_positions(R, half_dt);
+  ContactWorld W;
+  build_capsules(R, *contact, W, x.data());
+  for (int64_t s : W.cap_ids) {
+    const Capsule& k = W.caps[s];
+    const double vals[15] = {k.c.x, k.c.y, k.c.z, k.L, k.r, k.u.x, k.u.y, k.u.z,
+                             k.lo[0], k.lo[1], k.lo[2], k.hi[0], k.hi[1], k.hi[2], 0.0};
+    for (int f = 0; f < 14; ++f) out[f * S + s] = vals[f];
+  }
+  return 0;
+}
+
+extern "C" int64_t orc_contact_pairs(const OrcRods* rods, const OrcContact* contact, double half_dt, int exhaustive,
+                                     int64_t* pairs, int64_t capacity) {
+  if (check(rods) != 0) return -1;
+  const OrcRods& R = *rods;
+  if (check_contact(R, contact) != 0) return -1;
+  const std::vector<double> x = drifted_positions(R, half_dt);
+  ContactWorld W;
+  build_capsules(R, *contact, W, x.data());
+  std::vector<int64_t> p;
+  if (exhaustive)
+    pairs_exhaustive(R, W, p);
+  else
+    pairs_grid(R, W, p);
+  const int64_t n = static_cast<int64_t>(p.size() / 2);
+  for (int64_t k = 0; k < std::min(n, capacity); ++k) {
+    pairs[2 * k] = p[2 * k];
+    pairs[2 * k + 1] = p[2 * k + 1];
+  }
+  return n;
+}
+
+namespace {
+Capsule capsule_from_desc(const double* d) {
+  Capsule k;
+  k.c = {d[0], d[1], d[2]};
+  const Basis B = bases_from_tangent({d[3], d[4], d[5]});
+  k.u = B.r2;
+  k.r = d[6];
+  k.L = d[7];
+  k.vel = {d[8], d[9], d[10]};
+  const V3 w = {d[11], d[12], d[13]};
+  k.ww = {B.r0.x * w.x + B.r1.x * w.y + B.r2.x * w.z, B.r0.y * w.x + B.r1.y * w.y + B.r2.y * w.z,
+          B.r0.z * w.x + B.r1.z * w.y + B.r2.z * w.z};
+  k.material = 0;
+  return k;
+}
+void put_contacts(const ContactPoint* pts, int n, double* out) {
+  for (int i = 0; i < n; ++i) {
+    const double v[7] = {pts[i].pos.x, pts[i].pos.y, pts[i].pos.z, pts[i].n.x, pts[i].n.y, pts[i].n.z,
+                         pts[i].dist};
+    for (int k = 0; k < 7; ++k) out[7 * i + k] = v[k];
+  }
+}
+}  // namespace
+
+extern "C" int orc_fine_capsule_capsule(const double* a, const double* b, double* contacts) {
+  ContactPoint pts[2];
+  const int n = rod_capsule_contacts(capsule_from_desc(a), capsule_from_desc(b), pts);
+  if (contacts) put_contacts(pts, n, contacts);
+  return n;
+}
+
+extern "C" int orc_fine_capsule_plane(const double* capsule, const double* plane, double* contacts) {
+  ContactPoint pts[2];
+  const Plane P = make_plane({plane[0], plane[1], plane[2]}, {plane[3], plane[4], plane[5]}, 0);
+  const int n = capsule_plane_contacts(capsule_from_desc(capsule), P, pts);
+  if (contacts) put_contacts(pts, n, contacts);
+  return n;
+}
+
+extern "C" int orc_fine_pair_loads(const double* a, const double* b, const double* pmv, double* out) {
+  const Capsule c1 = capsule_from_desc(a), c2 = capsule_from_desc(b);
+  const PairMaterial pm = {pmv[0], pmv[1], pmv[2], pmv[3], pmv[4]};
+  ContactPoint pts[2];
+  const int n = rod_capsule_contacts(c1, c2, pts);
+  V3 F1 = {0.0, 0.0, 0.0}, T1 = F1, F2 = F1, T2 = F1;
+  for (int k = 0; k < n; ++k) {
+    const V3 rvel = sub(point_velocity(c1, pts[k].pos), point_velocity(c2, pts[k].pos));
+    V3 net;
+    if (!spring_dashpot(pts[k], rvel, pm, net)) continue;
+    F2 = add3(F2, neg3(net));
+    T2 = add3(T2, cross(sub(pts[k].pos, c2.c), neg3(net)));
+    F1 = add3(F1, net);
+    T1 = add3(T1, cross(sub(pts[k].pos, c1.c), net));
+  }
+  const V3 all[4] = {F1, T1, F2, T2};
+  for (int i = 0; i < 4; ++i) {
+    out[3 * i] = all[i].x;
+    out[3 * i + 1] = all[i].y;
+    out[3 * i + 2] = all[i].z;
+  }
+  return n;
 }
 
 extern "C" int orc_force_eval(const OrcRods* rods, int n_threads) {

@@ -89,6 +89,59 @@ int orc_force_eval(const OrcRods* rods, int n_threads);
  * translational, rotational, shear/stretch, bend/twist. */
 int orc_energy(const OrcRods* rods, double* out, int n_threads);
 
+/* ---- rod-rod and rod-plane contact (capsule collision system) ----------
+ *
+ * Every element of a participating rod is a capsule (centre = mid-point of
+ * its nodes, length = dilatation * rest length, radius = the element
+ * dimension, axis = the tangent).  Capsule ids are element slot indices;
+ * plane p has id n_slots + p in pair lists.  Pair lists hold (a, b) with
+ * a < b, sorted. */
+typedef struct OrcContactMaterial {
+  double stiffness, normal_damping, tangential_damping, static_friction, dynamic_friction;
+} OrcContactMaterial;
+
+typedef struct OrcContact {
+  int32_t n_materials;
+  const OrcContactMaterial* materials;
+  const int32_t* rod_material; /* n_rods; < 0 => the rod takes no part */
+  int32_t n_planes;
+  const double* plane_point;   /* 3 * n_planes (row-major [3p+c]) */
+  const double* plane_normal;  /* 3 * n_planes */
+  const int32_t* plane_material;
+  /* per element slot, lab frame, of the last force evaluation (NULL => skip) */
+  double* capsule_force;  /* 3*S */
+  double* capsule_torque; /* 3*S */
+} OrcContact;
+
+/* PositionVerlet steps with the collision system resolved inside every
+ * dynamic substep (after the internal forces, after gravity). */
+int orc_step_contact(const OrcRods* rods, const OrcContact* contact, double dt, int64_t n_steps,
+                     int n_threads);
+
+/* Capsules of the current state after a kinematic drift of half_dt (0: as
+ * is) and the clamp's value constraint, the way one step would build them:
+ * out[k*S + s] for k = 0..14 = centre(3), length, radius, axis(3), AABB
+ * min(3), AABB max(3); non-capsule slots are left untouched. */
+int orc_contact_capsules(const OrcRods* rods, const OrcContact* contact, double half_dt, double* out);
+
+/* Candidate pairs (closed AABB overlap) of those capsules, from an
+ * exhaustive search (exhaustive != 0) or a uniform grid.  Writes up to
+ * capacity pairs as (a, b) int64 couples and returns the total count, or -1. */
+int64_t orc_contact_pairs(const OrcRods* rods, const OrcContact* contact, double half_dt, int exhaustive,
+                          int64_t* pairs, int64_t capacity);
+
+/* Single-pair kernels for the reference's fine-detection and response
+ * tests.  A capsule is described by 14 doubles: centre(3), axis(3), radius,
+ * length, velocity(3), angular velocity(3) (body frame of the rotation built
+ * from the axis); a plane by point(3), normal(3).  Contacts are written as 7
+ * doubles each: position(3), normal(3), distance; the return value is their
+ * count.  orc_fine_pair_loads applies the spring-dashpot model with pair
+ * parameters pm = {k, c_n, c_t, mu_static, mu_dynamic} to every contact of
+ * the pair and writes force1(3), torque1(3), force2(3), torque2(3). */
+int orc_fine_capsule_capsule(const double* a, const double* b, double* contacts);
+int orc_fine_capsule_plane(const double* capsule, const double* plane, double* contacts);
+int orc_fine_pair_loads(const double* a, const double* b, const double* pm, double* out);
+
 /* Straight-rod initializer (reference Initializers/detail/Geometry.hpp and the
  * component initialize() chains).  Fills one rod of n elements:
  * x[3*(n+1)], Q[9*n], l0[n], D0[n-1], V[n], radius[n], mass[n+1],

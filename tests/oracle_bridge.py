@@ -46,6 +46,17 @@ def oracle_from_workload(wl, damped: bool = False, diagnostics: bool = False):
     return rods
 
 
+def contact_spec(wl):
+    """The oracle's collision-system description of a workload (None if the
+    workload has no contact)."""
+    if not wl.contact_materials:
+        return None
+    mats = [[m.stiffness, m.normal_damping, m.tangential_damping, m.static_friction, m.dynamic_friction]
+            for m in wl.contact_materials]
+    rod_mat = wl.contact_rod_material if wl.contact_rod_material is not None else [0] * len(wl.rods)
+    return oracle.ContactSpec(mats, rod_mat, list(wl.planes or []))
+
+
 STATE_MAP = {"Position": "x", "Velocity": "v", "Director": "Q", "AngularVelocity": "w"}
 
 
@@ -111,6 +122,20 @@ def oracle_spread(wl, n_steps, damped=False):
         p = oracle_from_workload(wl, damped=damped)
         p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
         p.step(wl.dt, n_steps)
+        for name, k, place in STATE_FIELDS:
+            spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
+    return base, spread
+
+
+def oracle_spread_contact(wl, n_steps):
+    """oracle_spread for a workload with a collision system (orc_step_contact)."""
+    base = oracle_from_workload(wl)
+    oracle.contact_step(base, contact_spec(wl), wl.dt, n_steps)
+    spread = {name: 0.0 for name, _, _ in STATE_FIELDS}
+    for key in ("x", "Q"):
+        p = oracle_from_workload(wl)
+        p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
+        oracle.contact_step(p, contact_spec(wl), wl.dt, n_steps)
         for name, k, place in STATE_FIELDS:
             spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
     return base, spread
