@@ -251,6 +251,68 @@ def mixed_comparison(W, eb, torch, args, rank, local, barrier, pg):
     return out
 
 
+def contact_comparison(W, eb, torch, args, rank, local, world, barrier, pg):
+    """The contact batch (8,192 free rods of 64 elements, six walls) on the
+    FP64 streaming step with the collision system.  Its dynamics diverges
+    within tens of microseconds in the reference's model (thin capsules,
+    contact torques on a 4e-11 kg m^2 element inertia), so every timed step
+    starts from the batch's initial state: the state is restored between
+    steps outside the timed region and each step is timed alone."""
+    wl = W.contact_batch(n_rods=args.contact_rods, seed=1004 + rank)
+    sim = wl.build(device=local)
+    names = ("Position", "Velocity", "Director", "AngularVelocity")
+    init = {n: sim.get_slots(n).copy() for n in names}
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
+    times = []
+    l0 = sim.launch_count()
+    for i in range(args.warmup + args.contact_steps):
+        for n in names:
+            sim.set_slots(n, init[n])
+        torch.cuda.synchronize()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(eb.PositionVerlet(), 0.0, wl.dt, 1)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(a.elapsed_time(b))
+    launches = (sim.launch_count() - l0) // (args.warmup + args.contact_steps)
+    ms = torch.tensor([sum(times) / len(times)], device="cuda")
+    if pg is not None:
+        pg.all_reduce(ms, op=pg.ReduceOp.MAX)
+    pairs = sim.contact_pairs()
+    n_slots = sim.n_slots()
+    force = sim.get_slots("ContactForce")
+    out = {"workload": "contact_batch", "rods": len(wl.rods), "capsules": wl.total_elements, "dt": wl.dt,
+           "planes": len(wl.planes), "seed": wl.seed,
+           "value": world * wl.total_elements / (float(ms.item()) / 1e3), "unit": UNIT,
+           "ms_per_step": float(ms.item()), "steps_timed": args.contact_steps,
+           "launches_per_step": int(launches),
+           "candidate_pairs": int(pairs.shape[0]),
+           "capsule_plane_pairs": int((pairs[:, 1] >= n_slots).sum()),
+           "capsules_with_contact_force": int(np.count_nonzero(np.abs(force).sum(axis=0))),
+           "timing": "each step from the initial state (state restored between steps, outside the timing)",
+           "parity": "candidate pair set bit-exact and capsule loads equal to the oracle (tests/test_gpu_contact.py)"}
+    sim.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle  # noqa: F401  (checker / CPU baseline only)
+        import oracle_bridge as ob
+
+        orc = ob.oracle_from_workload(wl)
+        spec = ob.contact_spec(wl)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.contact_step(orc, spec, wl.dt, 1, n_threads=cores)
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": wl.total_elements / el, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": "one contact step of the whole batch (CPU restatement: uniform-grid "
+                                         "broad phase, narrow phase, spring-dashpot, rod step)"}
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -267,6 +329,9 @@ def main(argv=None) -> int:
     ap.add_argument("--mixed-rods", type=int, default=65536, help="rods of the mixed-precision batch")
     ap.add_argument("--mixed-steps", type=int, default=10000,
                     help="steps of the FP64-vs-mixed comparison on the mixed batch; 0 skips it")
+    ap.add_argument("--contact-rods", type=int, default=8192, help="rods of the contact batch")
+    ap.add_argument("--contact-steps", type=int, default=10,
+                    help="timed steps of the contact batch (each from its initial state); 0 skips it")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-rounding", action="store_true",
@@ -415,6 +480,10 @@ def main(argv=None) -> int:
     if args.mixed_steps > 0:
         mixed = mixed_comparison(W, eb, torch, args, rank, local, barrier, pg)
 
+    contact = None
+    if args.contact_steps > 0:
+        contact = contact_comparison(W, eb, torch, args, rank, local, world, barrier, pg)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, sample = cpu_reference_rate(wl, 0, budget_s=args.cpu_budget_s, max_rods=2048)
@@ -445,6 +514,7 @@ def main(argv=None) -> int:
             "state_finite": bool(finite),
             "batched": batched,
             "mixed": mixed,
+            "contact": contact,
         }
         print(json.dumps(line), flush=True)
     if sim is not None:

@@ -200,12 +200,25 @@ __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
   const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
   if (s >= a.n_slots || a.cap_material[s] < 0) return;
   const int64_t S = a.stride;
+  // a capsule whose box is not finite (a diverged state, already flagged by
+  // the capsule kernel) takes no part: it would overlap every box
+  bool finite = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lo = a.cap[(kCapLo + d) * S + s], hi = a.cap[(kCapHi + d) * S + s];
+    finite = finite && (hi - lo >= 0.0) && (hi - lo < 1e300) && (fabs(lo) < 1e300);
+  }
+  if (!finite) {
+    a.bucket[s] = 0xffffffffu;
+    a.pair_count[s] = 0;
+    return;
+  }
   const double ih = inverse_cell(a);
   int32_t c[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     double f = floor(a.cap[(kCapLo + d) * S + s] * ih);
-    f = fmin(fmax(f, -kCellClamp), kCellClamp);  // a NaN becomes -2^30 (and is flagged)
+    f = fmin(fmax(f, -kCellClamp), kCellClamp);
     c[d] = static_cast<int32_t>(f);
     a.cell[d * S + s] = c[d];
   }
@@ -219,6 +232,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) 
   if (s >= a.n_slots || a.cap_material[s] < 0) return;
   const int64_t S = a.stride;
   const uint32_t b = a.bucket[s];
+  if (b > a.table_mask) return;  // excluded (not finite)
   // bucket_count was zeroed by the scan and now serves as the fill cursor
   const int32_t pos = a.bucket_start[b] + atomicAdd(a.bucket_count + b, 1);
   if (pos < 0 || pos >= a.n_caps) {  // cannot happen with consistent counts; never write out of range
@@ -237,7 +251,9 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) 
 // ---- stage 3: candidate pairs ----------------------------------------------
 
 template <bool kWrite>
-__global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps) {
+__global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps_max) {
+  // entries filed this evaluation (the capsules with finite boxes)
+  const int32_t n_caps = min(a.bucket_start[a.table_mask + 1], n_caps_max);
   const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
   if (e >= n_caps) return;
   const int32_t id = a.sorted_id[e];
