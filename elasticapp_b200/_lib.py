@@ -111,6 +111,8 @@ SIGNATURES = {
     "eb_get_stream": ([_sim, _P(ctypes.c_void_p)], ctypes.c_int),
     "eb_step_plan": ([_sim, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_float), ctypes.c_int32], ctypes.c_int),
     "eb_launch_count": ([_sim, _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_box_pairs_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                              _P(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
 }
 
 

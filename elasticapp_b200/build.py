@@ -29,6 +29,7 @@ SOURCES = [
     # rounded as written (no contracted multiply-adds): capsules, boxes and
     # candidate pairs bit-identical to a scalar FP64 evaluation
     ("contact.o", "contact.cu", ["--fmad=false"]),
+    ("box_pairs_noalloc.o", "box_pairs_noalloc.cu", []),
 ]
 HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -485,6 +485,10 @@ eb_status setup_contact(eb_sim* s) {
 
 }  // namespace
 
+namespace eb {
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace eb
+
 extern "C" {
 
 EB_API const char* eb_last_error(void) { return g_last_error.c_str(); }

@@ -297,6 +297,30 @@ EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* 
 /* Number of kernel launches this simulator has issued (diagnostic). */
 EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);
 
+/* --- candidate pairs of caller-provided boxes, allocating nothing.  No
+ * counterpart in the reference: it is the collision system's broad phase
+ * (the search behind eb_contact_pairs) for callers that cannot allocate device
+ * memory, for example operators inside a host framework that reserves the
+ * whole GPU memory pool and hands them their buffers, or loops that cannot
+ * take the device-wide synchronisation of cudaMalloc / cudaFree.  Its working
+ * memory is a fixed 16 MiB device array inside the library, held by every GPU
+ * that loads it until the process exits.
+ *
+ * boxes: device pointer, n_boxes boxes of 6 doubles (lo x, lo y, lo z,
+ * hi x, hi y, hi z), closed intervals, finite, hi >= lo.  n_boxes <= 131072
+ * (larger counts are rejected with EB_ERR_INVALID_ARGUMENT).  pairs: device
+ * pointer to capacity pairs of int64 (i, j), i < j; the overlapping pairs are
+ * written sorted by i then j.  *count (host) receives their number; when it
+ * exceeds capacity nothing is written and EB_ERR_INVALID_ARGUMENT is
+ * returned.  stream: a cudaStream_t of the current device (NULL = default
+ * stream); the call returns after its work on the stream has finished.
+ * The first call on a device finds the device address of the working array
+ * (make it before any stream capture begins).  Every call shares that array:
+ * calls whose GPU work overlaps (other streams or host threads) race and must
+ * be serialised by the caller. */
+EB_API eb_status eb_box_pairs_noalloc(const double* boxes, int64_t n_boxes, int64_t* pairs, int64_t capacity,
+                                      int64_t* count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
