@@ -78,6 +78,38 @@ class EbContactMaterial(ctypes.Structure):
                 ("dynamic_friction", ctypes.c_double)]
 
 
+class EbServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("steps_per_launch", ctypes.c_int32),
+                ("flags", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_double),
+                ("energy_tolerance", ctypes.c_double)]
+
+
+class EbRequest(ctypes.Structure):
+    _fields_ = [("rods", ctypes.POINTER(EbStraightRod)), ("n_rods", ctypes.c_int64),
+                ("velocities", ctypes.POINTER(ctypes.c_double)), ("dt", ctypes.c_double),
+                ("n_steps", ctypes.c_int64), ("gravity", ctypes.c_double * 3), ("options", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("damper_translational", ctypes.c_double),
+                ("damper_rotational", ctypes.c_double)]
+
+
+class EbCompletion(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_int64), ("precision", ctypes.c_int32), ("fell_back", ctypes.c_int32),
+                ("latency_s", ctypes.c_double), ("energy_initial", ctypes.c_double),
+                ("energy_final", ctypes.c_double), ("elements", ctypes.c_int64), ("steps", ctypes.c_int64)]
+
+
+class EbServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("queued", "active", "finishing", "completed", "fallbacks",
+                                               "bins_total", "bins_used", "ticks")] + \
+               [("element_steps", ctypes.c_double)]
+
+
+EB_SERVER_FORCE_FALLBACK = 0x1
+EB_REQUEST_CLAMP = 0x1
+EB_REQUEST_DAMPER = 0x2
+EB_REQUEST_GRAVITY = 0x4
+
+
 # every entry point of include/elastica_b200.h with its ctypes signature
 _P = ctypes.POINTER
 _sim = ctypes.c_void_p
@@ -111,6 +143,15 @@ SIGNATURES = {
     "eb_get_stream": ([_sim, _P(ctypes.c_void_p)], ctypes.c_int),
     "eb_step_plan": ([_sim, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_float), ctypes.c_int32], ctypes.c_int),
     "eb_launch_count": ([_sim, _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_server_create": ([_P(EbServerConfig), _P(ctypes.c_void_p)], ctypes.c_int),
+    "eb_server_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "eb_server_submit": ([ctypes.c_void_p, _P(EbRequest), _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_server_tick": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_server_poll": ([ctypes.c_void_p, _P(EbCompletion), ctypes.c_int32, _P(ctypes.c_int32)], ctypes.c_int),
+    "eb_server_result": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P(ctypes.c_double),
+                          ctypes.c_int64], ctypes.c_int),
+    "eb_server_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "eb_server_get_stats": ([ctypes.c_void_p, _P(EbServerStats)], ctypes.c_int),
     "eb_box_pairs_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                               _P(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
 }

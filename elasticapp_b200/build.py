@@ -30,8 +30,9 @@ SOURCES = [
     # candidate pairs bit-identical to a scalar FP64 evaluation
     ("contact.o", "contact.cu", ["--fmad=false"]),
     ("box_pairs_noalloc.o", "box_pairs_noalloc.cu", []),
+    ("serve.o", "serve.cu", []),
 ]
-HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h"]
+HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h", "eb_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -18,6 +18,7 @@
 
 #include "../../include/elastica_b200.h"
 #include "contact.h"
+#include "eb_host.h"
 #include "eb_internal.h"
 
 namespace eb {
@@ -487,6 +488,16 @@ eb_status setup_contact(eb_sim* s) {
 
 namespace eb {
 void set_last_error(const std::string& message) { g_last_error = message; }
+
+eb_status host_straight_rod(const eb_straight_rod& p, HostRodData& out) {
+  RodHost r;
+  if (eb_status st = init_straight_rod(p, r)) return st;
+  out.n = r.n;
+  out.damped = r.model == EB_ROD_DAMPED;
+  out.state = std::move(r.state);
+  out.param = std::move(r.param);
+  return EB_OK;
+}
 }  // namespace eb
 
 extern "C" {

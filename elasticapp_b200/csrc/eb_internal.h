@@ -105,6 +105,20 @@ struct StepArgs {
   const double* contact_torque;
 };
 
+// Per-CTA work of the serving launches (resident kernels): the CTA's slot
+// range, its step count for this launch and the time step and environment of
+// the request that owns it.
+struct ServeCta {
+  int64_t start;  // first slot
+  int32_t count;  // slots
+  int32_t steps;  // steps to run in this launch (>= 1)
+  double dt;
+  double half_dt;
+  double gravity[3];
+  uint32_t flags;  // kSim* bits of the request
+  uint32_t pad;
+};
+
 // device status bits reported back to the host
 enum StatusBits : uint32_t {
   kStatusCopyTimeout = 1u,

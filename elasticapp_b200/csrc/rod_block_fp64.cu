@@ -71,16 +71,37 @@ __device__ __forceinline__ int param_row(int f) {
   return -1;  // volume: only read for diagnostics, straight from global memory
 }
 
-template <int kCap, int kThreads, bool kDamped, bool kSplit>
+// kServe: the CTA's slot range, step count, time step and environment come
+// from serve[blockIdx.x] (serving launches)
+template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe>
 __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
-                                                                    int n_steps) {
+                                                                    int n_steps_launch, const ServeCta* serve) {
   extern __shared__ __align__(128) double smem[];
   const BRows<kCap> R{smem};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + bRows * kCap);
 
   const int tid = threadIdx.x;
-  const int64_t g0 = cta_start[blockIdx.x];
-  const int count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
+  int64_t g0;
+  int count, n_steps = n_steps_launch;
+  double dt = a.dt, hdt = a.half_dt;
+  uint32_t flags = a.sim_flags;
+  double gvec[3] = {a.gravity[0], a.gravity[1], a.gravity[2]};
+  if constexpr (kServe) {
+    const ServeCta& sc = serve[blockIdx.x];
+    g0 = sc.start;
+    count = sc.count;
+    n_steps = min(n_steps_launch, sc.steps);
+    dt = sc.dt;
+    hdt = sc.half_dt;
+    flags = sc.flags;
+    gvec[0] = sc.gravity[0];
+    gvec[1] = sc.gravity[1];
+    gvec[2] = sc.gravity[2];
+  } else {
+    g0 = cta_start[blockIdx.x];
+    count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
+  }
+  if (n_steps <= 0) return;
   const int64_t S = a.stride;
 
   // ---- stage state, parameters and slot metadata (coalesced loads)
@@ -98,8 +119,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
   __syncthreads();
 
-  const double dt = a.dt, hdt = a.half_dt;
-  const bool any_rod = (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
+  const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
 
   for (int step = 0; step < n_steps; ++step) {
     // ---- drift: half on the first step; afterwards the merged full drift,
@@ -208,7 +228,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         const double cf = m * R.at(bNuF, s);
         F = {F.x - cf * v.x, F.y - cf * v.y, F.z - cf * v.z};
       }
-      if (a.sim_flags & kSimGravity) F = F + D3{a.gravity[0] * m, a.gravity[1] * m, a.gravity[2] * m};
+      if (flags & kSimGravity) F = F + D3{gvec[0] * m, gvec[1] * m, gvec[2] * m};
       const double im = 1.0 / m;
       v = {v.x + dt * (F.x * im), v.y + dt * (F.y * im), v.z + dt * (F.z * im)};
       D3 w{0.0, 0.0, 0.0};
@@ -298,18 +318,18 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
 }
 
-template <int kCap, int kThreads, bool kSplit>
+template <int kCap, int kThreads, bool kSplit, bool kServe = false>
 cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, const ServeCta* serve = nullptr) {
   const size_t bytes = size_t(bRows) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps);
+    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve);
     return cudaGetLastError();
   };
-  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit>)
-                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit>);
+  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe>)
+                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe>);
 }
 
 }  // namespace
@@ -338,6 +358,13 @@ cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start
     case 3: return launch_block_cfg<264, 288, true>(args, cta_start, n_ctas, n_steps, damped, stream);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// Serving launches (see launch_rod_block_mixed_serve): 520-slot CTAs.
+cudaError_t launch_rod_block_fp64_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
+                                        bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  return launch_block_cfg<520, 256, true, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
 }
 
 }  // namespace eb

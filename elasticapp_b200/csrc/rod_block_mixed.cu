@@ -178,21 +178,43 @@ __device__ __forceinline__ int mixed_param_row(int f) {
   return -1;
 }
 
-template <int kCap, int kThreads, int kMinBlocks, bool kDamped>
+// kServe: the CTA's slot range, step count, time step and environment come
+// from serve[blockIdx.x] (serving launches) instead of the work list and the
+// launch-wide values
+template <int kCap, int kThreads, int kMinBlocks, bool kDamped, bool kServe>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
-    rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps) {
+    rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps_launch, const ServeCta* serve) {
   extern __shared__ __align__(128) double smem[];
   const MRows<kCap> R{smem, reinterpret_cast<float*>(smem + dRowsD * kCap)};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + fRowsF * kCap);
   uint32_t* rflag_s = meta_s + kCap;
 
   const int tid = threadIdx.x;
-  const int64_t g0 = cta_start[blockIdx.x];
-  const int count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
+  int64_t g0;
+  int count, n_steps = n_steps_launch;
+  double dt = a.dt, hdt = a.half_dt;
+  uint32_t flags = a.sim_flags;
+  double gvec[3] = {a.gravity[0], a.gravity[1], a.gravity[2]};
+  if constexpr (kServe) {
+    const ServeCta& sc = serve[blockIdx.x];
+    g0 = sc.start;
+    count = sc.count;
+    n_steps = min(n_steps_launch, sc.steps);
+    dt = sc.dt;
+    hdt = sc.half_dt;
+    flags = sc.flags;
+    gvec[0] = sc.gravity[0];
+    gvec[1] = sc.gravity[1];
+    gvec[2] = sc.gravity[2];
+  } else {
+    g0 = cta_start[blockIdx.x];
+    count = static_cast<int>(cta_start[blockIdx.x + 1] - g0);
+  }
+  if (n_steps <= 0) return;
   const int64_t S = a.stride;
 
   // ---- stage state, parameters, reciprocals, FP32 copies and rod data
-  const bool any_rod = (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
+  const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
   for (int s = tid; s < count; s += kThreads) {
     const int64_t g = g0 + s;
     const uint32_t meta = a.meta[g];
@@ -233,10 +255,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
   __syncthreads();
 
-  const double dt = a.dt, hdt = a.half_dt;
   const float dtf = static_cast<float>(dt);
-  const F3 grav = {static_cast<float>(a.gravity[0]), static_cast<float>(a.gravity[1]),
-                   static_cast<float>(a.gravity[2])};
+  const F3 grav = {static_cast<float>(gvec[0]), static_cast<float>(gvec[1]), static_cast<float>(gvec[2])};
 
   // ---- first half drift of the first step and the clamp's value constraint
   for (int s = tid; s < count; s += kThreads) {
@@ -351,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const F3 vf = tof(v);
         F = {F.x - cf * vf.x, F.y - cf * vf.y, F.z - cf * vf.z};
       }
-      if (a.sim_flags & kSimGravity) F = F + F3{grav.x * m, grav.y * m, grav.z * m};
+      if (flags & kSimGravity) F = F + F3{grav.x * m, grav.y * m, grav.z * m};
       const float im = R.af(fInvMass, s);
       v = {v.x + dt * static_cast<double>(F.x * im), v.y + dt * static_cast<double>(F.y * im),
            v.z + dt * static_cast<double>(F.z * im)};
@@ -415,19 +435,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
 }
 
-template <int kCap, int kThreads, int kMinBlocks>
+template <int kCap, int kThreads, int kMinBlocks, bool kServe = false>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, const ServeCta* serve = nullptr) {
   const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(fRowsF) * kCap * sizeof(float) +
                        2 * size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps);
+    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve);
     return cudaGetLastError();
   };
-  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true>)
-                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false>);
+  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true, kServe>)
+                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false, kServe>);
 }
 
 }  // namespace
@@ -445,6 +465,14 @@ cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_star
     case 3: return launch_mixed_cfg<264, 288, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// Serving launches: CTA c runs serve[c] (its request's slot range, time step,
+// environment and min(n_steps, serve[c].steps) steps); 520-slot CTAs.
+cudaError_t launch_rod_block_mixed_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
+                                         bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  return launch_mixed_cfg<520, 256, 1, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
 }
 
 }  // namespace eb

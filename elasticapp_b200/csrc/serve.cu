@@ -1,0 +1,733 @@
+// Serving: continuous batching of rod-assembly simulations on one GPU.
+//
+// Requests (a set of straight rods, a time step, a horizon, gravity, clamp
+// and damper options) arrive at any time.  The server owns a device pool of
+// bins, each 520 slots (one CTA of the resident step kernels), sized from an
+// HBM budget at creation.  A request is admitted when enough bins are free:
+// its rods are packed into its own bins (next fit), initialised on the host
+// and copied in, and its initial energy is computed on the device.  Every
+// tick is one launch of the resident kernel per precision (mixed, and FP64
+// for requests that fell back) over the bins of every active request: each
+// CTA reads its bin, step count, time step and environment from a per-CTA
+// table, so requests of different sizes, time steps and horizons share the
+// launch.  A request advances steps_per_launch steps per tick, counted from
+// its own admission, so its result does not depend on what else is running.
+//
+// Retirement needs no host round trip: the host knows from the step counts
+// which requests finish in a tick; right after that tick's launch it enqueues,
+// on the same stream, their final energies and a copy of their state into a
+// pinned host arena, records an event and returns their bins to the free list
+// (stream order keeps the copy ahead of any later reuse).  eb_server_poll
+// checks the events without blocking.  A mixed-precision result whose
+// mechanical energy (kinetic, elastic and gravitational) grew by more than
+// the tolerance, or is not finite, is run again in FP64 from its initial
+// conditions.  At most two ticks are in flight.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/elastica_b200.h"
+#include "eb_host.h"
+#include "eb_internal.h"
+
+namespace eb {
+cudaError_t launch_rod_block_mixed_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
+                                         bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_fp64_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
+                                        bool damped, cudaStream_t stream);
+cudaError_t launch_rod_energy_list(int64_t n_rods, int64_t stride, const int64_t* start, const int32_t* n_el,
+                                   const double* state, const double* params, const double gravity[3], double* out,
+                                   cudaStream_t stream);
+}  // namespace eb
+
+namespace {
+
+constexpr int64_t kBin = 520;                 // slots per bin (one CTA)
+constexpr int64_t kRodsPerBin = kBin / 3;     // a rod takes at least 3 slots
+constexpr size_t kArenaBytes = size_t(1) << 30;  // pinned result arena
+using Clock = std::chrono::steady_clock;
+
+eb_status fail(eb_status st, const std::string& m) {
+  eb::set_last_error(m);
+  return st;
+}
+
+#define SV_CUDA(call)                                                                             \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(EB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// first-fit allocator of contiguous id ranges
+struct RangeAlloc {
+  std::map<int64_t, int64_t> free_;  // start -> length
+  void init(int64_t cap) {
+    free_.clear();
+    if (cap > 0) free_[0] = cap;
+  }
+  int64_t alloc(int64_t n) {
+    for (auto it = free_.begin(); it != free_.end(); ++it)
+      if (it->second >= n) {
+        const int64_t s = it->first, len = it->second;
+        free_.erase(it);
+        if (len > n) free_[s + n] = len - n;
+        return s;
+      }
+    return -1;
+  }
+  void release(int64_t s, int64_t n) {
+    auto it = free_.emplace(s, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && s + n == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+// FIFO ring of pinned host memory (allocations are freed in order)
+struct Ring {
+  unsigned char* base = nullptr;
+  size_t cap = 0, head = 0, tail = 0, used = 0;
+  std::deque<std::pair<size_t, size_t>> live;  // (offset, bytes incl. wrap padding)
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) / 256 * 256;
+    if (bytes > cap) return false;
+    size_t pad = 0;
+    if (head + bytes > cap) pad = cap - head;  // wrap
+    if (used + pad + bytes > cap) return false;
+    if (pad) {
+      head = 0;
+      used += pad;
+    }
+    *off = head;
+    live.emplace_back(head, bytes + pad);
+    head = (head + bytes) % cap;
+    used += bytes;
+    return true;
+  }
+  void free_oldest() {
+    if (live.empty()) return;
+    used -= live.front().second;
+    live.pop_front();
+    if (live.empty()) head = tail = used = 0;
+  }
+};
+
+enum ReqState { kQueued = 0, kActive = 1, kFinishing = 2, kDone = 3 };
+
+struct Request {
+  int64_t id = 0;
+  std::vector<eb_straight_rod> rods;
+  std::vector<double> velocities;  // concatenated per rod 3 x (n + 1), or empty
+  double dt = 0.0;
+  int64_t n_steps = 0;
+  double gravity[3] = {0.0, 0.0, 0.0};
+  uint32_t options = 0;
+  double nu_t = 0.0, nu_r = 0.0;
+  int precision = EB_PRECISION_MIXED;
+  bool fell_back = false;
+  bool damped = false;
+  Clock::time_point t_submit;
+  double latency_s = 0.0;
+  ReqState state = kQueued;
+  // placement
+  std::vector<int64_t> bins;
+  std::vector<int32_t> bin_count;
+  std::vector<int64_t> rod_bin, rod_off;  // bin and slot offset inside it, per rod
+  int64_t rod0 = -1;
+  int64_t elements = 0;
+  int64_t steps_done = 0;
+  // completion
+  cudaEvent_t event = nullptr;
+  size_t arena_off = 0;
+  double e0 = 0.0, e1 = 0.0, escale = 0.0;
+  std::vector<double> result;  // per rod, kStateFields rows of n + 1 slots
+  std::vector<int64_t> result_off;
+};
+
+}  // namespace
+
+struct eb_server {
+  eb_server_config cfg{};
+  cudaStream_t stream = nullptr;
+  int64_t n_bins = 0, n_slots = 0, stride = 0, rod_cap = 0;
+  double* state[2] = {nullptr, nullptr};
+  double* par = nullptr;
+  uint32_t* meta = nullptr;
+  eb::RodInfo* rods = nullptr;
+  int64_t* rod_start = nullptr;
+  int32_t* rod_n = nullptr;
+  double* e0 = nullptr;
+  double* e1 = nullptr;
+  uint32_t* status = nullptr;
+  eb::ServeCta* d_cta[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][precision]
+  eb::ServeCta* h_cta[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  cudaEvent_t tick_event[2] = {nullptr, nullptr};
+  bool tick_pending[2] = {false, false};
+  int cur = 0;
+  int64_t ticks = 0;
+  Ring arena;
+  std::vector<int64_t> free_bins;
+  RangeAlloc rod_ids;
+  int64_t next_id = 1;
+  std::map<int64_t, std::unique_ptr<Request>> requests;
+  std::deque<Request*> queue;
+  std::vector<Request*> active;
+  std::deque<Request*> finishing;
+  std::deque<eb_completion> completed;
+  int64_t n_completed = 0, n_fallbacks = 0;
+  double element_steps = 0.0;
+};
+
+namespace {
+
+void server_free(eb_server* s) {
+  cudaSetDevice(s->cfg.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  void* dev[] = {s->state[0], s->state[1], s->par, s->meta, s->rods, s->rod_start, s->rod_n, s->e0, s->e1, s->status};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      if (s->d_cta[a][b]) cudaFree(s->d_cta[a][b]);
+      if (s->h_cta[a][b]) cudaFreeHost(s->h_cta[a][b]);
+    }
+  for (auto& kv : s->requests)
+    if (kv.second->event) cudaEventDestroy(kv.second->event);
+  for (auto& e : s->tick_event)
+    if (e) cudaEventDestroy(e);
+  if (s->arena.base) cudaFreeHost(s->arena.base);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// next-fit packing of the request's rods into bins
+void pack(Request& r) {
+  r.bins.clear();
+  r.bin_count.clear();
+  r.rod_bin.assign(r.rods.size(), 0);
+  r.rod_off.assign(r.rods.size(), 0);
+  int64_t used = kBin;
+  for (size_t k = 0; k < r.rods.size(); ++k) {
+    const int64_t w = r.rods[k].n_elements + 1;
+    if (used + w > kBin) {
+      r.bin_count.push_back(0);
+      used = 0;
+    }
+    r.rod_bin[k] = static_cast<int64_t>(r.bin_count.size()) - 1;
+    r.rod_off[k] = used;
+    used += w;
+    r.bin_count.back() = static_cast<int32_t>(used);
+  }
+}
+
+uint32_t request_flags(const Request& r) {
+  uint32_t f = 0;
+  if (r.options & EB_REQUEST_GRAVITY) f |= eb::kSimGravity;
+  if (r.options & EB_REQUEST_CLAMP) f |= eb::kSimClamp;
+  if (r.options & EB_REQUEST_DAMPER) f |= eb::kSimDamper;
+  return f;
+}
+
+// Copy the request's initial rods into its bins and compute its initial energy.
+eb_status place(eb_server* s, Request& r) {
+  const int64_t S = s->stride;
+  std::vector<std::vector<double>> st(r.bin_count.size()), pr(r.bin_count.size());
+  std::vector<std::vector<uint32_t>> mt(r.bin_count.size());
+  for (size_t b = 0; b < r.bin_count.size(); ++b) {
+    const int64_t c = r.bin_count[b];
+    st[b].assign(static_cast<size_t>(eb::kStateFields * c), 0.0);
+    pr[b].assign(static_cast<size_t>(eb::kParamFields * c), 0.0);
+    mt[b].assign(static_cast<size_t>(c), 0u);
+  }
+  std::vector<eb::RodInfo> info(r.rods.size());
+  std::vector<int64_t> rstart(r.rods.size());
+  std::vector<int32_t> rn(r.rods.size());
+  size_t voff = 0;
+  for (size_t k = 0; k < r.rods.size(); ++k) {
+    eb::HostRodData h;
+    if (eb_status e = eb::host_straight_rod(r.rods[k], h)) return e;
+    const int64_t n = h.n, W = n + 1, b = r.rod_bin[k], o = r.rod_off[k], c = r.bin_count[b];
+    if (!r.velocities.empty()) {
+      for (int d = 0; d < 3; ++d)
+        for (int64_t j = 0; j <= n; ++j) h.state[(eb::kStV + d) * W + j] = r.velocities[voff + d * W + j];
+      voff += static_cast<size_t>(3 * W);
+    }
+    for (int f = 0; f < eb::kStateFields; ++f)
+      std::memcpy(&st[b][f * c + o], &h.state[f * W], W * sizeof(double));
+    for (int f = 0; f < eb::kParamFields; ++f)
+      std::memcpy(&pr[b][f * c + o], &h.param[f * W], W * sizeof(double));
+    const int64_t rid = r.rod0 + static_cast<int64_t>(k);
+    for (int64_t j = 0; j <= n; ++j) {
+      uint32_t m = static_cast<uint32_t>(rid) << eb::kRodShift;
+      if (j < n) m |= eb::kElem;
+      if (j < n - 1) m |= eb::kVor;
+      if (j == 0) m |= eb::kFirst;
+      if (j == n) m |= eb::kLastNode;
+      if (j == n - 1) m |= eb::kLastElem;
+      mt[b][o + j] = m;
+    }
+    eb::RodInfo& ri = info[k];
+    std::memset(&ri, 0, sizeof(ri));
+    for (int d = 0; d < 3; ++d) ri.clamp_x[d] = h.state[(eb::kStX + d) * W];
+    for (int q = 0; q < 9; ++q) ri.clamp_Q[q] = h.state[(eb::kStQ + q) * W];
+    ri.damper_t = 1.0;
+    if (r.options & EB_REQUEST_CLAMP) ri.flags |= eb::kRodClamp;
+    if (r.options & EB_REQUEST_DAMPER) {
+      ri.flags |= eb::kRodDamper;
+      ri.damper_t = std::exp(-r.nu_t * r.dt);
+      ri.damper_r = r.nu_r;
+    }
+    rstart[k] = r.bins[b] * kBin + o;
+    rn[k] = static_cast<int32_t>(n);
+    if (h.damped) r.damped = true;
+  }
+  for (size_t b = 0; b < r.bin_count.size(); ++b) {
+    const int64_t c = r.bin_count[b], g0 = r.bins[b] * kBin;
+    const size_t pitch = static_cast<size_t>(S) * sizeof(double), w = static_cast<size_t>(c) * sizeof(double);
+    SV_CUDA(cudaMemcpy2DAsync(s->state[s->cur] + g0, pitch, st[b].data(), w, w, eb::kStateFields,
+                              cudaMemcpyHostToDevice, s->stream));
+    SV_CUDA(cudaMemcpy2DAsync(s->par + g0, pitch, pr[b].data(), w, w, eb::kParamFields, cudaMemcpyHostToDevice,
+                              s->stream));
+    SV_CUDA(cudaMemcpyAsync(s->meta + g0, mt[b].data(), c * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  }
+  const size_t nr = r.rods.size();
+  SV_CUDA(cudaMemcpyAsync(s->rods + r.rod0, info.data(), nr * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
+  SV_CUDA(cudaMemcpyAsync(s->rod_start + r.rod0, rstart.data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice,
+                          s->stream));
+  SV_CUDA(cudaMemcpyAsync(s->rod_n + r.rod0, rn.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+  const double g[3] = {(r.options & EB_REQUEST_GRAVITY) ? r.gravity[0] : 0.0,
+                       (r.options & EB_REQUEST_GRAVITY) ? r.gravity[1] : 0.0,
+                       (r.options & EB_REQUEST_GRAVITY) ? r.gravity[2] : 0.0};
+  SV_CUDA(eb::launch_rod_energy_list(static_cast<int64_t>(nr), S, s->rod_start + r.rod0, s->rod_n + r.rod0,
+                                     s->state[s->cur], s->par, g, s->e0 + 5 * r.rod0, s->stream));
+  return EB_OK;
+}
+
+eb_status admit(eb_server* s) {
+  while (!s->queue.empty()) {
+    Request& r = *s->queue.front();
+    pack(r);
+    if (static_cast<int64_t>(r.bin_count.size()) > static_cast<int64_t>(s->free_bins.size())) break;
+    const int64_t rid = s->rod_ids.alloc(static_cast<int64_t>(r.rods.size()));
+    if (rid < 0) break;
+    r.rod0 = rid;
+    r.bins.clear();
+    for (size_t b = 0; b < r.bin_count.size(); ++b) {
+      r.bins.push_back(s->free_bins.back());
+      s->free_bins.pop_back();
+    }
+    r.steps_done = 0;
+    r.damped = false;
+    if (eb_status e = place(s, r)) return e;
+    r.state = kActive;
+    s->queue.pop_front();
+    s->active.push_back(&r);
+  }
+  return EB_OK;
+}
+
+eb_status poll_events(eb_server* s, bool block_oldest);
+
+// Enqueue the retirement of a request whose last step ran in this tick.
+eb_status retire(eb_server* s, Request& r) {
+  const int64_t S = s->stride, nr = static_cast<int64_t>(r.rods.size());
+  const double g[3] = {(r.options & EB_REQUEST_GRAVITY) ? r.gravity[0] : 0.0,
+                       (r.options & EB_REQUEST_GRAVITY) ? r.gravity[1] : 0.0,
+                       (r.options & EB_REQUEST_GRAVITY) ? r.gravity[2] : 0.0};
+  SV_CUDA(eb::launch_rod_energy_list(nr, S, s->rod_start + r.rod0, s->rod_n + r.rod0, s->state[s->cur], s->par, g,
+                                     s->e1 + 5 * r.rod0, s->stream));
+  size_t slots = 0;
+  for (int32_t c : r.bin_count) slots += static_cast<size_t>(c);
+  const size_t bytes = (slots * eb::kStateFields + 10 * static_cast<size_t>(nr)) * sizeof(double);
+  size_t off = 0;
+  while (!s->arena.alloc(bytes, &off)) {
+    if (s->finishing.empty()) return fail(EB_ERR_OUT_OF_MEMORY, "request result larger than the host arena");
+    // the arena is full: wait for the oldest retirement and take it out
+    if (eb_status st = poll_events(s, true)) return st;
+  }
+  r.arena_off = off;
+  double* dst = reinterpret_cast<double*>(s->arena.base + off);
+  size_t pos = 0;
+  for (size_t b = 0; b < r.bin_count.size(); ++b) {
+    const int64_t c = r.bin_count[b], g0 = r.bins[b] * kBin;
+    const size_t w = static_cast<size_t>(c) * sizeof(double);
+    SV_CUDA(cudaMemcpy2DAsync(dst + pos, w, s->state[s->cur] + g0, static_cast<size_t>(S) * sizeof(double), w,
+                              eb::kStateFields, cudaMemcpyDeviceToHost, s->stream));
+    pos += static_cast<size_t>(c) * eb::kStateFields;
+  }
+  SV_CUDA(cudaMemcpyAsync(dst + pos, s->e0 + 5 * r.rod0, 5 * nr * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  SV_CUDA(cudaMemcpyAsync(dst + pos + 5 * nr, s->e1 + 5 * r.rod0, 5 * nr * sizeof(double), cudaMemcpyDeviceToHost,
+                          s->stream));
+  if (!r.event) SV_CUDA(cudaEventCreateWithFlags(&r.event, cudaEventDisableTiming));
+  SV_CUDA(cudaEventRecord(r.event, s->stream));
+  // bins and rod ids go back at once: the copies above run before any later
+  // use of them on this stream
+  for (int64_t b : r.bins) s->free_bins.push_back(b);
+  s->rod_ids.release(r.rod0, nr);
+  r.state = kFinishing;
+  s->finishing.push_back(&r);
+  return EB_OK;
+}
+
+// Take a landed retirement out of the arena: energies, drift check, result.
+void land(eb_server* s, Request& r) {
+  const int64_t nr = static_cast<int64_t>(r.rods.size());
+  size_t slots = 0;
+  for (int32_t c : r.bin_count) slots += static_cast<size_t>(c);
+  const double* src = reinterpret_cast<const double*>(s->arena.base + r.arena_off);
+  const double* e0 = src + slots * eb::kStateFields;
+  const double* e1 = e0 + 5 * nr;
+  double E0 = 0.0, E1 = 0.0, scale = 0.0;
+  bool finite = true;
+  for (int64_t k = 0; k < nr; ++k)
+    for (int c = 0; c < 5; ++c) {
+      E0 += e0[5 * k + c];
+      E1 += e1[5 * k + c];
+      scale += std::fabs(e0[5 * k + c]);
+      finite = finite && std::isfinite(e1[5 * k + c]);
+    }
+  r.e0 = E0;
+  r.e1 = E1;
+  r.escale = scale;
+  // result per rod in the local slot layout
+  r.result.clear();
+  r.result_off.assign(r.rods.size(), 0);
+  std::vector<size_t> bin_pos(r.bin_count.size(), 0);
+  size_t pos = 0;
+  for (size_t b = 0; b < r.bin_count.size(); ++b) {
+    bin_pos[b] = pos;
+    pos += static_cast<size_t>(r.bin_count[b]) * eb::kStateFields;
+  }
+  for (size_t k = 0; k < r.rods.size(); ++k) {
+    const int64_t W = r.rods[k].n_elements + 1, b = r.rod_bin[k], o = r.rod_off[k], c = r.bin_count[b];
+    r.result_off[k] = static_cast<int64_t>(r.result.size());
+    for (int f = 0; f < eb::kStateFields; ++f) {
+      const double* row = src + bin_pos[b] + static_cast<size_t>(f * c + o);
+      r.result.insert(r.result.end(), row, row + W);
+    }
+  }
+  s->arena.free_oldest();
+  const bool drift_ok = finite && (E1 - E0) <= s->cfg.energy_tolerance * (scale > 0.0 ? scale : 1.0) &&
+                       !(s->cfg.flags & EB_SERVER_FORCE_FALLBACK);
+  if (!drift_ok && r.precision == EB_PRECISION_MIXED) {
+    // rerun from the initial conditions in FP64
+    r.precision = EB_PRECISION_FP64;
+    r.fell_back = true;
+    ++s->n_fallbacks;
+    r.state = kQueued;
+    r.result.clear();
+    s->queue.push_front(&r);
+    return;
+  }
+  r.latency_s = std::chrono::duration<double>(Clock::now() - r.t_submit).count();
+  r.state = kDone;
+  ++s->n_completed;
+  eb_completion c{};
+  c.request_id = r.id;
+  c.precision = r.precision;
+  c.fell_back = r.fell_back ? 1 : 0;
+  c.latency_s = r.latency_s;
+  c.energy_initial = E0;
+  c.energy_final = E1;
+  c.elements = r.elements;
+  c.steps = r.n_steps;
+  s->completed.push_back(c);
+}
+
+eb_status poll_events(eb_server* s, bool block_oldest) {
+  while (!s->finishing.empty()) {
+    Request* r = s->finishing.front();
+    cudaError_t q = block_oldest ? cudaEventSynchronize(r->event) : cudaEventQuery(r->event);
+    block_oldest = false;
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return fail(EB_ERR_CUDA, std::string("retirement event: ") + cudaGetErrorString(q));
+    s->finishing.pop_front();
+    land(s, *r);
+  }
+  return EB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** out) {
+  if (!out) return fail(EB_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = nullptr;
+  eb_server_config cfg{};
+  if (config) cfg = *config;
+  if (cfg.precision != EB_PRECISION_MIXED && cfg.precision != EB_PRECISION_FP64)
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (cfg.flags & ~static_cast<uint32_t>(EB_SERVER_FORCE_FALLBACK)) return fail(EB_ERR_INVALID_ARGUMENT, "unknown flag");
+  if (cfg.steps_per_launch == 0) cfg.steps_per_launch = 128;
+  if (cfg.steps_per_launch < 1 || cfg.steps_per_launch > 4096)
+    return fail(EB_ERR_INVALID_ARGUMENT, "steps_per_launch must be in [1, 4096]");
+  if (cfg.hbm_budget_bytes == 0.0) cfg.hbm_budget_bytes = 40e9;
+  if (!(cfg.hbm_budget_bytes > 0.0)) return fail(EB_ERR_INVALID_ARGUMENT, "HBM budget must be positive");
+  if (cfg.energy_tolerance == 0.0) cfg.energy_tolerance = 1e-3;
+  if (!(cfg.energy_tolerance > 0.0)) return fail(EB_ERR_INVALID_ARGUMENT, "energy tolerance must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg.device < 0 || cfg.device >= ndev)
+    return fail(EB_ERR_CUDA, "no such CUDA device");
+  // bytes per bin: two state copies, parameters, metadata, rod table,
+  // energies, rod lists, CTA tables
+  const double per_bin = static_cast<double>(kBin) * (2 * eb::kStateFields + eb::kParamFields) * sizeof(double) +
+                         kBin * sizeof(uint32_t) +
+                         kRodsPerBin * (sizeof(eb::RodInfo) + 10 * sizeof(double) + sizeof(int64_t) + sizeof(int32_t)) +
+                         4 * sizeof(eb::ServeCta);
+  const int64_t n_bins = static_cast<int64_t>(cfg.hbm_budget_bytes / per_bin);
+  if (n_bins < 1) return fail(EB_ERR_INVALID_ARGUMENT, "HBM budget holds no bin");
+  if (n_bins * kRodsPerBin >= (int64_t(1) << (32 - eb::kRodShift)))
+    return fail(EB_ERR_UNSUPPORTED, "HBM budget too large for the rod id field");
+  auto s = std::make_unique<eb_server>();
+  s->cfg = cfg;
+  s->n_bins = n_bins;
+  s->n_slots = n_bins * kBin;
+  s->stride = (s->n_slots + 31) / 32 * 32;
+  s->rod_cap = n_bins * kRodsPerBin;
+  cudaError_t e = cudaSetDevice(cfg.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  auto alloc = [&](auto** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s->stream);
+  };
+  const size_t S = static_cast<size_t>(s->stride);
+  alloc(&s->state[0], S * eb::kStateFields * sizeof(double));
+  alloc(&s->state[1], S * eb::kStateFields * sizeof(double));
+  alloc(&s->par, S * eb::kParamFields * sizeof(double));
+  alloc(&s->meta, S * sizeof(uint32_t));
+  alloc(&s->rods, static_cast<size_t>(s->rod_cap) * sizeof(eb::RodInfo));
+  alloc(&s->rod_start, static_cast<size_t>(s->rod_cap) * sizeof(int64_t));
+  alloc(&s->rod_n, static_cast<size_t>(s->rod_cap) * sizeof(int32_t));
+  alloc(&s->e0, static_cast<size_t>(s->rod_cap) * 5 * sizeof(double));
+  alloc(&s->e1, static_cast<size_t>(s->rod_cap) * 5 * sizeof(double));
+  alloc(&s->status, sizeof(uint32_t));
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      alloc(&s->d_cta[a][b], static_cast<size_t>(n_bins) * sizeof(eb::ServeCta));
+      if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void**>(&s->h_cta[a][b]),
+                          static_cast<size_t>(n_bins) * sizeof(eb::ServeCta), cudaHostAllocDefault);
+    }
+  if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&s->arena.base), kArenaBytes, cudaHostAllocDefault);
+  for (auto& ev : s->tick_event)
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("server allocation: ") + cudaGetErrorString(e);
+    server_free(s.get());
+    return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA, msg);
+  }
+  s->arena.cap = kArenaBytes;
+  s->free_bins.reserve(static_cast<size_t>(n_bins));
+  for (int64_t b = n_bins - 1; b >= 0; --b) s->free_bins.push_back(b);
+  s->rod_ids.init(s->rod_cap);
+  *out = s.release();
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_destroy(eb_server* s) {
+  if (!s) return EB_OK;
+  server_free(s);
+  delete s;
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_submit(eb_server* s, const eb_request* req, int64_t* request_id) {
+  if (!s || !req || !request_id) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (req->n_rods < 1 || !req->rods) return fail(EB_ERR_INVALID_ARGUMENT, "a request needs at least one rod");
+  if (!(req->dt > 0.0) || !std::isfinite(req->dt)) return fail(EB_ERR_INVALID_ARGUMENT, "dt must be positive");
+  if (req->n_steps < 1) return fail(EB_ERR_INVALID_ARGUMENT, "a request needs at least one step");
+  if (req->options & ~static_cast<uint32_t>(EB_REQUEST_CLAMP | EB_REQUEST_DAMPER | EB_REQUEST_GRAVITY))
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown request option");
+  auto r = std::make_unique<Request>();
+  r->rods.assign(req->rods, req->rods + req->n_rods);
+  for (const auto& p : r->rods) {
+    eb::HostRodData check;  // the reference initializer's argument checks
+    if (p.n_elements >= 2 && p.n_elements + 1 <= kBin)
+      if (eb_status st = eb::host_straight_rod(p, check)) return st;
+  }
+  int64_t bins_needed = 0, used = kBin;
+  for (const auto& p : r->rods) {
+    if (p.n_elements < 2) return fail(EB_ERR_INVALID_ARGUMENT, "a rod needs at least 2 elements");
+    if (p.n_elements + 1 > kBin)
+      return fail(EB_ERR_UNSUPPORTED, "served rods hold at most " + std::to_string(kBin - 1) + " elements");
+    r->elements += p.n_elements;
+    if (used + p.n_elements + 1 > kBin) {
+      ++bins_needed;
+      used = 0;
+    }
+    used += p.n_elements + 1;
+  }
+  if (bins_needed > s->n_bins) return fail(EB_ERR_OUT_OF_MEMORY, "request larger than the server's HBM budget");
+  if (req->velocities) {
+    int64_t total = 0;
+    for (const auto& p : r->rods) total += 3 * (p.n_elements + 1);
+    r->velocities.assign(req->velocities, req->velocities + total);
+  }
+  r->dt = req->dt;
+  r->n_steps = req->n_steps;
+  for (int d = 0; d < 3; ++d) r->gravity[d] = req->gravity[d];
+  r->options = req->options;
+  r->nu_t = req->damper_translational;
+  r->nu_r = req->damper_rotational;
+  r->precision = s->cfg.precision;
+  r->id = s->next_id++;
+  r->t_submit = Clock::now();
+  Request* raw = r.get();
+  s->requests[r->id] = std::move(r);
+  s->queue.push_back(raw);
+  *request_id = raw->id;
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_tick(eb_server* s, int64_t* in_flight) {
+  if (!s) return fail(EB_ERR_INVALID_ARGUMENT, "null server");
+  SV_CUDA(cudaSetDevice(s->cfg.device));
+  const int parity = static_cast<int>(s->ticks & 1);
+  // flow control: the tick that used this parity's tables must be done
+  if (s->tick_pending[parity]) {
+    SV_CUDA(cudaEventSynchronize(s->tick_event[parity]));
+    s->tick_pending[parity] = false;
+  }
+  if (eb_status st = poll_events(s, false)) return st;
+  if (eb_status st = admit(s)) return st;
+  const int K = s->cfg.steps_per_launch;
+  int n_cta[2] = {0, 0};
+  bool damped[2] = {false, false};
+  for (Request* r : s->active) {
+    const int p = r->precision == EB_PRECISION_MIXED ? 0 : 1;
+    const int32_t steps = static_cast<int32_t>(std::min<int64_t>(K, r->n_steps - r->steps_done));
+    for (size_t b = 0; b < r->bins.size(); ++b) {
+      eb::ServeCta& c = s->h_cta[parity][p][n_cta[p]++];
+      c.start = r->bins[b] * kBin;
+      c.count = r->bin_count[b];
+      c.steps = steps;
+      c.dt = r->dt;
+      c.half_dt = 0.5 * r->dt;
+      for (int d = 0; d < 3; ++d) c.gravity[d] = r->gravity[d];
+      c.flags = request_flags(*r);
+      c.pad = 0;
+    }
+    damped[p] = damped[p] || r->damped;
+  }
+  if (n_cta[0] + n_cta[1] > 0) {
+    eb::StepArgs a{};
+    a.stride = s->stride;
+    a.n_slots = s->n_slots;
+    a.in = s->state[s->cur];
+    a.out = s->state[s->cur ^ 1];
+    a.par = s->par;
+    a.meta = s->meta;
+    a.rods = s->rods;
+    a.status = s->status;
+    for (int p = 0; p < 2; ++p) {
+      if (!n_cta[p]) continue;
+      SV_CUDA(cudaMemcpyAsync(s->d_cta[parity][p], s->h_cta[parity][p], n_cta[p] * sizeof(eb::ServeCta),
+                              cudaMemcpyHostToDevice, s->stream));
+      if (p == 0)
+        SV_CUDA(eb::launch_rod_block_mixed_serve(a, s->d_cta[parity][p], n_cta[p], K, damped[p], s->stream));
+      else
+        SV_CUDA(eb::launch_rod_block_fp64_serve(a, s->d_cta[parity][p], n_cta[p], K, damped[p], s->stream));
+    }
+    s->cur ^= 1;
+    std::vector<Request*> still;
+    for (Request* r : s->active) {
+      const int64_t steps = std::min<int64_t>(K, r->n_steps - r->steps_done);
+      r->steps_done += steps;
+      s->element_steps += static_cast<double>(steps) * static_cast<double>(r->elements);
+      if (r->steps_done >= r->n_steps) {
+        if (eb_status st = retire(s, *r)) return st;
+      } else {
+        still.push_back(r);
+      }
+    }
+    s->active.swap(still);
+  }
+  SV_CUDA(cudaEventRecord(s->tick_event[parity], s->stream));
+  s->tick_pending[parity] = true;
+  ++s->ticks;
+  if (in_flight)
+    *in_flight = static_cast<int64_t>(s->queue.size() + s->active.size() + s->finishing.size());
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_poll(eb_server* s, eb_completion* out, int32_t capacity, int32_t* count) {
+  if (!s || !count || (capacity > 0 && !out)) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  SV_CUDA(cudaSetDevice(s->cfg.device));
+  if (eb_status st = poll_events(s, false)) return st;
+  int32_t n = 0;
+  while (n < capacity && !s->completed.empty()) {
+    out[n++] = s->completed.front();
+    s->completed.pop_front();
+  }
+  *count = n;
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_result(eb_server* s, int64_t request_id, int64_t rod, int32_t field, double* values,
+                                  int64_t count) {
+  if (!s || !values) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  auto it = s->requests.find(request_id);
+  if (it == s->requests.end()) return fail(EB_ERR_NOT_FOUND, "unknown request");
+  const Request& r = *it->second;
+  if (r.state != kDone) return fail(EB_ERR_INVALID_STATE, "request not completed");
+  if (rod < 0 || rod >= static_cast<int64_t>(r.rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod");
+  int row = 0, ncomp = 0;
+  const int64_t n = r.rods[rod].n_elements, W = n + 1;
+  int64_t per = 0;
+  switch (field) {
+    case EB_POSITION: row = eb::kStX; ncomp = 3; per = W; break;
+    case EB_VELOCITY: row = eb::kStV; ncomp = 3; per = W; break;
+    case EB_DIRECTOR: row = eb::kStQ; ncomp = 9; per = n; break;
+    case EB_ANGULAR_VELOCITY: row = eb::kStW; ncomp = 3; per = n; break;
+    default: return fail(EB_ERR_UNSUPPORTED, "served results hold the state fields only");
+  }
+  if (count != ncomp * per) return fail(EB_ERR_INVALID_ARGUMENT, "value count mismatch");
+  const double* base = r.result.data() + r.result_off[rod];
+  for (int c = 0; c < ncomp; ++c)
+    std::memcpy(values + c * per, base + (row + c) * W, static_cast<size_t>(per) * sizeof(double));
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_release(eb_server* s, int64_t request_id) {
+  if (!s) return fail(EB_ERR_INVALID_ARGUMENT, "null server");
+  auto it = s->requests.find(request_id);
+  if (it == s->requests.end()) return fail(EB_ERR_NOT_FOUND, "unknown request");
+  if (it->second->state != kDone) return fail(EB_ERR_INVALID_STATE, "request not completed");
+  if (it->second->event) cudaEventDestroy(it->second->event);
+  s->requests.erase(it);
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_get_stats(const eb_server* s, eb_server_stats* out) {
+  if (!s || !out) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  out->queued = static_cast<int64_t>(s->queue.size());
+  out->active = static_cast<int64_t>(s->active.size());
+  out->finishing = static_cast<int64_t>(s->finishing.size());
+  out->completed = s->n_completed;
+  out->fallbacks = s->n_fallbacks;
+  out->bins_total = s->n_bins;
+  out->bins_used = s->n_bins - static_cast<int64_t>(s->free_bins.size());
+  out->ticks = s->ticks;
+  out->element_steps = s->element_steps;
+  return EB_OK;
+}
+
+}  // extern "C"

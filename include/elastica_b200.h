@@ -297,6 +297,80 @@ EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* 
 /* Number of kernel launches this simulator has issued (diagnostic). */
 EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);
 
+/* --- serving: continuous batching of rod-assembly simulations.  No
+ * counterpart in the reference (its simulator runs one case study at a time);
+ * this is the serving form of the same step.  Requests arrive at any time,
+ * are admitted into a device pool of 520-slot bins sized from an HBM budget
+ * as bins free up, and every tick advances all admitted requests with one
+ * launch of the resident step kernel per precision (steps_per_launch steps
+ * each, counted from the request's own admission, so a result does not depend
+ * on the other requests).  A finished request's state and energies are copied
+ * to host memory on the server's stream and its bins are reused at once;
+ * eb_server_poll reports completions without blocking.  Mixed-precision
+ * requests whose mechanical energy (kinetic + elastic + gravitational) grows
+ * by more than energy_tolerance times the sum of its initial magnitudes, or
+ * turns non-finite, are rerun in FP64 from their initial conditions.  Rods of
+ * a request hold at most 519 elements (one bin). */
+typedef struct eb_server_config {
+  int32_t device;
+  int32_t precision;          /* EB_PRECISION_MIXED (with FP64 fallback) or EB_PRECISION_FP64 */
+  int32_t steps_per_launch;   /* 0: 128 */
+  uint32_t flags;             /* EB_SERVER_* */
+  double hbm_budget_bytes;    /* device pool; 0: 40e9 */
+  double energy_tolerance;    /* 0: 1e-3 */
+} eb_server_config;
+
+/* every mixed-precision result is treated as failing the energy check (for
+ * exercising the FP64 fallback) */
+#define EB_SERVER_FORCE_FALLBACK 0x1u
+
+#define EB_REQUEST_CLAMP 0x1u   /* clamp node 0 / element 0 of every rod */
+#define EB_REQUEST_DAMPER 0x2u  /* analytical linear damper on every rod */
+#define EB_REQUEST_GRAVITY 0x4u /* uniform gravity */
+
+typedef struct eb_request {
+  const eb_straight_rod* rods;
+  int64_t n_rods;
+  const double* velocities;   /* NULL, or per rod 3 x (n + 1) node velocities, concatenated */
+  double dt;
+  int64_t n_steps;
+  double gravity[3];
+  uint32_t options;           /* EB_REQUEST_* */
+  uint32_t reserved;
+  double damper_translational;
+  double damper_rotational;
+} eb_request;
+
+typedef struct eb_completion {
+  int64_t request_id;
+  int32_t precision;          /* precision of the delivered result */
+  int32_t fell_back;          /* 1: the mixed run failed the energy check and was rerun in FP64 */
+  double latency_s;           /* submission to observed completion */
+  double energy_initial;
+  double energy_final;
+  int64_t elements;
+  int64_t steps;
+} eb_completion;
+
+typedef struct eb_server_stats {
+  int64_t queued, active, finishing, completed, fallbacks, bins_total, bins_used, ticks;
+  double element_steps;
+} eb_server_stats;
+
+EB_API eb_status eb_server_create(const eb_server_config* config, struct eb_server** out);
+EB_API eb_status eb_server_destroy(struct eb_server* server);
+EB_API eb_status eb_server_submit(struct eb_server* server, const eb_request* request, int64_t* request_id);
+/* admit what fits, launch one tick, enqueue the retirement of the requests it
+ * finishes; *in_flight (optional) = queued + active + finishing requests */
+EB_API eb_status eb_server_tick(struct eb_server* server, int64_t* in_flight);
+EB_API eb_status eb_server_poll(struct eb_server* server, eb_completion* out, int32_t capacity, int32_t* count);
+/* final state of rod `rod` of a completed request: EB_POSITION, EB_VELOCITY,
+ * EB_DIRECTOR or EB_ANGULAR_VELOCITY, in the per-rod layout of eb_get_field */
+EB_API eb_status eb_server_result(struct eb_server* server, int64_t request_id, int64_t rod, int32_t field,
+                                  double* values, int64_t count);
+EB_API eb_status eb_server_release(struct eb_server* server, int64_t request_id);
+EB_API eb_status eb_server_get_stats(const struct eb_server* server, eb_server_stats* out);
+
 /* --- candidate pairs of caller-provided boxes, allocating nothing.  No
  * counterpart in the reference: it is the collision system's broad phase
  * (the search behind eb_contact_pairs) for callers that cannot allocate device
