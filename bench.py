@@ -313,6 +313,80 @@ def contact_comparison(W, eb, torch, args, rank, local, world, barrier, pg):
     return out
 
 
+def _serve_request(eb, W, rng):
+    """One request of the serving stream: 1-256 rods (log-uniform), n ~
+    U{32..519}, horizon ~ U{1e3..1e5} steps, per-rod parameters as in the
+    uneven batch (clamp, damper 0.1, gravity, node velocities N(0, 1e-3^2))."""
+    k = int(min(256, max(1, round(float(np.exp(rng.uniform(0.0, np.log(256.0))))))))
+    rods, n, L, E, d = W._random_rods(rng, k, 32, 519)
+    vel = [rng.normal(0.0, 1e-3, size=(3, int(m) + 1)) for m in n]
+    dt = 0.1 * float(np.min((L / n) / np.sqrt(E / 1000.0)))
+    steps = int(rng.integers(1000, 100001))
+    return rods, vel, dt, steps, int(n.sum())
+
+
+def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
+    """Poisson arrivals at `rate` requests/s for `seconds`, then up to
+    `drain_s` more seconds; latency = completion seen - scheduled arrival."""
+    from elasticapp_b200.server import Server
+
+    srv = Server(precision="mixed", hbm_budget_bytes=budget)
+    arr_rng = np.random.Generator(np.random.PCG64(seed))
+    arrivals, t = [], 0.0
+    while True:
+        t += float(arr_rng.exponential(1.0 / rate))
+        if t >= seconds:
+            break
+        arrivals.append(t)
+    arrival_of, lat, work = {}, [], 0.0
+    nxt = 0
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < len(arrivals) and arrivals[nxt] <= now:
+            rng = np.random.Generator(np.random.PCG64(seed * 1000003 + nxt))
+            rods, vel, dt, steps, elems = _serve_request(eb, W, rng)
+            rid = srv.submit(rods, dt, steps, gravity=(0.0, 0.0, -9.81), clamp=True, damper=(0.1, 0.1),
+                             velocities=vel)
+            arrival_of[rid] = arrivals[nxt]
+            work += float(elems) * steps
+            nxt += 1
+        left = srv.tick()
+        done = srv.poll()
+        if done:
+            seen = time.perf_counter() - t0
+            for c in done:
+                lat.append(seen - arrival_of.pop(c["request_id"]))
+                srv.release(c["request_id"])
+        if (nxt == len(arrivals) and left == 0) or now > seconds + drain_s:
+            break
+    elapsed = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat) if lat else np.array([np.nan])
+    return {"rate_req_s": rate, "arrival_window_s": seconds, "submitted": len(arrivals),
+            "completed": int(st["completed"]), "in_flight_at_end": len(arrivals) - int(st["completed"]),
+            "fallbacks": int(st["fallbacks"]), "p50_latency_s": float(np.nanpercentile(lat, 50)),
+            "p99_latency_s": float(np.nanpercentile(lat, 99)), "elapsed_s": elapsed,
+            "value": st["element_steps"] / elapsed, "unit": UNIT,
+            "offered_element_steps_per_s": work / max(seconds, 1e-9), "ticks": int(st["ticks"]),
+            "bins_total": int(st["bins_total"])}
+
+
+def serving_section(eb, W, args, capacity_hint):
+    """The serving stream at the stated load (200 requests/s) for a bounded
+    window, and at a sustainable load (half the measured capacity)."""
+    out = {"workload": "serve_stream", "hbm_budget_bytes": args.serve_budget, "precision": "mixed (FP64 fallback)",
+           "steps_per_launch": 128,
+           "request": "1-256 rods log-uniform, n ~ U{32..519} (one 520-slot bin per CTA), horizon U{1e3..1e5}, "
+                      "clamp + damper 0.1 + gravity, velocities N(0, 1e-3^2); dt = 0.1 min(l/c) per request"}
+    mean_work = 46.0 * 275.5 * 50500.0  # mean rods x mean n x mean horizon
+    out["stated_load"] = serve_stream(eb, W, 200.0, args.serve_seconds, args.serve_drain, 1005, args.serve_budget)
+    rate = args.serve_rate if args.serve_rate > 0 else max(1.0, 0.5 * capacity_hint / mean_work)
+    out["sustained_load"] = serve_stream(eb, W, rate, args.serve_seconds, args.serve_drain, 1006, args.serve_budget)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,6 +406,12 @@ def main(argv=None) -> int:
     ap.add_argument("--contact-rods", type=int, default=8192, help="rods of the contact batch")
     ap.add_argument("--contact-steps", type=int, default=10,
                     help="timed steps of the contact batch (each from its initial state); 0 skips it")
+    ap.add_argument("--serve-seconds", type=float, default=15.0,
+                    help="arrival window of each serving stream; 0 skips serving")
+    ap.add_argument("--serve-drain", type=float, default=30.0, help="extra seconds to finish in-flight requests")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="sustained-load arrival rate (0: half the measured mixed capacity)")
+    ap.add_argument("--serve-budget", type=float, default=40e9, help="HBM budget of the serving pool (bytes)")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-rounding", action="store_true",
@@ -480,6 +560,11 @@ def main(argv=None) -> int:
     if args.mixed_steps > 0:
         mixed = mixed_comparison(W, eb, torch, args, rank, local, barrier, pg)
 
+    serving = None
+    if args.serve_seconds > 0 and rank == 0 and world == 1:
+        cap = mixed["value"] if mixed else 2.0e10
+        serving = serving_section(eb, W, args, cap)
+
     contact = None
     if args.contact_steps > 0:
         contact = contact_comparison(W, eb, torch, args, rank, local, world, barrier, pg)
@@ -515,6 +600,7 @@ def main(argv=None) -> int:
             "batched": batched,
             "mixed": mixed,
             "contact": contact,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if sim is not None:
