@@ -23,6 +23,9 @@ EB_FLAG_RECORD_DIAGNOSTICS = 0x1
 EB_FLAG_REFERENCE_ROUNDING = 0x2
 EB_FLAG_STEP_STREAMING = 0x4
 EB_FLAG_STEP_RESIDENT = 0x8
+EB_FLAG_CUDA_GRAPH = 0x10
+EB_STEPPER_POSITION_VERLET = 0
+EB_STEPPER_PEFRL = 1
 EB_ROD_DAMPED = 0
 EB_ROD_UNDAMPED = 1
 EB_LAYOUT_PER_ROD = 0
@@ -60,7 +63,7 @@ CONTACT_FIELDS = {"ContactForce", "ContactTorque"}
 class EbConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("flags", ctypes.c_uint32), ("step_window", ctypes.c_int32),
-                ("resident_config", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("resident_config", ctypes.c_int32), ("stepper", ctypes.c_int32)]
 
 
 class EbStraightRod(ctypes.Structure):

@@ -168,6 +168,9 @@ struct eb_sim {
   std::vector<int64_t*> d_cta_start;  // per block configuration (or null)
   std::vector<int> n_ctas;
   float plan_ms[16] = {0};
+  // captured streaming steps: per starting buffer parity, for graph_dt
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0.0, 0.0};
   // collision system
   std::vector<eb_contact_material> materials;
   std::vector<eb::ContactPlane> planes;
@@ -333,6 +336,11 @@ void host_free(eb_sim* s) {
   for (auto* p : s->d_cta_start)
     if (p) cudaFree(p);
   s->d_cta_start.clear();
+  for (auto& g : s->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   ContactDevice& c = s->contact;
   void* cptrs[] = {c.cap, c.cap_material, c.extent, c.cell, c.bucket, c.bucket_count, c.bucket_start,
                    c.sorted_id, c.sorted_cell, c.sorted_box, c.pair_count, c.pair_offset, c.partners,
@@ -518,6 +526,13 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
     return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
   if (cfg.precision == EB_PRECISION_MIXED && (cfg.flags & (EB_FLAG_REFERENCE_ROUNDING | EB_FLAG_STEP_STREAMING)))
     return fail(EB_ERR_INVALID_ARGUMENT, "mixed precision runs on the resident kernels only");
+  if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.stepper != EB_STEPPER_PEFRL)
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown time stepper");
+  if (cfg.stepper == EB_STEPPER_PEFRL && cfg.precision == EB_PRECISION_MIXED)
+    return fail(EB_ERR_UNSUPPORTED, "PEFRL runs on the FP64 streaming kernel only");
+  if (cfg.flags & ~static_cast<uint32_t>(EB_FLAG_RECORD_DIAGNOSTICS | EB_FLAG_REFERENCE_ROUNDING |
+                                          EB_FLAG_STEP_STREAMING | EB_FLAG_STEP_RESIDENT | EB_FLAG_CUDA_GRAPH))
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown flag");
   int ndev = 0;
   EB_CUDA(cudaGetDeviceCount(&ndev));
   if (cfg.device < 0 || cfg.device >= ndev) return fail(EB_ERR_INVALID_ARGUMENT, "no such CUDA device");
@@ -920,6 +935,9 @@ eb::StepArgs step_args(eb_sim* s, double dt) {
   a.rods = s->d_rods;
   a.dt = dt;
   a.half_dt = 0.5 * dt;
+  a.drift_pre = 0.5 * dt;
+  a.kick = dt;
+  a.drift_post = 0.5 * dt;
   for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
   a.sim_flags = s->sim_flags;
   a.status = s->d_status;
@@ -977,13 +995,101 @@ eb_status build_block_worklists(eb_sim* s) {
   return EB_OK;
 }
 
+// Substeps of one step as (drift before, kick, drift after) in units of dt:
+// PositionVerlet (PositionVerlet.hpp:49-88) fuses its two half drifts around
+// one kick; PEFRL (Omelyan, Mryglod and Folk 2002) is four kicks with the
+// drifts xi, chi, 1 - 2 (chi + xi), chi, xi between them.
+struct Substep {
+  double pre, kick, post;
+};
+constexpr double kPefrlXi = 0.1786178958448091;
+constexpr double kPefrlLambda = -0.2123418310626054;
+constexpr double kPefrlChi = -0.06626458266981849;
+const Substep kVerlet[1] = {{0.5, 1.0, 0.5}};
+const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0},
+                           {kPefrlChi, kPefrlLambda, 0.0},
+                           {1.0 - 2.0 * (kPefrlChi + kPefrlXi), kPefrlLambda, 0.0},
+                           {kPefrlChi, 0.5 * (1.0 - 2.0 * kPefrlLambda), kPefrlXi}};
+
+int substeps(const eb_sim* s, const Substep** table) {
+  if (s->cfg.stepper == EB_STEPPER_PEFRL) {
+    *table = kPefrl;
+    return 4;
+  }
+  *table = kVerlet;
+  return 1;
+}
+
+// One step on the streaming kernel: one launch per substep.
+cudaError_t stream_one_step(eb_sim* s, eb::StepArgs& a, double dt, bool rec) {
+  const Substep* sub;
+  const int ns = substeps(s, &sub);
+  for (int k = 0; k < ns; ++k) {
+    if (ns == 1) {
+      a.drift_pre = 0.5 * dt;  // PositionVerlet: bit-identical to half_dt
+      a.kick = dt;
+      a.drift_post = 0.5 * dt;
+    } else {
+      a.drift_pre = sub[k].pre * dt;
+      a.kick = sub[k].kick * dt;
+      a.drift_post = sub[k].post * dt;
+    }
+    a.in = s->d_state[s->cur];
+    a.out = s->d_state[s->cur ^ 1];
+    cudaError_t e = launch_streaming(s, a, rec && k == ns - 1);
+    if (e != cudaSuccess) return e;
+    s->cur ^= 1;
+    ++s->launches;
+  }
+  return cudaSuccess;
+}
+
+constexpr int64_t kGraphSteps = 32;  // steps per captured graph (an even launch count)
+
+// Replay (capturing first if needed) the graph of kGraphSteps streaming steps
+// that starts from the current buffer parity.
+eb_status graph_steps(eb_sim* s, double dt) {
+  const int p = s->cur;
+  if (!s->graph[p] || s->graph_dt[p] != dt) {
+    if (s->graph[p]) {
+      cudaGraphExecDestroy(s->graph[p]);
+      s->graph[p] = nullptr;
+    }
+    eb::StepArgs a = step_args(s, dt);
+    const int64_t launches0 = s->launches;
+    EB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int64_t k = 0; k < kGraphSteps && e == cudaSuccess; ++k) e = stream_one_step(s, a, dt, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    // capture only recorded the launches: restore the parity and the count
+    s->cur = p;
+    s->launches = launches0;
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(EB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    const cudaError_t e3 = cudaGraphInstantiate(&s->graph[p], g, 0);
+    cudaGraphDestroy(g);
+    EB_CUDA(e3);
+    s->graph_dt[p] = dt;
+  }
+  EB_CUDA(cudaGraphLaunch(s->graph[p], s->stream));
+  const Substep* sub;
+  const int64_t per = substeps(s, &sub);
+  s->launches += per * kGraphSteps;
+  if ((per * kGraphSteps) & 1) s->cur ^= 1;
+  return EB_OK;
+}
+
 // Choose between the streaming kernel and the resident configurations by
 // timing each for kProbeSteps steps from the current state into the spare
 // buffer (the current state is left untouched).
 eb_status plan_steps(eb_sim* s, double dt) {
-  // contact needs a global exchange every step: the streaming kernel
-  const bool force_stream =
-      (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 || s->contact.on;
+  // contact needs a global exchange every step, PEFRL four force evaluations
+  // a step: the streaming kernel
+  const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
+                            s->contact.on || s->cfg.stepper == EB_STEPPER_PEFRL;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -1101,14 +1207,25 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
     const int c0 = s->cur;
     EB_CUDA(cudaMemcpyAsync(c.backup, s->d_state[c0], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
     eb::ContactArgs ca = contact_args(s, dt);
+    const Substep* sub;
+    const int ns = substeps(s, &sub);
     for (int64_t i = 0; i < k; ++i) {
-      ca.state = s->d_state[s->cur];
-      EB_CUDA(eb::launch_contact(ca, s->stream, &s->launches));
-      a.in = s->d_state[s->cur];
-      a.out = s->d_state[s->cur ^ 1];
-      EB_CUDA(launch_streaming(s, a, diag && done + i == n_steps - 1));
-      s->cur ^= 1;
-      ++s->launches;
+      for (int j = 0; j < ns; ++j) {
+        // one contact evaluation per force evaluation, at its drifted state
+        if (ns > 1) {
+          a.drift_pre = sub[j].pre * dt;
+          a.kick = sub[j].kick * dt;
+          a.drift_post = sub[j].post * dt;
+          ca.half_dt = a.drift_pre;
+        }
+        ca.state = s->d_state[s->cur];
+        EB_CUDA(eb::launch_contact(ca, s->stream, &s->launches));
+        a.in = s->d_state[s->cur];
+        a.out = s->d_state[s->cur ^ 1];
+        EB_CUDA(launch_streaming(s, a, diag && done + i == n_steps - 1 && j == ns - 1));
+        s->cur ^= 1;
+        ++s->launches;
+      }
     }
     uint32_t st = 0;
     unsigned long long req = 0;
@@ -1185,13 +1302,14 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
       done += k;
     }
   }
-  for (; done < n_steps; ++done) {
-    a.in = s->d_state[s->cur];
-    a.out = s->d_state[s->cur ^ 1];
-    EB_CUDA(launch_streaming(s, a, diag && done == n_steps - 1));
-    s->cur ^= 1;
-    ++s->launches;
+  if (s->cfg.flags & EB_FLAG_CUDA_GRAPH) {
+    // whole graphs of kGraphSteps steps; a recorded last step stays outside
+    while (n_steps - done - (diag ? 1 : 0) >= kGraphSteps) {
+      if (eb_status st = graph_steps(s, dt)) return st;
+      done += kGraphSteps;
+    }
   }
+  for (; done < n_steps; ++done) EB_CUDA(stream_one_step(s, a, dt, diag && done == n_steps - 1));
   if (time) {
     for (int64_t k = 0; k < n_steps; ++k) {
       // two TimeUpdate substeps of dt/2 (PositionVerlet.hpp:52-58)

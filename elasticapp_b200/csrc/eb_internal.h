@@ -97,6 +97,11 @@ struct StepArgs {
   uint32_t* status;     // device status word (kStatus* bits), never cleared by kernels
   double dt;
   double half_dt;
+  // substep times of one streaming launch: drift before the force
+  // evaluation, kick, drift after it (PositionVerlet: dt/2, dt, dt/2)
+  double drift_pre;
+  double kick;
+  double drift_post;
   double gravity[3];
   uint32_t sim_flags;   // kSim* below
   // capsule contact loads of this step (lab frame, 3 x stride each, per

@@ -170,7 +170,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     return;
   }
 
-  const double hdt = a.half_dt;
+  const double hdt = a.drift_pre;
 
   // ---- phase 1: first kinematic half step and clamp value constraint,
   // in place in shared memory
@@ -315,7 +315,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
 
   // ---- dynamic step and rate constraints
-  const double dt = a.dt;
+  const double dt = a.kick;
   v = {v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z};
   if (meta & kElem) w = {w.x + dt * alpha.x, w.y + dt * alpha.y, w.z + dt * alpha.z};
   if ((meta & kFirst) && (rflags & kRodClamp)) {
@@ -323,6 +323,8 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     w = D3{0.0, 0.0, 0.0};
   }
   if (rflags & kRodDamper) {
+    // exp(-nu_t dt) for a kick of dt; a fractional kick (PEFRL) scales the exponent
+    if (a.kick != a.dt) damper_t = exp(log(damper_t) * (a.kick / a.dt));
     v = {v.x * damper_t, v.y * damper_t, v.z * damper_t};
     if (meta & kElem) {
       // AnalyticalLinearDamper.hpp:40-75: w_k *= exp(y_k)^e with
@@ -345,12 +347,13 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
 
   // ---- second kinematic half step and store
-  x = {x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z};
+  const double hdt2 = a.drift_post;
+  x = {x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z};
   double* __restrict__ out = a.out;
   st3(out + kStX * S, S, g, x);
   st3(out + kStV * S, S, g, v);
   if (meta & kElem) {
-    so3(q, hdt * w.x, hdt * w.y, hdt * w.z);
+    so3(q, hdt2 * w.x, hdt2 * w.y, hdt2 * w.z);
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[(kStQ + k) * S + g] = q[k];
     st3(out + kStW * S, S, g, w);

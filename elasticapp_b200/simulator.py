@@ -144,6 +144,13 @@ class PositionVerlet:
     """Time/SymplecticSteppers/Algorithms/PositionVerlet.hpp:49-88."""
 
 
+@dataclass
+class PEFRL:
+    """Position-extended Forest-Ruth-like stepper (Omelyan, Mryglod, Folk
+    2002), declared in Time/SymplecticSteppers/Algorithms/Types.hpp:31.  A
+    simulator steps with the stepper it was created with."""
+
+
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -209,7 +216,7 @@ class Simulator:
 
     def __init__(self, device: int = 0, precision: str = "fp64", record_diagnostics: bool = False,
                  reference_rounding: bool = False, window: int = 0, step_mode: str = "auto",
-                 resident_config: int = 0):
+                 resident_config: int = 0, stepper=None, cuda_graph: bool = False):
         cfg = L.EbConfig()
         cfg.device = int(device)
         cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
@@ -218,6 +225,10 @@ class Simulator:
             "auto": 0, "streaming": L.EB_FLAG_STEP_STREAMING, "resident": L.EB_FLAG_STEP_RESIDENT}[step_mode]
         cfg.step_window = int(window)
         cfg.resident_config = int(resident_config)
+        if cuda_graph:
+            cfg.flags |= L.EB_FLAG_CUDA_GRAPH
+        self.stepper = PEFRL if isinstance(stepper, PEFRL) or stepper is PEFRL else PositionVerlet
+        cfg.stepper = L.EB_STEPPER_PEFRL if self.stepper is PEFRL else L.EB_STEPPER_POSITION_VERLET
         h = ctypes.c_void_p()
         L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h
@@ -320,8 +331,8 @@ class Simulator:
 
     # -- time stepping -------------------------------------------------------
     def step(self, stepper, time: float, dt: float, n_steps: int = 1) -> float:
-        if not isinstance(stepper, PositionVerlet):
-            raise TypeError("only PositionVerlet is provided")
+        if not isinstance(stepper, self.stepper):
+            raise TypeError(f"this simulator was created for {self.stepper.__name__}")
         t = ctypes.c_double(time)
         L.call("eb_step", self._h, ctypes.byref(t), float(dt), int(n_steps))
         return t.value

@@ -66,11 +66,11 @@ class Workload:
 
     def build(self, device: int = 0, record_diagnostics: bool = False, precision: str = "fp64",
               reference_rounding: bool = False, window: int = 0, step_mode: str = "auto",
-              resident_config: int = 0) -> Simulator:
+              resident_config: int = 0, stepper=None, cuda_graph: bool = False) -> Simulator:
         """Create the simulator through the reference-style plugin surface."""
         sim = Simulator(device=device, precision=precision, record_diagnostics=record_diagnostics,
                         reference_rounding=reference_rounding, window=window, step_mode=step_mode,
-                        resident_config=resident_config)
+                        resident_config=resident_config, stepper=stepper, cuda_graph=cuda_graph)
         refs = sim.emplace_back_many(self.model, self.rods)
         if self.gravity is not None:
             sim.add_environment(GravityField(self.gravity))

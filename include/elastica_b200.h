@@ -76,6 +76,11 @@ typedef enum eb_precision {
                                            128 steps per launch) when the rods
                                            fit; by default the first eb_step
                                            times both and keeps the faster */
+#define EB_FLAG_CUDA_GRAPH 0x10u       /* streaming steps (without contact)
+                                           replayed from a captured CUDA graph
+                                           of 32 steps: one graph launch
+                                           instead of 32 (128 with PEFRL)
+                                           kernel launches */
 
 typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
@@ -83,8 +88,19 @@ typedef struct eb_config {
   uint32_t flags;          /* EB_FLAG_* */
   int32_t step_window;     /* slots per CTA of the streaming kernel: 0 (default, 128), 128 or 256 */
   int32_t resident_config; /* 0: chosen by timing; c > 0: resident configuration c - 1 */
-  int32_t reserved;
+  int32_t stepper;         /* eb_stepper (0: PositionVerlet) */
 } eb_config;
+
+/* Time steppers (elastica/Time/SymplecticSteppers/Algorithms/Types.hpp:31).
+ * PositionVerlet follows PositionVerlet.hpp:49-88.  PEFRL is declared but not
+ * implemented in the reference; here it is the position-extended
+ * Forest-Ruth-like integrator of Omelyan, Mryglod and Folk (Comput. Phys.
+ * Commun. 146, 188-202, 2002): four force evaluations per step with
+ * xi = 0.1786178958448091, lambda = -0.2123418310626054,
+ * chi = -0.06626458266981849, value constraints after every drift and rate
+ * constraints after every kick (the damper's factors for the kick's share of
+ * dt).  PEFRL runs on the FP64 streaming kernel. */
+typedef enum eb_stepper { EB_STEPPER_POSITION_VERLET = 0, EB_STEPPER_PEFRL = 1 } eb_stepper;
 
 /* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and
  * Aliases/CosseratRodWithoutDamping.hpp). */

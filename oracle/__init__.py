@@ -80,6 +80,7 @@ def lib():
         _lib = ctypes.CDLL(LIB_PATH)
         _lib.orc_step.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64, ctypes.c_int]
         _lib.orc_force_eval.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_int]
+        _lib.orc_step_pefrl.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64, ctypes.c_int]
         _lib.orc_energy.argtypes = [ctypes.POINTER(_OrcRods), _P, ctypes.c_int]
         _lib.orc_straight_rod.argtypes = [ctypes.c_int64, _P, _P, _P, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double] + [_P] * 11
@@ -202,9 +203,10 @@ class RodArrays:
                 setattr(s, k, a.ctypes.data_as(_P))
         return s
 
-    def step(self, dt, n_steps=1, n_threads=0):
+    def step(self, dt, n_steps=1, n_threads=0, stepper="position_verlet"):
         s = self._struct()
-        rc = lib().orc_step(ctypes.byref(s), float(dt), int(n_steps), int(n_threads))
+        fn = lib().orc_step_pefrl if stepper == "pefrl" else lib().orc_step
+        rc = fn(ctypes.byref(s), float(dt), int(n_steps), int(n_threads))
         if rc != 0:
             raise RuntimeError("orc_step failed")
 

@@ -80,6 +80,10 @@ typedef struct OrcRods {
  * n_threads <= 0 uses all OpenMP threads. */
 int orc_step(const OrcRods* rods, double dt, int64_t n_steps, int n_threads);
 
+/* n_steps PEFRL steps (declared, not implemented, in the reference;
+ * Omelyan, Mryglod and Folk 2002): four force evaluations per step. */
+int orc_step_pefrl(const OrcRods* rods, double dt, int64_t n_steps, int n_threads);
+
 /* One force evaluation without any time update (the reference's
  * compute_internal_forces + compute_internal_torques + update_acceleration),
  * writing the diagnostics. */

@@ -110,18 +110,18 @@ def max_rel_error_per_rod(got, want, n_elems, place):
 STATE_FIELDS = (("Position", "x", 0), ("Velocity", "v", 0), ("Director", "Q", 1), ("AngularVelocity", "w", 1))
 
 
-def oracle_spread(wl, n_steps, damped=False):
+def oracle_spread(wl, n_steps, damped=False, stepper="position_verlet"):
     """Conditioning envelope of a workload: the largest per-rod normwise
     relative change of each state field after n_steps when every initial
     position, or every initial director entry, of the oracle is moved by one
     ulp.  Returns (reference_run, {field: spread})."""
     base = oracle_from_workload(wl, damped=damped)
-    base.step(wl.dt, n_steps)
+    base.step(wl.dt, n_steps, stepper=stepper)
     spread = {name: 0.0 for name, _, _ in STATE_FIELDS}
     for key in ("x", "Q"):
         p = oracle_from_workload(wl, damped=damped)
         p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
-        p.step(wl.dt, n_steps)
+        p.step(wl.dt, n_steps, stepper=stepper)
         for name, k, place in STATE_FIELDS:
             spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
     return base, spread
