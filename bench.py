@@ -201,7 +201,8 @@ def workload_config(wl, world):
             "n_elements": [int(wl.n_elements.min()), int(wl.n_elements.max())], "dt": wl.dt,
             "seed": wl.seed, "stepper": "PositionVerlet",
             "constraints": "clamp(node 0) + analytical damper 0.1", "gravity": list(wl.gravity or []),
-            "parallelism": f"{world} independent rod shards (weak)" if world > 1 else "single GPU",
+            "parallelism": f"{world} element-balanced shards of one batch of {world} x the per-GPU rods "
+                           "(Karmarkar-Karp partition, weak)" if world > 1 else "single GPU",
             "l2": "no flush: state + parameters exceed the 126 MB L2 many times over"}
 
 
@@ -313,6 +314,55 @@ def contact_comparison(W, eb, torch, args, rank, local, world, barrier, pg):
     return out
 
 
+def cantilever_section(eb, W, torch, args, local):
+    """The single-rod cantilever (1 rod, 100 elements, clamp, gravity,
+    analytical damper 0.1, dt 1e-5, 1e5 steps): timed run on the planner's
+    kernel, then the tip trajectory every 1000 steps against the oracle."""
+    wl = W.cantilever()
+    n_steps, every = args.cantilever_steps, 1000
+    out = {"workload": "cantilever", "rods": 1, "elements": wl.total_elements, "dt": wl.dt, "steps": n_steps}
+    for label, kw in (("auto", {}), ("streaming_graph", {"step_mode": "streaming", "cuda_graph": True})):
+        sim = wl.build(device=local, **kw)
+        t = sim.step(eb.PositionVerlet(), 0.0, wl.dt, 128)  # plan + warm-up
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(eb.PositionVerlet(), t, wl.dt, n_steps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out[label] = {"value": wl.total_elements * n_steps / (ms / 1e3), "unit": UNIT, "ms_total": ms,
+                      "us_per_step": 1e3 * ms / n_steps, "plan": sim.step_plan()["mode"]}
+        sim.close()
+    out["value"] = max(out["auto"]["value"], out["streaming_graph"]["value"])
+    # tip trajectory against the oracle (fresh runs from the initial state)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bridge as ob
+
+    sim = wl.build(device=local)
+    orc = ob.oracle_from_workload(wl)
+    t, errs = 0.0, []
+    t0 = time.perf_counter()
+    cpu_s = 0.0
+    for _ in range(n_steps // every):
+        t = sim.step(eb.PositionVerlet(), t, wl.dt, every)
+        c0 = time.perf_counter()
+        orc.step(wl.dt, every, n_threads=1)
+        cpu_s += time.perf_counter() - c0
+        tip_g = sim.rods[0].get("Position")[:, -1]
+        tip_o = orc.get_rod("x", 0, wl.n_elements[0] + 1)[:, -1]
+        errs.append(float(np.linalg.norm(tip_g - tip_o)) / wl.rods[0].length)
+    sim.close()
+    out["tip_trajectory"] = {"samples": len(errs), "every_steps": every, "max_rel_error": max(errs),
+                             "final_rel_error": errs[-1], "final_tip": [float(v) for v in tip_g],
+                             "definition": "|tip_gpu - tip_oracle| / rod length, sampled every 1000 steps"}
+    out["cpu_baseline"] = {"value": wl.total_elements * n_steps / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+                           "sample": "the whole 1e5-step run (one rod: one core)"}
+    return out
+
+
 def _serve_request(eb, W, rng):
     """One request of the serving stream: 1-256 rods (log-uniform), n ~
     U{32..519}, horizon ~ U{1e3..1e5} steps, per-rod parameters as in the
@@ -406,6 +456,8 @@ def main(argv=None) -> int:
     ap.add_argument("--contact-rods", type=int, default=8192, help="rods of the contact batch")
     ap.add_argument("--contact-steps", type=int, default=10,
                     help="timed steps of the contact batch (each from its initial state); 0 skips it")
+    ap.add_argument("--cantilever-steps", type=int, default=100000,
+                    help="steps of the single-rod cantilever; 0 skips it")
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="arrival window of each serving stream; 0 skips serving")
     ap.add_argument("--serve-drain", type=float, default=30.0, help="extra seconds to finish in-flight requests")
@@ -448,7 +500,14 @@ def main(argv=None) -> int:
 
     import elasticapp_b200 as eb
 
-    wl = wl_fn(rank)
+    if world > 1 and args.workload != "cantilever":
+        # one global batch of world x the per-GPU size, sharded by the
+        # Karmarkar-Karp partition of its rods (element-balanced, weak scaling)
+        from elasticapp_b200 import dist as ebdist
+        per = args.rods if args.rods is not None else 16384
+        wl = ebdist.shard(W.CONFIGS[args.workload](n_rods=per * world, seed=1002), rank, world)
+    else:
+        wl = wl_fn(rank)
     sim = wl.build(device=local, reference_rounding=args.reference_rounding, window=args.window,
                    step_mode="streaming")
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
@@ -560,6 +619,10 @@ def main(argv=None) -> int:
     if args.mixed_steps > 0:
         mixed = mixed_comparison(W, eb, torch, args, rank, local, barrier, pg)
 
+    cantilever = None
+    if args.cantilever_steps > 0 and rank == 0 and world == 1:
+        cantilever = cantilever_section(eb, W, torch, args, local)
+
     serving = None
     if args.serve_seconds > 0 and rank == 0 and world == 1:
         cap = mixed["value"] if mixed else 2.0e10
@@ -601,6 +664,7 @@ def main(argv=None) -> int:
             "mixed": mixed,
             "contact": contact,
             "serving": serving,
+            "cantilever": cantilever,
         }
         print(json.dumps(line), flush=True)
     if sim is not None:

@@ -31,6 +31,7 @@ SOURCES = [
     ("contact.o", "contact.cu", ["--fmad=false"]),
     ("box_pairs_noalloc.o", "box_pairs_noalloc.cu", []),
     ("serve.o", "serve.cu", []),
+    ("partition.o", "partition.cu", []),
 ]
 HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h", "eb_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -313,6 +313,12 @@ EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* 
 /* Number of kernel launches this simulator has issued (diagnostic). */
 EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);
 
+/* --- multi-GPU: k-way partition of rods by element count (the largest
+ * differencing method of elastica/Utilities/KarmarkarKarpPartition.hpp:
+ * 332-422), for sharding one batch across GPUs.  part_of[i] in [0, n_parts)
+ * receives item i's part; deterministic (ties by creation order). */
+EB_API eb_status eb_partition_rods(const int64_t* weights, int64_t n, int32_t n_parts, int32_t* part_of);
+
 /* --- serving: continuous batching of rod-assembly simulations.  No
  * counterpart in the reference (its simulator runs one case study at a time);
  * this is the serving form of the same step.  Requests arrive at any time,
