@@ -15,10 +15,12 @@
 //      just above the largest extent, hashed into a power-of-two table; every
 //      capsule is filed under the cell of its box's lower corner (a counting
 //      sort by bucket).
-//   3. pairs_kernel<false> + scan + pairs_kernel<true>: every capsule tests
-//      the capsules filed in its 27 neighbouring cells, then every plane;
-//      counts first, then each capsule writes its partner list into its own
-//      segment and sorts it.  Two boxes that overlap have lower corners less
+//   3. pairs_kernel<0>: every capsule tests the capsules filed in its 27
+//      neighbouring cells, then every plane, in one pass, writing up to
+//      kFixedPartners partners into its fixed-stride list (sorted) and its
+//      count; pairs_kernel<1> (after a scan of the larger counts) writes the
+//      whole sorted list of a capsule with more partners into the overflow
+//      lists.  Two boxes that overlap have lower corners less
 //      than one cell apart on each axis, so the candidate set equals the
 //      exhaustive search's (Detection/Coarse/ExhaustiveSearch.hpp:322-435,
 //      closed intervals of BoundingBox.hpp:532-540), which the reference's
@@ -211,6 +213,7 @@ __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
   if (!finite) {
     a.bucket[s] = 0xffffffffu;
     a.pair_count[s] = 0;
+    a.ovf_count[s] = 0;
     return;
   }
   const double ih = inverse_cell(a);
@@ -250,31 +253,46 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) 
 
 // ---- stage 3: candidate pairs ----------------------------------------------
 
-template <bool kWrite>
+__device__ __forceinline__ void sort_ids(int32_t* v, int32_t n) {
+  for (int32_t i = 1; i < n; ++i) {
+    const int32_t x = v[i];
+    int32_t j = i - 1;
+    while (j >= 0 && v[j] > x) {
+      v[j + 1] = v[j];
+      --j;
+    }
+    v[j + 1] = x;
+  }
+}
+
+// kPass 0: count and fill the fixed-stride list; kPass 1: overflow lists of
+// the capsules with more than kFixedPartners partners
+template <int kPass>
 __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps_max) {
   // entries filed this evaluation (the capsules with finite boxes)
   const int32_t n_caps = min(a.bucket_start[a.table_mask + 1], n_caps_max);
   const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
   if (e >= n_caps) return;
   const int32_t id = a.sorted_id[e];
+  int32_t* out;
+  if (kPass == 1) {
+    if (a.pair_count[id] <= kFixedPartners) return;
+    const int64_t total = a.pair_offset[a.n_slots];
+    if (total > a.capacity) {
+      atomicOr(a.status, kStatusPairOverflow);
+      atomicMax(a.required, static_cast<unsigned long long>(total));
+      return;
+    }
+    out = a.partners + a.pair_offset[id];  // within [0, capacity)
+  } else {
+    out = a.fixed + static_cast<int64_t>(id) * kFixedPartners;
+  }
   const int32_t cx = a.sorted_cell[3 * e], cy = a.sorted_cell[3 * e + 1], cz = a.sorted_cell[3 * e + 2];
   double lo[3], hi[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     lo[d] = a.sorted_box[6 * e + d];
     hi[d] = a.sorted_box[6 * e + 3 + d];
-  }
-  int32_t* out = nullptr;
-  if (kWrite) {
-    const int64_t total = a.pair_offset[a.n_slots];
-    if (total > a.capacity) {
-      if (e == 0) {
-        atomicOr(a.status, kStatusPairOverflow);
-        atomicMax(a.required, static_cast<unsigned long long>(total));
-      }
-      return;
-    }
-    out = a.partners + a.pair_offset[id];  // within [0, capacity)
   }
   int32_t cnt = 0;
   for (int dz = -1; dz <= 1; ++dz)
@@ -289,28 +307,21 @@ __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, in
           if (other == id) continue;
           const double* bx = a.sorted_box + 6 * k;
           if (!overlaps(lo, hi, bx, bx + 3)) continue;
-          if (kWrite) out[cnt] = other;
+          if (kPass == 1 || cnt < kFixedPartners) out[cnt] = other;
           ++cnt;
         }
       }
   for (int32_t p = 0; p < a.n_planes; ++p) {
     if (!overlaps(lo, hi, a.planes[p].lo, a.planes[p].hi)) continue;
-    if (kWrite) out[cnt] = static_cast<int32_t>(a.n_slots) + p;
+    if (kPass == 1 || cnt < kFixedPartners) out[cnt] = static_cast<int32_t>(a.n_slots) + p;
     ++cnt;
   }
-  if (!kWrite) {
+  if (kPass == 0) {
     a.pair_count[id] = cnt;
+    a.ovf_count[id] = cnt > kFixedPartners ? cnt : 0;
+    if (cnt <= kFixedPartners) sort_ids(out, cnt);  // ascending partner order
   } else {
-    // ascending partner order (insertion sort of this capsule's segment)
-    for (int32_t i = 1; i < cnt; ++i) {
-      const int32_t v = out[i];
-      int32_t j = i - 1;
-      while (j >= 0 && out[j] > v) {
-        out[j + 1] = out[j];
-        --j;
-      }
-      out[j + 1] = v;
-    }
+    sort_ids(out, cnt);
   }
 }
 
@@ -560,13 +571,19 @@ __global__ void __launch_bounds__(kThreads) force_kernel(const ContactArgs a) {
   if (mat < 0) return;
   const int64_t S = a.stride;
   D3 F = {0.0, 0.0, 0.0}, T = {0.0, 0.0, 0.0};
-  const int64_t total = a.pair_offset[a.n_slots];
-  if (total <= a.capacity) {
+  const int32_t cnt = a.pair_count[s];
+  const int32_t* list = a.fixed + s * kFixedPartners;
+  bool ok = true;
+  if (cnt > kFixedPartners) {
+    const int64_t total = a.pair_offset[a.n_slots];
+    ok = total <= a.capacity;
+    list = a.partners + a.pair_offset[s];
+  }
+  if (ok) {
     const Capsule me = load_capsule(a.cap, S, s);
-    const int64_t k0 = a.pair_offset[s], k1 = a.pair_offset[s + 1];
     ContactPoint pts[2];
-    for (int64_t k = k0; k < k1; ++k) {
-      const int64_t o = a.partners[k];
+    for (int32_t k = 0; k < cnt; ++k) {
+      const int64_t o = list[k];
       if (o >= 0 && o < a.n_slots) {
         const int32_t om = a.cap_material[o];
         if (om < 0) continue;
@@ -625,11 +642,11 @@ cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* l
   if (e != cudaSuccess) return e;
   scatter_kernel<<<gs, kThreads, 0, stream>>>(a);
   const unsigned ge = static_cast<unsigned>((a.n_caps + kThreads - 1) / kThreads);
-  if (ge > 0) pairs_kernel<false><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
+  if (ge > 0) pairs_kernel<0><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
   *launches += 2;
-  e = exclusive_scan<int64_t>(a.pair_count, a.pair_offset, a.n_slots, a.scan_blocks, false, stream, launches);
+  e = exclusive_scan<int64_t>(a.ovf_count, a.pair_offset, a.n_slots, a.scan_blocks, false, stream, launches);
   if (e != cudaSuccess) return e;
-  if (ge > 0) pairs_kernel<true><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
+  if (ge > 0) pairs_kernel<1><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
   force_kernel<<<gs, kThreads, 0, stream>>>(a);
   *launches += 2;
   return cudaGetLastError();

@@ -23,6 +23,10 @@ enum CapsuleRow : int {
   kCapRows = 20
 };
 
+// partners a capsule keeps in its fixed-stride list; a capsule with more
+// (a pile-up) gets its whole list in the overflow lists instead
+constexpr int kFixedPartners = 32;
+
 struct ContactPlane {
   double p[3];   // point on the plane
   double n[3];   // unit normal
@@ -58,9 +62,11 @@ struct ContactArgs {
   int32_t* sorted_id;                // capsules grouped by bucket
   int32_t* sorted_cell;              // 3 per entry
   double* sorted_box;                // 6 per entry
-  int32_t* pair_count;               // stride (zero outside capsules)
-  int64_t* pair_offset;              // n_slots + 1
-  int32_t* partners;                 // capacity
+  int32_t* pair_count;               // stride (zero outside capsules): partners per capsule
+  int32_t* fixed;                    // kFixedPartners x stride: partner lists of up to kFixedPartners
+  int32_t* ovf_count;                // stride: the count of capsules beyond kFixedPartners, else 0
+  int64_t* pair_offset;              // n_slots + 1: offsets of the overflow lists
+  int32_t* partners;                 // capacity: overflow lists
   int64_t capacity;
   unsigned long long* required;      // largest pair total seen when over capacity
   const ContactPlane* planes;

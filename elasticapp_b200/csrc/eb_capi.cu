@@ -125,6 +125,8 @@ struct ContactDevice {
   int32_t* sorted_cell = nullptr;
   double* sorted_box = nullptr;
   int32_t* pair_count = nullptr;
+  int32_t* fixed = nullptr;
+  int32_t* ovf_count = nullptr;
   int64_t* pair_offset = nullptr;
   int32_t* partners = nullptr;
   unsigned long long* required = nullptr;
@@ -343,7 +345,8 @@ void host_free(eb_sim* s) {
     }
   ContactDevice& c = s->contact;
   void* cptrs[] = {c.cap, c.cap_material, c.extent, c.cell, c.bucket, c.bucket_count, c.bucket_start,
-                   c.sorted_id, c.sorted_cell, c.sorted_box, c.pair_count, c.pair_offset, c.partners,
+                   c.sorted_id, c.sorted_cell, c.sorted_box, c.pair_count, c.fixed, c.ovf_count, c.pair_offset,
+                   c.partners,
                    c.required, c.planes, c.pair_table, c.loads, c.scan_blocks, c.backup};
   for (void* p : cptrs)
     if (p) cudaFree(p);
@@ -441,7 +444,7 @@ eb_status setup_contact(eb_sim* s) {
   int64_t table = 1024;
   while (table < 2 * n_caps) table <<= 1;
   c.table_mask = static_cast<uint32_t>(table - 1);
-  c.capacity = std::max<int64_t>(int64_t(1) << 16, 24 * n_caps);
+  c.capacity = std::max<int64_t>(int64_t(1) << 16, 4 * n_caps);  // overflow lists only
   const size_t nm = s->materials.size();
   std::vector<eb::ContactPair> pairs(nm * nm);
   for (size_t i = 0; i < nm; ++i)
@@ -470,6 +473,8 @@ eb_status setup_contact(eb_sim* s) {
   alloc(&c.sorted_cell, static_cast<size_t>(3 * n_caps) * sizeof(int32_t));
   alloc(&c.sorted_box, static_cast<size_t>(6 * n_caps) * sizeof(double));
   alloc(&c.pair_count, static_cast<size_t>(S) * sizeof(int32_t));
+  alloc(&c.fixed, static_cast<size_t>(S) * eb::kFixedPartners * sizeof(int32_t));
+  alloc(&c.ovf_count, static_cast<size_t>(S) * sizeof(int32_t));
   alloc(&c.pair_offset, static_cast<size_t>(s->n_slots + 1) * sizeof(int64_t));
   alloc(&c.partners, static_cast<size_t>(c.capacity) * sizeof(int32_t));
   alloc(&c.required, sizeof(unsigned long long));
@@ -1175,6 +1180,8 @@ eb::ContactArgs contact_args(eb_sim* s, double dt) {
   a.sorted_cell = c.sorted_cell;
   a.sorted_box = c.sorted_box;
   a.pair_count = c.pair_count;
+  a.fixed = c.fixed;
+  a.ovf_count = c.ovf_count;
   a.pair_offset = c.pair_offset;
   a.partners = c.partners;
   a.capacity = c.capacity;
@@ -1327,29 +1334,36 @@ EB_API eb_status eb_contact_pairs(eb_sim* s, int64_t* pairs, int64_t capacity, i
   if (!c.on) return fail(EB_ERR_UNSUPPORTED, "no rod takes part in contact");
   if (!c.evaluated) return fail(EB_ERR_INVALID_STATE, "no contact evaluation yet: step first");
   if (eb_status st = set_device(s)) return st;
-  std::vector<int64_t> off(static_cast<size_t>(s->n_slots + 1));
+  const size_t n = static_cast<size_t>(s->n_slots);
+  std::vector<int32_t> cnt(n), fixed(n * eb::kFixedPartners);
+  std::vector<int64_t> off(n + 1);
+  EB_CUDA(cudaMemcpyAsync(cnt.data(), c.pair_count, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaMemcpyAsync(fixed.data(), c.fixed, fixed.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
   EB_CUDA(cudaMemcpyAsync(off.data(), c.pair_offset, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
                           s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
-  const int64_t total = off[static_cast<size_t>(s->n_slots)];
+  const int64_t total = off[n];
   if (total > c.capacity) return fail(EB_ERR_INVALID_STATE, "the last evaluation overflowed the pair buffer");
   std::vector<int32_t> part(static_cast<size_t>(std::max<int64_t>(total, 1)));
   if (total > 0)
     EB_CUDA(cudaMemcpyAsync(part.data(), c.partners, static_cast<size_t>(total) * sizeof(int32_t),
                             cudaMemcpyDeviceToHost, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
-  int64_t n = 0;
-  for (int64_t a = 0; a < s->n_slots; ++a)
-    for (int64_t k = off[static_cast<size_t>(a)]; k < off[static_cast<size_t>(a + 1)]; ++k) {
-      const int64_t b = part[static_cast<size_t>(k)];
-      if (b <= a) continue;
-      if (n < capacity) {
-        pairs[2 * n] = a;
-        pairs[2 * n + 1] = b;
+  int64_t m = 0;
+  for (size_t a = 0; a < n; ++a) {
+    const int32_t k = cnt[a];
+    const int32_t* list = k <= eb::kFixedPartners ? &fixed[a * eb::kFixedPartners] : &part[static_cast<size_t>(off[a])];
+    for (int32_t j = 0; j < k; ++j) {
+      const int64_t b = list[j];
+      if (b <= static_cast<int64_t>(a)) continue;
+      if (m < capacity) {
+        pairs[2 * m] = static_cast<int64_t>(a);
+        pairs[2 * m + 1] = b;
       }
-      ++n;
+      ++m;
     }
-  *count = n;
+  }
+  *count = m;
   return check_device_status(s);
 }
 

@@ -402,6 +402,14 @@ void land(eb_server* s, Request& r) {
       scale += std::fabs(e0[5 * k + c]);
       finite = finite && std::isfinite(e1[5 * k + c]);
     }
+  // plus the gravitational energy range of each rod over its own length, so a
+  // rod that starts near the potential's zero is not held to a tighter check
+  if (r.options & EB_REQUEST_GRAVITY) {
+    const double g = std::sqrt(r.gravity[0] * r.gravity[0] + r.gravity[1] * r.gravity[1] +
+                               r.gravity[2] * r.gravity[2]);
+    for (const auto& p : r.rods)
+      scale += p.density * (M_PI * p.radius * p.radius * p.length) * g * p.length;
+  }
   r.e0 = E0;
   r.e1 = E1;
   r.escale = scale;

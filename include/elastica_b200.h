@@ -330,8 +330,9 @@ EB_API eb_status eb_partition_rods(const int64_t* weights, int64_t n, int32_t n_
  * to host memory on the server's stream and its bins are reused at once;
  * eb_server_poll reports completions without blocking.  Mixed-precision
  * requests whose mechanical energy (kinetic + elastic + gravitational) grows
- * by more than energy_tolerance times the sum of its initial magnitudes, or
- * turns non-finite, are rerun in FP64 from their initial conditions.  Rods of
+ * by more than energy_tolerance times a scale (the sum of the initial energy
+ * magnitudes plus m |g| L of every rod), or turns non-finite, are rerun in
+ * FP64 from their initial conditions.  Rods of
  * a request hold at most 519 elements (one bin). */
 typedef struct eb_server_config {
   int32_t device;
