@@ -24,6 +24,7 @@ EB_FLAG_REFERENCE_ROUNDING = 0x2
 EB_FLAG_STEP_STREAMING = 0x4
 EB_FLAG_STEP_RESIDENT = 0x8
 EB_FLAG_CUDA_GRAPH = 0x10
+EB_FLAG_STEP_BUCKETED = 0x20
 EB_STEPPER_POSITION_VERLET = 0
 EB_STEPPER_PEFRL = 1
 EB_ROD_DAMPED = 0

@@ -31,6 +31,10 @@ cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start
                                   int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
                                    int config, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_fp64_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                         int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                          int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -165,8 +169,19 @@ struct eb_sim {
   int64_t launches = 0;
   // step plan: streaming kernel (one launch per step) or the resident kernel
   // with one of the block configurations, chosen by timing both
-  int plan_mode = 0;    // 0 undecided, 1 streaming, 2 resident
+  int plan_mode = 0;    // 0 undecided, 1 streaming, 2 resident, 3 resident per size bucket
   int plan_config = -1;
+  // per-size-bucket plan: bucket 0 holds the rods of at most 263 elements,
+  // bucket 1 the rods of 264 to 519; per bucket and configuration a gathered
+  // work list (CTA offsets into a list of slots)
+  struct Bucket {
+    int64_t* d_off[4] = {nullptr, nullptr, nullptr, nullptr};
+    int32_t* d_map[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n_ctas[4] = {0, 0, 0, 0};
+    int64_t rods = 0;
+  };
+  Bucket buckets[2];
+  int bucket_config[2] = {-1, -1};
   std::vector<int64_t*> d_cta_start;  // per block configuration (or null)
   std::vector<int> n_ctas;
   float plan_ms[16] = {0};
@@ -338,6 +353,13 @@ void host_free(eb_sim* s) {
   for (auto* p : s->d_cta_start)
     if (p) cudaFree(p);
   s->d_cta_start.clear();
+  for (auto& b : s->buckets) {
+    for (int c = 0; c < 4; ++c) {
+      if (b.d_off[c]) cudaFree(b.d_off[c]);
+      if (b.d_map[c]) cudaFree(b.d_map[c]);
+    }
+    b = eb_sim::Bucket{};
+  }
   for (auto& g : s->graph)
     if (g) {
       cudaGraphExecDestroy(g);
@@ -536,7 +558,8 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
   if (cfg.stepper == EB_STEPPER_PEFRL && cfg.precision == EB_PRECISION_MIXED)
     return fail(EB_ERR_UNSUPPORTED, "PEFRL runs on the FP64 streaming kernel only");
   if (cfg.flags & ~static_cast<uint32_t>(EB_FLAG_RECORD_DIAGNOSTICS | EB_FLAG_REFERENCE_ROUNDING |
-                                          EB_FLAG_STEP_STREAMING | EB_FLAG_STEP_RESIDENT | EB_FLAG_CUDA_GRAPH))
+                                          EB_FLAG_STEP_STREAMING | EB_FLAG_STEP_RESIDENT | EB_FLAG_CUDA_GRAPH |
+                                          EB_FLAG_STEP_BUCKETED))
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown flag");
   int ndev = 0;
   EB_CUDA(cudaGetDeviceCount(&ndev));
@@ -1087,6 +1110,100 @@ eb_status graph_steps(eb_sim* s, double dt) {
   return EB_OK;
 }
 
+// Per-size-bucket work lists: the rods of each bucket, in slot order, packed
+// next-fit into CTAs of each configuration's capacity; a CTA's slots are
+// listed in a gather map, so its rods need not be neighbours in the layout.
+constexpr int64_t kShortRodSlots = 264;
+eb_status build_bucket_worklists(eb_sim* s) {
+  for (int b = 0; b < 2; ++b) {
+    std::vector<size_t> rods;
+    for (size_t r = 0; r < s->rods.size(); ++r) {
+      const int64_t w = s->rods[r].n + 1;
+      if ((b == 0 && w <= kShortRodSlots) || (b == 1 && w > kShortRodSlots && w <= 520)) rods.push_back(r);
+    }
+    s->buckets[b].rods = static_cast<int64_t>(rods.size());
+    if (rods.empty()) continue;
+    for (int c = 0; c < eb::block_config_count(); ++c) {
+      const int64_t cap = eb::block_config_capacity(c);
+      std::vector<int64_t> off{0};
+      std::vector<int32_t> map;
+      int64_t used = 0;
+      bool fits = true;
+      for (size_t r : rods) {
+        const int64_t w = s->rods[r].n + 1;
+        if (w > cap) {
+          fits = false;
+          break;
+        }
+        if (used + w > cap) {
+          off.push_back(static_cast<int64_t>(map.size()));
+          used = 0;
+        }
+        for (int64_t j = 0; j < w; ++j) map.push_back(static_cast<int32_t>(s->offsets[r] + j));
+        used += w;
+      }
+      if (!fits) continue;
+      off.push_back(static_cast<int64_t>(map.size()));
+      eb_sim::Bucket& B = s->buckets[b];
+      EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&B.d_off[c]), off.size() * sizeof(int64_t)));
+      EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&B.d_map[c]), map.size() * sizeof(int32_t)));
+      EB_CUDA(cudaMemcpyAsync(B.d_off[c], off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                              s->stream));
+      EB_CUDA(cudaMemcpyAsync(B.d_map[c], map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              s->stream));
+      B.n_ctas[c] = static_cast<int>(off.size() - 1);
+    }
+  }
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+cudaError_t launch_bucket(eb_sim* s, eb::StepArgs& a, int b, int config, int steps) {
+  const eb_sim::Bucket& B = s->buckets[b];
+  if (s->cfg.precision == EB_PRECISION_MIXED)
+    return eb::launch_rod_block_mixed_gather(a, B.d_off[config], B.d_map[config], B.n_ctas[config], steps, config,
+                                             s->any_damped, s->stream);
+  return eb::launch_rod_block_fp64_gather(a, B.d_off[config], B.d_map[config], B.n_ctas[config], steps, config,
+                                          s->any_damped, s->stream);
+}
+
+// Per-size-bucket plan: when the batch has both short and long rods (and none
+// longer than 519 elements), time every configuration on each bucket alone
+// for kProbeSteps steps into the spare buffer; *total_ms = the sum of the two
+// buckets' best times, or -1 when the plan does not apply.
+eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cudaEvent_t e1, float* total_ms) {
+  *total_ms = -1.0f;
+  for (const auto& r : s->rods)
+    if (r.n + 1 > 520) return EB_OK;
+  if (eb_status st = build_bucket_worklists(s)) return st;
+  if (s->buckets[0].rods == 0 || s->buckets[1].rods == 0) return EB_OK;
+  eb::StepArgs a = args;
+  float bucket_best[2] = {0.0f, 0.0f};
+  int bucket_cfg[2] = {-1, -1};
+  for (int b = 0; b < 2; ++b)
+    for (int c = 0; c < eb::block_config_count(); ++c) {
+      if (!s->buckets[b].d_off[c]) continue;
+      for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
+        EB_CUDA(cudaEventRecord(e0, s->stream));
+        EB_CUDA(launch_bucket(s, a, b, c, kProbeSteps));
+        EB_CUDA(cudaEventRecord(e1, s->stream));
+        EB_CUDA(cudaEventSynchronize(e1));
+      }
+      float ms = 0.0f;
+      EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      s->plan_ms[5 + 4 * b + c] = ms;
+      if (bucket_cfg[b] < 0 || ms < bucket_best[b]) {
+        bucket_best[b] = ms;
+        bucket_cfg[b] = c;
+      }
+    }
+  if (bucket_cfg[0] < 0 || bucket_cfg[1] < 0) return EB_OK;
+  s->bucket_config[0] = bucket_cfg[0];
+  s->bucket_config[1] = bucket_cfg[1];
+  *total_ms = bucket_best[0] + bucket_best[1];
+  return EB_OK;
+}
+
 // Choose between the streaming kernel and the resident configurations by
 // timing each for kProbeSteps steps from the current state into the spare
 // buffer (the current state is left untouched).
@@ -1118,6 +1235,19 @@ eb_status plan_steps(eb_sim* s, double dt) {
   a.out = s->d_state[s->cur ^ 1];
   float best = 0.0f;
   int best_mode = 1, best_cfg = -1;
+  float bucket_ms = -1.0f;
+  bool bucket_done = false;
+  if (s->cfg.flags & EB_FLAG_STEP_BUCKETED) {
+    bucket_done = true;
+    if (eb_status st = probe_buckets(s, a, e0, e1, &bucket_ms)) return st;
+    if (bucket_ms >= 0.0f) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      s->plan_mode = 3;
+      s->plan_config = s->bucket_config[0] + 4 * s->bucket_config[1];
+      return check_device_status(s);
+    }
+  }
   // mixed precision exists only on the resident kernels: the streaming FP64
   // kernel is then a fallback for rods too long for any configuration
   const bool force_resident =
@@ -1148,9 +1278,17 @@ eb_status plan_steps(eb_sim* s, double dt) {
       best_cfg = c;
     }
   }
+  if (best_mode == 2 && best_cfg < 0) best_mode = 1;
+  // per size bucket: keep the best pair if it beats the plans above
+  if (!bucket_done) {
+    if (eb_status st = probe_buckets(s, a, e0, e1, &bucket_ms)) return st;
+    if (bucket_ms >= 0.0f && bucket_ms < best) {
+      best_mode = 3;
+      best_cfg = s->bucket_config[0] + 4 * s->bucket_config[1];
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (best_mode == 2 && best_cfg < 0) best_mode = 1;
   s->plan_mode = best_mode;
   s->plan_config = best_cfg;
   return check_device_status(s);
@@ -1294,7 +1432,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   }
   eb::StepArgs a = step_args(s, dt);
   int64_t done = 0;
-  if (s->plan_mode == 2) {
+  if (s->plan_mode == 2 || s->plan_mode == 3) {
     // resident kernel in chunks; the last step of a call that records
     // diagnostics runs on the streaming kernel, which writes them
     const int64_t resident_steps = diag ? n_steps - 1 : n_steps;
@@ -1303,9 +1441,16 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
       const int k = static_cast<int>(std::min<int64_t>(kResidentChunk, resident_steps - done));
       a.in = s->d_state[s->cur];
       a.out = s->d_state[s->cur ^ 1];
-      EB_CUDA(launch_resident(s, a, c, k));
+      if (s->plan_mode == 2) {
+        EB_CUDA(launch_resident(s, a, c, k));
+        ++s->launches;
+      } else {
+        // one launch per size bucket over the same buffers
+        EB_CUDA(launch_bucket(s, a, 0, s->bucket_config[0], k));
+        EB_CUDA(launch_bucket(s, a, 1, s->bucket_config[1], k));
+        s->launches += 2;
+      }
       s->cur ^= 1;
-      ++s->launches;
       done += k;
     }
   }

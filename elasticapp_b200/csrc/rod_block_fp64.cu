@@ -73,9 +73,12 @@ __device__ __forceinline__ int param_row(int f) {
 
 // kServe: the CTA's slot range, step count, time step and environment come
 // from serve[blockIdx.x] (serving launches)
-template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe>
+// kGather: cta_start indexes gmap, the list of the CTA's slots (rods that
+// need not be neighbours in the slot layout)
+template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false>
 __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
-                                                                    int n_steps_launch, const ServeCta* serve) {
+                                                                    int n_steps_launch, const ServeCta* serve,
+                                                                    const int32_t* gmap) {
   extern __shared__ __align__(128) double smem[];
   const BRows<kCap> R{smem};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + bRows * kCap);
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
 
   // ---- stage state, parameters and slot metadata (coalesced loads)
   for (int s = tid; s < count; s += kThreads) {
-    const int64_t g = g0 + s;
+    const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
     meta_s[s] = a.meta[g];
 #pragma unroll 1
     for (int f = 0; f < kStateFields; ++f) R.at(f, s) = a.in[f * S + g];
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   // ---- final half drift and write-back
   for (int s = tid; s < count; s += kThreads) {
     const uint32_t meta = meta_s[s];
-    const int64_t g = g0 + s;
+    const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
     const D3 v = R.get3(bV, s);
     D3 x = R.get3(bX, s);
     x = {x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z};
@@ -318,18 +321,18 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
 }
 
-template <int kCap, int kThreads, bool kSplit, bool kServe = false>
+template <int kCap, int kThreads, bool kSplit, bool kServe = false, bool kGather = false>
 cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
-                             cudaStream_t stream, const ServeCta* serve = nullptr) {
+                             cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
   const size_t bytes = size_t(bRows) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve);
+    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
     return cudaGetLastError();
   };
-  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe>)
-                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe>);
+  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather>)
+                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather>);
 }
 
 }  // namespace
@@ -365,6 +368,20 @@ cudaError_t launch_rod_block_fp64_serve(const StepArgs& args, const ServeCta* se
                                         bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
   return launch_block_cfg<520, 256, true, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+}
+
+// Gathered CTAs: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),
+// whole rods in slot order (the per-size-bucket plans).
+cudaError_t launch_rod_block_fp64_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                         int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  switch (config) {
+    case 0: return launch_block_cfg<520, 512, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 1: return launch_block_cfg<520, 256, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 2: return launch_block_cfg<264, 256, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 3: return launch_block_cfg<264, 288, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace eb

@@ -181,9 +181,12 @@ __device__ __forceinline__ int mixed_param_row(int f) {
 // kServe: the CTA's slot range, step count, time step and environment come
 // from serve[blockIdx.x] (serving launches) instead of the work list and the
 // launch-wide values
-template <int kCap, int kThreads, int kMinBlocks, bool kDamped, bool kServe>
+// kGather: cta_start indexes gmap, the list of the CTA's slots (rods that
+// need not be neighbours in the slot layout)
+template <int kCap, int kThreads, int kMinBlocks, bool kDamped, bool kServe, bool kGather = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
-    rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps_launch, const ServeCta* serve) {
+    rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps_launch, const ServeCta* serve,
+                           const int32_t* gmap) {
   extern __shared__ __align__(128) double smem[];
   const MRows<kCap> R{smem, reinterpret_cast<float*>(smem + dRowsD * kCap)};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + fRowsF * kCap);
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   // ---- stage state, parameters, reciprocals, FP32 copies and rod data
   const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
   for (int s = tid; s < count; s += kThreads) {
-    const int64_t g = g0 + s;
+    const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
     const uint32_t meta = a.meta[g];
     meta_s[s] = meta;
     uint32_t rf = 0;
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       drift(R, s, meta, last ? hdt : dt, v, w);
       if (clamped) clamp_value(R, s, a.rods[meta >> kRodShift]);
       if (last) {
-        const int64_t g = g0 + s;
+        const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
 #pragma unroll
         for (int fld = 0; fld < 6; ++fld) a.out[fld * S + g] = R.ad(fld, s);
         if (meta & kElem) {
@@ -435,19 +438,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
 }
 
-template <int kCap, int kThreads, int kMinBlocks, bool kServe = false>
+template <int kCap, int kThreads, int kMinBlocks, bool kServe = false, bool kGather = false>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
-                             cudaStream_t stream, const ServeCta* serve = nullptr) {
+                             cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
   const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(fRowsF) * kCap * sizeof(float) +
                        2 * size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve);
+    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
     return cudaGetLastError();
   };
-  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true, kServe>)
-                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false, kServe>);
+  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true, kServe, kGather>)
+                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false, kServe, kGather>);
 }
 
 }  // namespace
@@ -473,6 +476,20 @@ cudaError_t launch_rod_block_mixed_serve(const StepArgs& args, const ServeCta* s
                                          bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
   return launch_mixed_cfg<520, 256, 1, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+}
+
+// Gathered CTAs: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),
+// whole rods in slot order (the per-size-bucket plans).
+cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                          int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  switch (config) {
+    case 0: return launch_mixed_cfg<520, 512, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 1: return launch_mixed_cfg<520, 256, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 2: return launch_mixed_cfg<264, 256, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 3: return launch_mixed_cfg<264, 288, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace eb

@@ -222,7 +222,8 @@ class Simulator:
         cfg.precision = {"fp64": L.EB_PRECISION_FP64, "mixed": L.EB_PRECISION_MIXED}[precision]
         cfg.flags = (L.EB_FLAG_RECORD_DIAGNOSTICS if record_diagnostics else 0) | (
             L.EB_FLAG_REFERENCE_ROUNDING if reference_rounding else 0) | {
-            "auto": 0, "streaming": L.EB_FLAG_STEP_STREAMING, "resident": L.EB_FLAG_STEP_RESIDENT}[step_mode]
+            "auto": 0, "streaming": L.EB_FLAG_STEP_STREAMING, "resident": L.EB_FLAG_STEP_RESIDENT,
+            "bucketed": L.EB_FLAG_STEP_BUCKETED}[step_mode]
         cfg.step_window = int(window)
         cfg.resident_config = int(resident_config)
         if cuda_graph:
@@ -356,7 +357,7 @@ class Simulator:
         mode, cfg = ctypes.c_int32(), ctypes.c_int32()
         ms = (ctypes.c_float * 16)()
         L.call("eb_step_plan", self._h, ctypes.byref(mode), ctypes.byref(cfg), ms, 16)
-        return {"mode": {0: "undecided", 1: "streaming", 2: "resident"}[mode.value], "config": cfg.value,
+        return {"mode": {0: "undecided", 1: "streaming", 2: "resident", 3: "bucketed"}[mode.value], "config": cfg.value,
                 "probe_ms": list(ms)}
 
     def launch_count(self) -> int:

@@ -81,6 +81,13 @@ typedef enum eb_precision {
                                            of 32 steps: one graph launch
                                            instead of 32 (128 with PEFRL)
                                            kernel launches */
+#define EB_FLAG_STEP_BUCKETED 0x20u    /* always use the per-size-bucket
+                                           resident plan (rods of at most 263
+                                           elements and rods of 264 to 519 in
+                                           separate launches, each with its
+                                           fastest configuration) when the
+                                           batch has rods of both sizes and
+                                           none longer */
 
 typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
@@ -305,8 +312,11 @@ EB_API eb_status eb_energy(struct eb_sim* sim, double* out, int64_t count);
 EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
 
 /* The step plan chosen by the first eb_step: mode 1 = streaming kernel,
- * 2 = resident kernel with block configuration `config`; probe_ms[0] is the
- * streaming probe time, probe_ms[1 + c] configuration c's (up to count). */
+ * 2 = resident kernel with block configuration `config`, 3 = resident kernel
+ * per size bucket (rods of at most 263 elements with configuration config % 4,
+ * rods of 264 to 519 with config / 4, one launch each); probe_ms[0] is the
+ * streaming probe time, probe_ms[1 + c] configuration c's on the whole batch,
+ * probe_ms[5 + 4 b + c] configuration c's on bucket b alone (up to count). */
 EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* config, float* probe_ms,
                               int32_t count);
 

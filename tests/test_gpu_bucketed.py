@@ -1,0 +1,88 @@
+"""Per-size-bucket resident plan (GPU).
+
+Rods of at most 263 elements and rods of 264 to 519 elements run in separate
+launches over one state buffer, each bucket packed into its own CTAs through
+a gathered slot list and each with the configuration that timed fastest on
+it.  The plan must give the same rods the same results as the whole-batch
+resident plan and meet the oracle's FP64 parity bounds; its mixed-precision
+form meets the mixed path's tip tolerance."""
+import numpy as np
+import pytest
+
+import elasticapp_b200 as eb
+from elasticapp_b200 import workloads as W
+
+import oracle_bridge as B
+
+pytestmark = pytest.mark.gpu
+
+TIP_TOL = 1e-5
+STATE = ("Position", "Velocity", "Director", "AngularVelocity")
+
+
+def two_bucket_batch(n_rods=24, seed=31):
+    # rod lengths drawn across both buckets, interleaved in the slot layout
+    return W.uneven_batch(n_rods=n_rods, seed=seed, n_range=(8, 500), n_steps=300)
+
+
+def test_bucketed_plan_matches_oracle_and_resident_plan():
+    wl = two_bucket_batch()
+    n = np.array(wl.n_elements)
+    assert (n + 1 <= 264).any() and (n + 1 > 264).any()
+    sim = wl.build(step_mode="bucketed")
+    sim.step(eb.PositionVerlet(), 0.0, wl.dt, 300)
+    plan = sim.step_plan()
+    assert plan["mode"] == "bucketed"
+    c_short, c_long = plan["config"] % 4, plan["config"] // 4
+    assert plan["probe_ms"][5 + c_short] > 0.0 and plan["probe_ms"][9 + c_long] > 0.0
+    assert c_long in (0, 1)  # the long bucket needs the 520-slot configurations
+    # the oracle's FP64 parity bounds
+    orc, spread = B.oracle_spread(wl, 300)
+    want = B.state_slots(orc)
+    bounds = B.parity_bounds(spread)
+    for name, place in (("Position", 0), ("Velocity", 0), ("Director", 1), ("AngularVelocity", 1)):
+        err = B.max_rel_error_per_rod(sim.get_slots(name), want[name], wl.n_elements, place)
+        assert err <= bounds[name], (name, err, bounds[name])
+    # the whole-batch resident plan over the same steps
+    ref = wl.build(step_mode="resident")
+    ref.step(eb.PositionVerlet(), 0.0, wl.dt, 300)
+    assert ref.step_plan()["mode"] == "resident"
+    for name in STATE:
+        a, b = sim.get_slots(name), ref.get_slots(name)
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b))), name
+
+
+def test_bucketed_plan_is_deterministic_and_chunked():
+    wl = two_bucket_batch(n_rods=12, seed=5)
+    a = wl.build(step_mode="bucketed")
+    b = wl.build(step_mode="bucketed")
+    a.step(eb.PositionVerlet(), 0.0, wl.dt, 300)  # 128 + 128 + 44 steps per bucket
+    for k in (100, 7, 193):
+        b.step(eb.PositionVerlet(), 0.0, wl.dt, k)
+    for name in STATE:
+        assert np.array_equal(a.get_slots(name), b.get_slots(name)), name
+    assert a.launch_count() >= 6
+
+
+def test_bucketed_mixed_precision_tip_error():
+    wl = W.mixed_batch(n_rods=24, seed=77, n_range=(64, 500))
+    n = np.array(wl.n_elements)
+    assert (n + 1 <= 264).any() and (n + 1 > 264).any()
+    ref = wl.build(step_mode="streaming")
+    ref.step(eb.PositionVerlet(), 0.0, wl.dt, 2000)
+    mix = wl.build(precision="mixed", step_mode="bucketed")
+    mix.step(eb.PositionVerlet(), 0.0, wl.dt, 2000)
+    assert mix.step_plan()["mode"] == "bucketed"
+    lengths = np.array([r.length for r in wl.rods])
+    tip = lambda s: np.stack([r.get("Position")[:, -1] for r in s.rods])
+    err = np.linalg.norm(tip(mix) - tip(ref), axis=1) / lengths
+    assert np.all(np.isfinite(err)) and err.max() <= TIP_TOL, err.max()
+
+
+@pytest.mark.parametrize("n_range,mode", [((8, 200), ("resident", "streaming")), ((300, 700), ("streaming",))])
+def test_bucketed_flag_falls_back_when_plan_does_not_apply(n_range, mode):
+    # one bucket only, or rods longer than 519 elements: the usual plan
+    wl = W.uneven_batch(n_rods=4, seed=3, n_range=n_range)
+    sim = wl.build(step_mode="bucketed")
+    sim.step(eb.PositionVerlet(), 0.0, wl.dt, 4)
+    assert sim.step_plan()["mode"] in mode
