@@ -365,10 +365,10 @@ def cantilever_section(eb, W, torch, args, local):
 
 def _serve_request(eb, W, rng):
     """One request of the serving stream: 1-256 rods (log-uniform), n ~
-    U{32..519}, horizon ~ U{1e3..1e5} steps, per-rod parameters as in the
+    U{32..1024}, horizon ~ U{1e3..1e5} steps, per-rod parameters as in the
     uneven batch (clamp, damper 0.1, gravity, node velocities N(0, 1e-3^2))."""
     k = int(min(256, max(1, round(float(np.exp(rng.uniform(0.0, np.log(256.0))))))))
-    rods, n, L, E, d = W._random_rods(rng, k, 32, 519)
+    rods, n, L, E, d = W._random_rods(rng, k, 32, 1024)
     vel = [rng.normal(0.0, 1e-3, size=(3, int(m) + 1)) for m in n]
     dt = 0.1 * float(np.min((L / n) / np.sqrt(E / 1000.0)))
     steps = int(rng.integers(1000, 100001))
@@ -428,9 +428,10 @@ def serving_section(eb, W, args, capacity_hint):
     window, and at a sustainable load (half the measured capacity)."""
     out = {"workload": "serve_stream", "hbm_budget_bytes": args.serve_budget, "precision": "mixed (FP64 fallback)",
            "steps_per_launch": 128,
-           "request": "1-256 rods log-uniform, n ~ U{32..519} (one 520-slot bin per CTA), horizon U{1e3..1e5}, "
+           "request": "1-256 rods log-uniform, n ~ U{32..1024} (520-slot bins, one CTA each; rods of 520 or more "
+                      "elements on a bin pair run by a 2-CTA cluster), horizon U{1e3..1e5}, "
                       "clamp + damper 0.1 + gravity, velocities N(0, 1e-3^2); dt = 0.1 min(l/c) per request"}
-    mean_work = 46.0 * 275.5 * 50500.0  # mean rods x mean n x mean horizon
+    mean_work = 46.0 * 528.0 * 50500.0  # mean rods x mean n x mean horizon
     out["stated_load"] = serve_stream(eb, W, 200.0, args.serve_seconds, args.serve_drain, 1005, args.serve_budget)
     rate = args.serve_rate if args.serve_rate > 0 else max(1.0, 0.5 * capacity_hint / mean_work)
     out["sustained_load"] = serve_stream(eb, W, rate, args.serve_seconds, args.serve_drain, 1006, args.serve_budget)

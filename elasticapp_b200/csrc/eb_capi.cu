@@ -35,6 +35,10 @@ cudaError_t launch_rod_block_fp64_gather(const StepArgs& args, const int64_t* ct
                                          int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
                                           int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_fp64_pairs(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                        int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
+cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                         int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream);
 cudaError_t launch_rod_energy(int64_t n_rods, int64_t stride, const int64_t* offsets,
                               const double* state, const double* params, double* out,
                               cudaStream_t stream);
@@ -172,16 +176,17 @@ struct eb_sim {
   int plan_mode = 0;    // 0 undecided, 1 streaming, 2 resident, 3 resident per size bucket
   int plan_config = -1;
   // per-size-bucket plan: bucket 0 holds the rods of at most 263 elements,
-  // bucket 1 the rods of 264 to 519; per bucket and configuration a gathered
-  // work list (CTA offsets into a list of slots)
+  // bucket 1 the rods of 264 to 519, bucket 2 the rods of 520 to 1039 (on
+  // CTA pairs); per bucket and configuration a gathered work list (CTA
+  // offsets into a list of slots)
   struct Bucket {
     int64_t* d_off[4] = {nullptr, nullptr, nullptr, nullptr};
     int32_t* d_map[4] = {nullptr, nullptr, nullptr, nullptr};
     int n_ctas[4] = {0, 0, 0, 0};
     int64_t rods = 0;
   };
-  Bucket buckets[2];
-  int bucket_config[2] = {-1, -1};
+  Bucket buckets[3];
+  int bucket_config[3] = {-1, -1, -1};
   std::vector<int64_t*> d_cta_start;  // per block configuration (or null)
   std::vector<int> n_ctas;
   float plan_ms[16] = {0};
@@ -1113,16 +1118,48 @@ eb_status graph_steps(eb_sim* s, double dt) {
 // Per-size-bucket work lists: the rods of each bucket, in slot order, packed
 // next-fit into CTAs of each configuration's capacity; a CTA's slots are
 // listed in a gather map, so its rods need not be neighbours in the layout.
+// Rods of the pair bucket each take a cluster of two CTAs: the first
+// ceil(W / 2) slots on the even CTA, the rest on the odd one.
 constexpr int64_t kShortRodSlots = 264;
+constexpr int kPairConfigs = 2;  // 512 or 256 threads per CTA
+int bucket_of(int64_t w) {
+  if (w <= kShortRodSlots) return 0;
+  if (w <= 520) return 1;
+  if (w <= eb::kPairMaxSlots) return 2;
+  return -1;
+}
+
 eb_status build_bucket_worklists(eb_sim* s) {
-  for (int b = 0; b < 2; ++b) {
+  if (s->buckets[0].rods + s->buckets[1].rods + s->buckets[2].rods > 0) return EB_OK;  // built already
+  for (int b = 0; b < 3; ++b) {
     std::vector<size_t> rods;
-    for (size_t r = 0; r < s->rods.size(); ++r) {
-      const int64_t w = s->rods[r].n + 1;
-      if ((b == 0 && w <= kShortRodSlots) || (b == 1 && w > kShortRodSlots && w <= 520)) rods.push_back(r);
-    }
+    for (size_t r = 0; r < s->rods.size(); ++r)
+      if (bucket_of(s->rods[r].n + 1) == b) rods.push_back(r);
     s->buckets[b].rods = static_cast<int64_t>(rods.size());
     if (rods.empty()) continue;
+    if (b == 2) {
+      std::vector<int64_t> off{0};
+      std::vector<int32_t> map;
+      for (size_t r : rods) {
+        const int64_t w = s->rods[r].n + 1, h = (w + 1) / 2;
+        for (int64_t j = 0; j < w; ++j) map.push_back(static_cast<int32_t>(s->offsets[r] + j));
+        off.push_back(off.back() + h);
+        off.push_back(off.back() + (w - h));
+      }
+      eb_sim::Bucket& B = s->buckets[2];
+      for (int c = 0; c < kPairConfigs; ++c) {  // one list, shared by both configurations
+        if (c == 0) {
+          EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&B.d_off[0]), off.size() * sizeof(int64_t)));
+          EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&B.d_map[0]), map.size() * sizeof(int32_t)));
+          EB_CUDA(cudaMemcpyAsync(B.d_off[0], off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                  s->stream));
+          EB_CUDA(cudaMemcpyAsync(B.d_map[0], map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                  s->stream));
+        }
+        B.n_ctas[c] = static_cast<int>(off.size() - 1);
+      }
+      continue;
+    }
     for (int c = 0; c < eb::block_config_count(); ++c) {
       const int64_t cap = eb::block_config_capacity(c);
       std::vector<int64_t> off{0};
@@ -1160,6 +1197,13 @@ eb_status build_bucket_worklists(eb_sim* s) {
 
 cudaError_t launch_bucket(eb_sim* s, eb::StepArgs& a, int b, int config, int steps) {
   const eb_sim::Bucket& B = s->buckets[b];
+  if (b == 2) {
+    if (s->cfg.precision == EB_PRECISION_MIXED)
+      return eb::launch_rod_block_mixed_pairs(a, B.d_off[0], B.d_map[0], B.n_ctas[config], steps, config,
+                                              s->any_damped, s->stream);
+    return eb::launch_rod_block_fp64_pairs(a, B.d_off[0], B.d_map[0], B.n_ctas[config], steps, config,
+                                           s->any_damped, s->stream);
+  }
   if (s->cfg.precision == EB_PRECISION_MIXED)
     return eb::launch_rod_block_mixed_gather(a, B.d_off[config], B.d_map[config], B.n_ctas[config], steps, config,
                                              s->any_damped, s->stream);
@@ -1167,22 +1211,26 @@ cudaError_t launch_bucket(eb_sim* s, eb::StepArgs& a, int b, int config, int ste
                                           s->any_damped, s->stream);
 }
 
-// Per-size-bucket plan: when the batch has both short and long rods (and none
-// longer than 519 elements), time every configuration on each bucket alone
-// for kProbeSteps steps into the spare buffer; *total_ms = the sum of the two
-// buckets' best times, or -1 when the plan does not apply.
+// Per-size-bucket plan: when the batch has rods of two or more buckets, or
+// rods of 520 to 1039 elements (and none longer), time every configuration on
+// each bucket alone for kProbeSteps steps into the spare buffer; *total_ms =
+// the sum of the buckets' best times, or -1 when the plan does not apply.
 eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cudaEvent_t e1, float* total_ms) {
   *total_ms = -1.0f;
   for (const auto& r : s->rods)
-    if (r.n + 1 > 520) return EB_OK;
+    if (bucket_of(r.n + 1) < 0) return EB_OK;
   if (eb_status st = build_bucket_worklists(s)) return st;
-  if (s->buckets[0].rods == 0 || s->buckets[1].rods == 0) return EB_OK;
+  const int used = (s->buckets[0].rods > 0) + (s->buckets[1].rods > 0) + (s->buckets[2].rods > 0);
+  if (used < 2 && s->buckets[2].rods == 0) return EB_OK;
   eb::StepArgs a = args;
-  float bucket_best[2] = {0.0f, 0.0f};
-  int bucket_cfg[2] = {-1, -1};
-  for (int b = 0; b < 2; ++b)
-    for (int c = 0; c < eb::block_config_count(); ++c) {
-      if (!s->buckets[b].d_off[c]) continue;
+  float total = 0.0f;
+  for (int b = 0; b < 3; ++b) {
+    s->bucket_config[b] = -1;
+    if (s->buckets[b].rods == 0) continue;
+    float best = 0.0f;
+    const int n_cfg = b == 2 ? kPairConfigs : eb::block_config_count();
+    for (int c = 0; c < n_cfg; ++c) {
+      if (!s->buckets[b].d_off[b == 2 ? 0 : c]) continue;
       for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
         EB_CUDA(cudaEventRecord(e0, s->stream));
         EB_CUDA(launch_bucket(s, a, b, c, kProbeSteps));
@@ -1192,16 +1240,22 @@ eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cud
       float ms = 0.0f;
       EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       s->plan_ms[5 + 4 * b + c] = ms;
-      if (bucket_cfg[b] < 0 || ms < bucket_best[b]) {
-        bucket_best[b] = ms;
-        bucket_cfg[b] = c;
+      if (s->bucket_config[b] < 0 || ms < best) {
+        best = ms;
+        s->bucket_config[b] = c;
       }
     }
-  if (bucket_cfg[0] < 0 || bucket_cfg[1] < 0) return EB_OK;
-  s->bucket_config[0] = bucket_cfg[0];
-  s->bucket_config[1] = bucket_cfg[1];
-  *total_ms = bucket_best[0] + bucket_best[1];
+    if (s->bucket_config[b] < 0) return EB_OK;
+    total += best;
+  }
+  *total_ms = total;
   return EB_OK;
+}
+
+int bucket_plan_config(const eb_sim* s) {
+  int c = 0;
+  for (int b = 2; b >= 0; --b) c = 4 * c + std::max(0, s->bucket_config[b]);
+  return c;
 }
 
 // Choose between the streaming kernel and the resident configurations by
@@ -1244,7 +1298,7 @@ eb_status plan_steps(eb_sim* s, double dt) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       s->plan_mode = 3;
-      s->plan_config = s->bucket_config[0] + 4 * s->bucket_config[1];
+      s->plan_config = bucket_plan_config(s);
       return check_device_status(s);
     }
   }
@@ -1282,9 +1336,12 @@ eb_status plan_steps(eb_sim* s, double dt) {
   // per size bucket: keep the best pair if it beats the plans above
   if (!bucket_done) {
     if (eb_status st = probe_buckets(s, a, e0, e1, &bucket_ms)) return st;
-    if (bucket_ms >= 0.0f && bucket_ms < best) {
+    // (mixed precision: the streaming kernel was not timed, so any bucket
+    // plan beats the FP64 fallback)
+    const bool have_best = best_cfg >= 0 || !force_resident;
+    if (bucket_ms >= 0.0f && (!have_best || bucket_ms < best)) {
       best_mode = 3;
-      best_cfg = s->bucket_config[0] + 4 * s->bucket_config[1];
+      best_cfg = bucket_plan_config(s);
     }
   }
   cudaEventDestroy(e0);
@@ -1446,9 +1503,11 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
         ++s->launches;
       } else {
         // one launch per size bucket over the same buffers
-        EB_CUDA(launch_bucket(s, a, 0, s->bucket_config[0], k));
-        EB_CUDA(launch_bucket(s, a, 1, s->bucket_config[1], k));
-        s->launches += 2;
+        for (int b = 0; b < 3; ++b) {
+          if (s->buckets[b].rods == 0) continue;
+          EB_CUDA(launch_bucket(s, a, b, s->bucket_config[b], k));
+          ++s->launches;
+        }
       }
       s->cur ^= 1;
       done += k;

@@ -110,6 +110,12 @@ struct StepArgs {
   const double* contact_torque;
 };
 
+// Rods longer than one CTA's capacity run on a pair of CTAs (a thread-block
+// cluster of two): the left CTA holds the first ceil(W / 2) of the rod's W
+// slots, the right CTA the rest, and neighbour reads across the split go to
+// the partner's shared memory.
+constexpr int kPairMaxSlots = 1040;  // two 520-slot halves
+
 // Per-CTA work of the serving launches (resident kernels): the CTA's slot
 // range, its step count for this launch and the time step and environment of
 // the request that owns it.
@@ -121,7 +127,7 @@ struct ServeCta {
   double half_dt;
   double gravity[3];
   uint32_t flags;  // kSim* bits of the request
-  uint32_t pad;
+  uint32_t pair;   // 1: this CTA and CTA (index ^ 1) hold the two halves of one rod
 };
 
 // device status bits reported back to the host

@@ -19,6 +19,15 @@
 // dt differs from two by dt/2 by ~1e-14 per step, which the stiff rod modes
 // amplify into angular-velocity differences far above rounding.  The kernel
 // keeps a compile-time switch for it, unused by the configurations below.)
+//
+// Rod pairs (kPair): a rod of up to 1039 elements runs on a cluster of two
+// CTAs, each holding half of its slots.  Reads of a neighbouring slot past
+// the left half's end or before the right half's start go to the partner's
+// shared memory (distributed shared memory), and the barriers that order a
+// phase's writes before the next phase's neighbour reads become cluster
+// barriers.  Serving launches mix pairs and single CTAs in one cluster
+// launch; a single CTA takes only CTA barriers.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "eb_internal.h"
@@ -52,6 +61,25 @@ struct BRows {
   }
 };
 
+// Neighbour access for rod pairs: slot indices at or past `count` continue in
+// the partner's first slots (left half), indices below zero in the partner's
+// last `pcount` slots (right half).
+template <int kCap>
+struct BPair {
+  BRows<kCap> own, peer;
+  int count, pcount;
+  __device__ __forceinline__ double at(int r, int s) const {
+    if (s >= count) return peer.at(r, s - count);
+    if (s < 0) return peer.at(r, s + pcount);
+    return own.at(r, s);
+  }
+  __device__ __forceinline__ D3 get3(int r, int s) const {
+    if (s >= count) return peer.get3(r, s - count);
+    if (s < 0) return peer.get3(r, s + pcount);
+    return own.get3(r, s);
+  }
+};
+
 // parameter field -> shared row (the rows the resident kernel keeps)
 __device__ __forceinline__ int param_row(int f) {
   switch (f) {
@@ -75,7 +103,10 @@ __device__ __forceinline__ int param_row(int f) {
 // from serve[blockIdx.x] (serving launches)
 // kGather: cta_start indexes gmap, the list of the CTA's slots (rods that
 // need not be neighbours in the slot layout)
-template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false>
+// kPair: cluster launch of CTA pairs; with kServe, CTAs 2i and 2i + 1 form a
+// pair when both serve entries say so and run the same step count, and are
+// single CTAs otherwise; without kServe every cluster is a pair
+template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false, bool kPair = false>
 __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
                                                                     int n_steps_launch, const ServeCta* serve,
                                                                     const int32_t* gmap) {
@@ -106,6 +137,43 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
   if (n_steps <= 0) return;
   const int64_t S = a.stride;
+  // partner rows (its own rows for a single CTA) and cluster barriers
+  BPair<kCap> N{R, R, count, count};
+  bool paired = false;
+  if constexpr (kPair) {
+    const unsigned partner = blockIdx.x ^ 1u;
+    if constexpr (kServe) {
+      const ServeCta& sc = serve[blockIdx.x];
+      const ServeCta& o = serve[partner];
+      paired = sc.pair != 0 && o.pair != 0 && sc.steps == o.steps;
+      if (paired) N.pcount = o.count;
+    } else {
+      paired = true;
+      N.pcount = static_cast<int>(cta_start[partner + 1] - cta_start[partner]);
+    }
+    if (paired) {
+      cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+      N.peer.base = cl.map_shared_rank(smem, cl.block_rank() ^ 1u);
+    }
+  }
+  // orders this phase's writes before the next phase's neighbour reads
+  auto sync_neighbours = [&]() {
+    if constexpr (kPair) {
+      if (paired) {
+        cooperative_groups::this_cluster().sync();
+        return;
+      }
+    }
+    __syncthreads();
+  };
+  auto nb3 = [&](int r, int s) -> D3 {
+    if constexpr (kPair) return N.get3(r, s);
+    return R.get3(r, s);
+  };
+  auto nb = [&](int r, int s) -> double {
+    if constexpr (kPair) return N.at(r, s);
+    return R.at(r, s);
+  };
 
   // ---- stage state, parameters and slot metadata (coalesced loads)
   for (int s = tid; s < count; s += kThreads) {
@@ -155,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
       }
     }
-    __syncthreads();
+    sync_neighbours();
 
     // ---- element geometry, internal stress, element-local torque terms
     for (int s = tid; s < count; s += kThreads) {
@@ -166,7 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         double q[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
-        const D3 dx = R.get3(bX, s + 1) - R.get3(bX, s);
+        const D3 dx = nb3(bX, s + 1) - R.get3(bX, s);
         l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
         const double il = 1.0 / l;
         const D3 t = {dx.x * il, dx.y * il, dx.z * il};
@@ -182,7 +250,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         const D3 w = R.get3(bW, s);
         const D3 J = R.get3(bJ, s);
         const D3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
-        const D3 dv = R.get3(bV, s + 1) - R.get3(bV, s);
+        const D3 dv = nb3(bV, s + 1) - R.get3(bV, s);
         const double rate = dot(t, dv) / (e * l0);
         tl = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
       }
@@ -191,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       R.put3(bF, s, f);
       R.put3(bTl, s, tl);
     }
-    __syncthreads();
+    sync_neighbours();
 
     // ---- Voronoi curvature and couple
     for (int s = tid; s < count; s += kThreads) {
@@ -202,11 +270,11 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
           qc[k] = R.at(bQ + k, s);
-          qn[k] = R.at(bQ + k, s + 1);
+          qn[k] = nb(bQ + k, s + 1);
         }
         const double D0 = R.at(bD0, s);
         const D3 kappa = inv_rotate_divide_fast(qc, qn, D0);
-        const double eps = 0.5 * (R.at(bL, s) + R.at(bL, s + 1)) / D0;
+        const double eps = 0.5 * (R.at(bL, s) + nb(bL, s + 1)) / D0;
         const double ic = 1.0 / (eps * eps * eps);
         const D3 dk = kappa - R.get3(bKap0, s);
         const D3 B = R.get3(bBend, s);
@@ -217,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       R.put3(bG, s, gg);
       R.put3(bH, s, hh);
     }
-    __syncthreads();
+    sync_neighbours();
 
     // ---- loads, torques, accelerations, kick, rate constraints
     for (int s = tid; s < count; s += kThreads) {
@@ -226,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       const double m = R.at(bMass, s);
       D3 v = R.get3(bV, s);
       D3 F = R.get3(bF, s);
-      if (!first) F = F - R.get3(bF, s - 1);
+      if (!first) F = F - nb3(bF, s - 1);
       if (kDamped) {
         const double cf = m * R.at(bNuF, s);
         F = {F.x - cf * v.x, F.y - cf * v.y, F.z - cf * v.z};
@@ -242,12 +310,12 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         D3 T = R.get3(bG, s);
         D3 Q2 = R.get3(bH, s);
         if (!first) {
-          T = T - R.get3(bG, s - 1);
-          Q2 = Q2 + R.get3(bH, s - 1);
+          T = T - nb3(bG, s - 1);
+          Q2 = Q2 + nb3(bH, s - 1);
         }
         T = T + scale(Q2, 0.5) + R.get3(bTl, s);
         if (kDamped) {
-          const double ct = 0.5 * (m + R.at(bMass, s + 1)) * R.at(bNuT, s);
+          const double ct = 0.5 * (m + nb(bMass, s + 1)) * R.at(bNuT, s);
           T = {T.x - ct * w.x, T.y - ct * w.y, T.z - ct * w.z};
         }
         if (any_rod && (meta & kLastElem) && (ri->flags & kRodEndTorque)) {
@@ -259,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         const D3 ji = R.get3(bJinv, s);
         w = {w.x + dt * (ji.x * T.x * e), w.y + dt * (ji.y * T.y * e), w.z + dt * (ji.z * T.z * e)};
         if (any_rod && (ri->flags & kRodDamper)) {
-          const double mn = R.at(bMass, s + 1);
+          const double mn = nb(bMass, s + 1);
           double em = 0.5 * (m + mn);
           if (first) em += 0.5 * m;
           if (meta & kLastElem) em += 0.5 * mn;
@@ -290,7 +358,13 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         }
       }
     }
-    __syncthreads();
+    // the next step's drift reads only its own slot; a pair's partner must
+    // not leave (and free its rows) while this CTA still reads them
+    if (step + 1 < n_steps) {
+      __syncthreads();
+    } else {
+      sync_neighbours();
+    }
   }
 
   // ---- final half drift and write-back
@@ -321,18 +395,36 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
 }
 
-template <int kCap, int kThreads, bool kSplit, bool kServe = false, bool kGather = false>
+template <int kCap, int kThreads, bool kSplit, bool kServe = false, bool kGather = false, bool kPair = false>
 cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
   const size_t bytes = size_t(bRows) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
-    return cudaGetLastError();
+    if constexpr (kPair) {
+      // clusters of two CTAs; the grid is a whole number of clusters
+      if (n_ctas % 2 != 0) return cudaErrorInvalidValue;
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3(static_cast<unsigned>(n_ctas));
+      lc.blockDim = dim3(kThreads);
+      lc.dynamicSmemBytes = bytes;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      return cudaLaunchKernelEx(&lc, kern, args, cta_start, n_steps, serve, gmap);
+    } else {
+      kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
+      return cudaGetLastError();
+    }
   };
-  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather>)
-                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather>);
+  return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair>)
+                : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair>);
 }
 
 }  // namespace
@@ -363,11 +455,26 @@ cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start
   }
 }
 
-// Serving launches (see launch_rod_block_mixed_serve): 520-slot CTAs.
+// Serving launches (see launch_rod_block_mixed_serve): 520-slot CTAs in a
+// cluster launch (n_ctas even) in which serve entries 2i and 2i + 1 may hold
+// the two halves of one rod.
 cudaError_t launch_rod_block_fp64_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
                                         bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  return launch_block_cfg<520, 256, true, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+  return launch_block_cfg<520, 256, true, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+}
+
+// Rod pairs on gathered CTAs: CTAs 2i and 2i + 1 own the two halves of one
+// rod (slots gmap[cta_start[c] .. cta_start[c + 1])); config 0: 512 threads,
+// 1: 256 threads per CTA.
+cudaError_t launch_rod_block_fp64_pairs(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                        int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  switch (config) {
+    case 0: return launch_block_cfg<520, 512, true, false, true, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 1: return launch_block_cfg<520, 256, true, false, true, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // Gathered CTAs: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),

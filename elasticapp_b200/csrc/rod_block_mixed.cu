@@ -45,6 +45,11 @@
 // constants) is copied into shared memory once per launch, so the step loop
 // reads global memory only for the clamp target and end torque of the few
 // slots that carry them.
+//
+// Rod pairs (kPair) as in rod_block_fp64.cu: a rod of up to 1039 elements on
+// a cluster of two CTAs, neighbour reads across the split from the partner's
+// shared memory, both per-step barriers cluster barriers.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "eb_internal.h"
@@ -153,9 +158,46 @@ __device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, const R
   }
 }
 
-// FP32 length of element s from its FP64 position difference
+// Neighbour access for rod pairs: slot indices at or past `count` continue in
+// the partner's first slots (left half), indices below zero in the partner's
+// last `pcount` slots (right half).
 template <int kCap>
-__device__ __forceinline__ float element_length(const MRows<kCap>& R, int s) {
+struct MPair {
+  MRows<kCap> own, peer;
+  int count, pcount;
+  __device__ __forceinline__ const MRows<kCap>& rows(int& s) const {
+    if (s >= count) {
+      s -= count;
+      return peer;
+    }
+    if (s < 0) {
+      s += pcount;
+      return peer;
+    }
+    return own;
+  }
+  __device__ __forceinline__ double ad(int r, int s) const {
+    const MRows<kCap>& X = rows(s);
+    return X.ad(r, s);
+  }
+  __device__ __forceinline__ float af(int r, int s) const {
+    const MRows<kCap>& X = rows(s);
+    return X.af(r, s);
+  }
+  __device__ __forceinline__ D3 d3(int r, int s) const {
+    const MRows<kCap>& X = rows(s);
+    return X.d3(r, s);
+  }
+  __device__ __forceinline__ F3 f3(int r, int s) const {
+    const MRows<kCap>& X = rows(s);
+    return X.f3(r, s);
+  }
+};
+
+// FP32 length of element s from its FP64 position difference (Rows: MRows,
+// or MPair for slots that may lie in a pair's partner)
+template <class Rows>
+__device__ __forceinline__ float element_length(const Rows& R, int s) {
   const F3 dxf = tof(R.d3(dX, s + 1) - R.d3(dX, s));
   const float l2 = dot(dxf, dxf);
   return l2 * rsqrtf(l2);
@@ -183,7 +225,8 @@ __device__ __forceinline__ int mixed_param_row(int f) {
 // launch-wide values
 // kGather: cta_start indexes gmap, the list of the CTA's slots (rods that
 // need not be neighbours in the slot layout)
-template <int kCap, int kThreads, int kMinBlocks, bool kDamped, bool kServe, bool kGather = false>
+// kPair: cluster launch of CTA pairs (see rod_block_fp64_kernel)
+template <int kCap, int kThreads, int kMinBlocks, bool kDamped, bool kServe, bool kGather = false, bool kPair = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps_launch, const ServeCta* serve,
                            const int32_t* gmap) {
@@ -215,6 +258,36 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
   if (n_steps <= 0) return;
   const int64_t S = a.stride;
+  // partner rows (its own rows for a single CTA) and cluster barriers
+  MPair<kCap> N{R, R, count, count};
+  bool paired = false;
+  if constexpr (kPair) {
+    const unsigned partner = blockIdx.x ^ 1u;
+    if constexpr (kServe) {
+      const ServeCta& sc = serve[blockIdx.x];
+      const ServeCta& o = serve[partner];
+      paired = sc.pair != 0 && o.pair != 0 && sc.steps == o.steps;
+      if (paired) N.pcount = o.count;
+    } else {
+      paired = true;
+      N.pcount = static_cast<int>(cta_start[partner + 1] - cta_start[partner]);
+    }
+    if (paired) {
+      cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+      N.peer.d = cl.map_shared_rank(R.d, cl.block_rank() ^ 1u);
+      N.peer.f = cl.map_shared_rank(R.f, cl.block_rank() ^ 1u);
+    }
+  }
+  // orders a phase's writes before the next phase's neighbour reads
+  auto sync_neighbours = [&]() {
+    if constexpr (kPair) {
+      if (paired) {
+        cooperative_groups::this_cluster().sync();
+        return;
+      }
+    }
+    __syncthreads();
+  };
 
   // ---- stage state, parameters, reciprocals, FP32 copies and rod data
   const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
@@ -267,7 +340,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     drift(R, s, meta, hdt, R.d3(dV, s), R.d3(dW, s));
     if ((meta & kFirst) && (rflag_s[s] & kRodClamp)) clamp_value(R, s, a.rods[meta >> kRodShift]);
   }
-  __syncthreads();
+  sync_neighbours();
 
   // Two phases per step, one barrier after each.  Phase A: element s (strain,
   // internal load, element-local torque terms) and Voronoi s (curvature and
@@ -283,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       F3 f{0.f, 0.f, 0.f}, p{0.f, 0.f, 0.f}, mm{0.f, 0.f, 0.f};
       float e = 1.f;
       if (meta & kElem) {
-        const D3 dx = R.d3(dX, s + 1) - R.d3(dX, s);
+        const D3 dx = (kPair ? N.d3(dX, s + 1) : R.d3(dX, s + 1)) - R.d3(dX, s);
         double qd[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
@@ -310,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const F3 w = R.f3(fW, s);
         const F3 J = R.f3(fJ, s);
         const F3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
-        const F3 dv = tof(R.d3(dV, s + 1) - R.d3(dV, s));
+        const F3 dv = tof((kPair ? N.d3(dV, s + 1) : R.d3(dV, s + 1)) - R.d3(dV, s));
         const float rate = dot(t, dv) * il;
         p = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
 
@@ -323,7 +396,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           // both forms are free of the cancellation of the original products.
           float dd[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) dd[k] = static_cast<float>(R.ad(dQ + k, s + 1) - R.ad(dQ + k, s));
+          for (int k = 0; k < 9; ++k)
+            dd[k] = static_cast<float>((kPair ? N.ad(dQ + k, s + 1) : R.ad(dQ + k, s + 1)) - R.ad(dQ + k, s));
           float sq = 0.f;
 #pragma unroll
           for (int k = 0; k < 9; ++k) sq += dd[k] * dd[k];
@@ -341,7 +415,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           const F3 skew = {dot(d3, e2) - dot(d2, e3), dot(d1, e3) - dot(d3, e1), dot(d2, e1) - dot(d1, e2)};
           const F3 kappa = scale(skew, st);
           // 1 / eps^3 with eps = D / D0, D the mean length of elements s, s + 1
-          const float ieps = __fdividef(D0, 0.5f * (l + element_length(R, s + 1)));
+          const float ieps =
+              __fdividef(D0, 0.5f * (l + (kPair ? element_length(N, s + 1) : element_length(R, s + 1))));
           const float ic = ieps * ieps * ieps;
           const F3 dk = kappa - R.f3(fKap0, s);
           const F3 B = R.f3(fBend, s);
@@ -360,7 +435,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       R.pf3(fP, s, p);
       R.pf3(fM, s, mm);
     }
-    __syncthreads();
+    sync_neighbours();
 
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
@@ -368,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       const float m = R.af(fMass, s);
       D3 v = R.d3(dV, s);
       F3 F = R.f3(fF, s);
-      if (!first) F = F - R.f3(fF, s - 1);
+      if (!first) F = F - (kPair ? N.f3(fF, s - 1) : R.f3(fF, s - 1));
       if (kDamped) {
         const float cf = m * R.af(fNuF, s);
         const F3 vf = tof(v);
@@ -384,9 +459,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const float e = R.af(fE, s);
         w = R.d3(dW, s);
         F3 T = R.f3(fP, s);
-        if (!first) T = T - R.f3(fM, s - 1);
+        if (!first) T = T - (kPair ? N.f3(fM, s - 1) : R.f3(fM, s - 1));
         if (kDamped) {
-          const float ct = 0.5f * (m + R.af(fMass, s + 1)) * R.af(fNuT, s);
+          const float ct = 0.5f * (m + (kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1))) * R.af(fNuT, s);
           const F3 wf = R.f3(fW, s);
           T = {T.x - ct * wf.x, T.y - ct * wf.y, T.z - ct * wf.z};
         }
@@ -402,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         w = {w.x + dt * static_cast<double>(ji.x * T.x * e), w.y + dt * static_cast<double>(ji.y * T.y * e),
              w.z + dt * static_cast<double>(ji.z * T.z * e)};
         if (rf & kRodDamper) {
-          const float mn = R.af(fMass, s + 1);
+          const float mn = kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1);
           float em = 0.5f * (m + mn);
           if (first) em += 0.5f * m;
           if (meta & kLastElem) em += 0.5f * mn;
@@ -434,11 +509,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         }
       }
     }
-    __syncthreads();
+    sync_neighbours();
   }
 }
 
-template <int kCap, int kThreads, int kMinBlocks, bool kServe = false, bool kGather = false>
+template <int kCap, int kThreads, int kMinBlocks, bool kServe = false, bool kGather = false, bool kPair = false>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
   const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(fRowsF) * kCap * sizeof(float) +
@@ -446,11 +521,29 @@ cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
-    kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
-    return cudaGetLastError();
+    if constexpr (kPair) {
+      // clusters of two CTAs; the grid is a whole number of clusters
+      if (n_ctas % 2 != 0) return cudaErrorInvalidValue;
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3(static_cast<unsigned>(n_ctas));
+      lc.blockDim = dim3(kThreads);
+      lc.dynamicSmemBytes = bytes;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      return cudaLaunchKernelEx(&lc, kern, args, cta_start, n_steps, serve, gmap);
+    } else {
+      kern<<<n_ctas, kThreads, bytes, stream>>>(args, cta_start, n_steps, serve, gmap);
+      return cudaGetLastError();
+    }
   };
-  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true, kServe, kGather>)
-                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false, kServe, kGather>);
+  return damped ? go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, true, kServe, kGather, kPair>)
+                : go(rod_block_mixed_kernel<kCap, kThreads, kMinBlocks, false, kServe, kGather, kPair>);
 }
 
 }  // namespace
@@ -472,10 +565,24 @@ cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_star
 
 // Serving launches: CTA c runs serve[c] (its request's slot range, time step,
 // environment and min(n_steps, serve[c].steps) steps); 520-slot CTAs.
+// A cluster launch (n_ctas even) in which entries 2i and 2i + 1 may hold the
+// two halves of one rod (ServeCta::pair).  Every serving launch takes this
+// form, so a request's arithmetic is the same whatever it is served with.
 cudaError_t launch_rod_block_mixed_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
                                          bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  return launch_mixed_cfg<520, 256, 1, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+  return launch_mixed_cfg<520, 256, 1, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+}
+
+// Rod pairs on gathered CTAs (see launch_rod_block_fp64_pairs).
+cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
+                                         int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
+  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
+  switch (config) {
+    case 0: return launch_mixed_cfg<520, 512, 1, false, true, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 1: return launch_mixed_cfg<520, 256, 1, false, true, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // Gathered CTAs: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),

@@ -4,13 +4,16 @@
 // and damper options) arrive at any time.  The server owns a device pool of
 // bins, each 520 slots (one CTA of the resident step kernels), sized from an
 // HBM budget at creation.  A request is admitted when enough bins are free:
-// its rods are packed into its own bins (next fit), initialised on the host
-// and copied in, and its initial energy is computed on the device.  Every
-// tick is one launch of the resident kernel per precision (mixed, and FP64
-// for requests that fell back) over the bins of every active request: each
-// CTA reads its bin, step count, time step and environment from a per-CTA
-// table, so requests of different sizes, time steps and horizons share the
-// launch.  A request advances steps_per_launch steps per tick, counted from
+// its rods are packed into its own bins (next fit; a rod of 520 to 1039
+// elements takes a pair of adjacent bins, run by a cluster of two CTAs),
+// initialised on the host and copied in, and its initial energy is computed
+// on the device.  Every tick is one launch of the resident kernel per
+// precision (mixed, and FP64 for requests that fell back) over the bins of
+// every active request: each CTA reads its bin, step count, time step and
+// environment from a per-CTA table, so requests of different sizes, time
+// steps and horizons share the launch.  The launch is always a cluster
+// launch, pairs and single bins alike, so a request's arithmetic does not
+// depend on whether long rods run beside it.  A request advances steps_per_launch steps per tick, counted from
 // its own admission, so its result does not depend on what else is running.
 //
 // Retirement needs no host round trip: the host knows from the step counts
@@ -30,6 +33,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <set>
 #include <memory>
 #include <string>
 #include <vector>
@@ -51,6 +55,7 @@ cudaError_t launch_rod_energy_list(int64_t n_rods, int64_t stride, const int64_t
 namespace {
 
 constexpr int64_t kBin = 520;                 // slots per bin (one CTA)
+constexpr int64_t kPairSlots = 2 * kBin;      // a rod longer than a bin: two adjacent bins (a CTA pair)
 constexpr int64_t kRodsPerBin = kBin / 3;     // a rod takes at least 3 slots
 constexpr size_t kArenaBytes = size_t(1) << 30;  // pinned result arena
 using Clock = std::chrono::steady_clock;
@@ -96,6 +101,50 @@ struct RangeAlloc {
         pv->second += it->second;
         free_.erase(it);
       }
+    }
+  }
+};
+
+// Bins and bin pairs: a pair is bins 2k and 2k + 1 (adjacent slot ranges).
+// Free bins are kept as whole free pairs and as single bins whose buddy is in
+// use; a single comes from the latter when there is one, else by splitting a
+// pair, and a released bin rejoins its buddy when that is free.
+struct BinPool {
+  std::set<int64_t> pairs;   // even b with b and b + 1 free
+  std::set<int64_t> halves;  // free b whose buddy is in use
+  void init(int64_t n_bins) {
+    pairs.clear();
+    halves.clear();
+    for (int64_t b = 0; b + 1 < n_bins; b += 2) pairs.insert(b);
+  }
+  int64_t free_bins() const { return static_cast<int64_t>(halves.size() + 2 * pairs.size()); }
+  bool fits(int64_t n_pairs, int64_t n_singles) const {
+    const int64_t p = static_cast<int64_t>(pairs.size());
+    return n_pairs <= p && n_singles <= static_cast<int64_t>(halves.size()) + 2 * (p - n_pairs);
+  }
+  int64_t take_pair() {
+    const int64_t b = *pairs.begin();
+    pairs.erase(pairs.begin());
+    return b;
+  }
+  int64_t take_single() {
+    if (!halves.empty()) {
+      const int64_t b = *halves.begin();
+      halves.erase(halves.begin());
+      return b;
+    }
+    const int64_t b = take_pair();
+    halves.insert(b + 1);
+    return b;
+  }
+  void give_pair(int64_t b) { pairs.insert(b); }
+  void give_single(int64_t b) {
+    auto it = halves.find(b ^ 1);
+    if (it != halves.end()) {
+      halves.erase(it);
+      pairs.insert(b & ~int64_t(1));
+    } else {
+      halves.insert(b);
     }
   }
 };
@@ -146,9 +195,10 @@ struct Request {
   Clock::time_point t_submit;
   double latency_s = 0.0;
   ReqState state = kQueued;
-  // placement
-  std::vector<int64_t> bins;
-  std::vector<int32_t> bin_count;
+  // placement: units of one bin, or of a bin pair holding one long rod
+  std::vector<int64_t> bins;        // first bin of each unit
+  std::vector<int32_t> bin_count;   // slots used in each unit
+  std::vector<uint8_t> bin_pair;    // 1: the unit is a bin pair
   std::vector<int64_t> rod_bin, rod_off;  // bin and slot offset inside it, per rod
   int64_t rod0 = -1;
   int64_t elements = 0;
@@ -183,7 +233,7 @@ struct eb_server {
   int cur = 0;
   int64_t ticks = 0;
   Ring arena;
-  std::vector<int64_t> free_bins;
+  BinPool bins;
   RangeAlloc rod_ids;
   int64_t next_id = 1;
   std::map<int64_t, std::unique_ptr<Request>> requests;
@@ -216,24 +266,41 @@ void server_free(eb_server* s) {
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
-// next-fit packing of the request's rods into bins
+// Placement units of the request: each rod longer than a bin on its own bin
+// pair, the others packed next-fit into single bins.
 void pack(Request& r) {
   r.bins.clear();
   r.bin_count.clear();
+  r.bin_pair.clear();
   r.rod_bin.assign(r.rods.size(), 0);
   r.rod_off.assign(r.rods.size(), 0);
-  int64_t used = kBin;
+  int64_t used = kBin, open = -1;
   for (size_t k = 0; k < r.rods.size(); ++k) {
     const int64_t w = r.rods[k].n_elements + 1;
-    if (used + w > kBin) {
+    if (w > kBin) {
+      r.rod_bin[k] = static_cast<int64_t>(r.bin_count.size());
+      r.rod_off[k] = 0;
+      r.bin_count.push_back(static_cast<int32_t>(w));
+      r.bin_pair.push_back(1);
+      continue;
+    }
+    if (open < 0 || used + w > kBin) {
+      open = static_cast<int64_t>(r.bin_count.size());
       r.bin_count.push_back(0);
+      r.bin_pair.push_back(0);
       used = 0;
     }
-    r.rod_bin[k] = static_cast<int64_t>(r.bin_count.size()) - 1;
+    r.rod_bin[k] = open;
     r.rod_off[k] = used;
     used += w;
-    r.bin_count.back() = static_cast<int32_t>(used);
+    r.bin_count[open] = static_cast<int32_t>(used);
   }
+}
+
+void unit_counts(const Request& r, int64_t* n_pairs, int64_t* n_singles) {
+  *n_pairs = 0;
+  for (uint8_t p : r.bin_pair) *n_pairs += p;
+  *n_singles = static_cast<int64_t>(r.bin_pair.size()) - *n_pairs;
 }
 
 uint32_t request_flags(const Request& r) {
@@ -323,15 +390,17 @@ eb_status admit(eb_server* s) {
   while (!s->queue.empty()) {
     Request& r = *s->queue.front();
     pack(r);
-    if (static_cast<int64_t>(r.bin_count.size()) > static_cast<int64_t>(s->free_bins.size())) break;
+    int64_t n_pairs = 0, n_singles = 0;
+    unit_counts(r, &n_pairs, &n_singles);
+    if (!s->bins.fits(n_pairs, n_singles)) break;
     const int64_t rid = s->rod_ids.alloc(static_cast<int64_t>(r.rods.size()));
     if (rid < 0) break;
     r.rod0 = rid;
-    r.bins.clear();
-    for (size_t b = 0; b < r.bin_count.size(); ++b) {
-      r.bins.push_back(s->free_bins.back());
-      s->free_bins.pop_back();
-    }
+    r.bins.assign(r.bin_count.size(), -1);
+    for (size_t b = 0; b < r.bin_count.size(); ++b)  // pairs first, so singles do not split them
+      if (r.bin_pair[b]) r.bins[b] = s->bins.take_pair();
+    for (size_t b = 0; b < r.bin_count.size(); ++b)
+      if (!r.bin_pair[b]) r.bins[b] = s->bins.take_single();
     r.steps_done = 0;
     r.damped = false;
     if (eb_status e = place(s, r)) return e;
@@ -378,7 +447,12 @@ eb_status retire(eb_server* s, Request& r) {
   SV_CUDA(cudaEventRecord(r.event, s->stream));
   // bins and rod ids go back at once: the copies above run before any later
   // use of them on this stream
-  for (int64_t b : r.bins) s->free_bins.push_back(b);
+  for (size_t b = 0; b < r.bins.size(); ++b) {
+    if (r.bin_pair[b])
+      s->bins.give_pair(r.bins[b]);
+    else
+      s->bins.give_single(r.bins[b]);
+  }
   s->rod_ids.release(r.rod0, nr);
   r.state = kFinishing;
   s->finishing.push_back(&r);
@@ -499,8 +573,8 @@ EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** ou
                          kBin * sizeof(uint32_t) +
                          kRodsPerBin * (sizeof(eb::RodInfo) + 10 * sizeof(double) + sizeof(int64_t) + sizeof(int32_t)) +
                          4 * sizeof(eb::ServeCta);
-  const int64_t n_bins = static_cast<int64_t>(cfg.hbm_budget_bytes / per_bin);
-  if (n_bins < 1) return fail(EB_ERR_INVALID_ARGUMENT, "HBM budget holds no bin");
+  const int64_t n_bins = static_cast<int64_t>(cfg.hbm_budget_bytes / per_bin) / 2 * 2;  // whole bin pairs
+  if (n_bins < 2) return fail(EB_ERR_INVALID_ARGUMENT, "HBM budget holds no bin pair");
   if (n_bins * kRodsPerBin >= (int64_t(1) << (32 - eb::kRodShift)))
     return fail(EB_ERR_UNSUPPORTED, "HBM budget too large for the rod id field");
   auto s = std::make_unique<eb_server>();
@@ -528,10 +602,11 @@ EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** ou
   alloc(&s->status, sizeof(uint32_t));
   for (int a = 0; a < 2; ++a)
     for (int b = 0; b < 2; ++b) {
-      alloc(&s->d_cta[a][b], static_cast<size_t>(n_bins) * sizeof(eb::ServeCta));
+      // one entry per bin, plus the padding entry of an odd count
+      alloc(&s->d_cta[a][b], static_cast<size_t>(n_bins + 2) * sizeof(eb::ServeCta));
       if (e == cudaSuccess)
         e = cudaHostAlloc(reinterpret_cast<void**>(&s->h_cta[a][b]),
-                          static_cast<size_t>(n_bins) * sizeof(eb::ServeCta), cudaHostAllocDefault);
+                          static_cast<size_t>(n_bins + 2) * sizeof(eb::ServeCta), cudaHostAllocDefault);
     }
   if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&s->arena.base), kArenaBytes, cudaHostAllocDefault);
   for (auto& ev : s->tick_event)
@@ -543,8 +618,7 @@ EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** ou
     return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA, msg);
   }
   s->arena.cap = kArenaBytes;
-  s->free_bins.reserve(static_cast<size_t>(n_bins));
-  for (int64_t b = n_bins - 1; b >= 0; --b) s->free_bins.push_back(b);
+  s->bins.init(n_bins);
   s->rod_ids.init(s->rod_cap);
   *out = s.release();
   return EB_OK;
@@ -568,22 +642,20 @@ EB_API eb_status eb_server_submit(eb_server* s, const eb_request* req, int64_t* 
   r->rods.assign(req->rods, req->rods + req->n_rods);
   for (const auto& p : r->rods) {
     eb::HostRodData check;  // the reference initializer's argument checks
-    if (p.n_elements >= 2 && p.n_elements + 1 <= kBin)
+    if (p.n_elements >= 2 && p.n_elements + 1 <= kPairSlots)
       if (eb_status st = eb::host_straight_rod(p, check)) return st;
   }
-  int64_t bins_needed = 0, used = kBin;
   for (const auto& p : r->rods) {
     if (p.n_elements < 2) return fail(EB_ERR_INVALID_ARGUMENT, "a rod needs at least 2 elements");
-    if (p.n_elements + 1 > kBin)
-      return fail(EB_ERR_UNSUPPORTED, "served rods hold at most " + std::to_string(kBin - 1) + " elements");
+    if (p.n_elements + 1 > kPairSlots)
+      return fail(EB_ERR_UNSUPPORTED, "served rods hold at most " + std::to_string(kPairSlots - 1) + " elements");
     r->elements += p.n_elements;
-    if (used + p.n_elements + 1 > kBin) {
-      ++bins_needed;
-      used = 0;
-    }
-    used += p.n_elements + 1;
   }
-  if (bins_needed > s->n_bins) return fail(EB_ERR_OUT_OF_MEMORY, "request larger than the server's HBM budget");
+  pack(*r);
+  int64_t n_pairs = 0, n_singles = 0;
+  unit_counts(*r, &n_pairs, &n_singles);
+  if (2 * n_pairs + n_singles > s->n_bins)
+    return fail(EB_ERR_OUT_OF_MEMORY, "request larger than the server's HBM budget");
   if (req->velocities) {
     int64_t total = 0;
     for (const auto& p : r->rods) total += 3 * (p.n_elements + 1);
@@ -619,22 +691,35 @@ EB_API eb_status eb_server_tick(eb_server* s, int64_t* in_flight) {
   const int K = s->cfg.steps_per_launch;
   int n_cta[2] = {0, 0};
   bool damped[2] = {false, false};
-  for (Request* r : s->active) {
-    const int p = r->precision == EB_PRECISION_MIXED ? 0 : 1;
-    const int32_t steps = static_cast<int32_t>(std::min<int64_t>(K, r->n_steps - r->steps_done));
-    for (size_t b = 0; b < r->bins.size(); ++b) {
-      eb::ServeCta& c = s->h_cta[parity][p][n_cta[p]++];
-      c.start = r->bins[b] * kBin;
-      c.count = r->bin_count[b];
-      c.steps = steps;
-      c.dt = r->dt;
-      c.half_dt = 0.5 * r->dt;
-      for (int d = 0; d < 3; ++d) c.gravity[d] = r->gravity[d];
-      c.flags = request_flags(*r);
-      c.pad = 0;
+  // CTA tables: the two halves of each pair unit first (entries 2i, 2i + 1
+  // form a cluster), then single bins, padded to an even count
+  for (int pass = 0; pass < 2; ++pass)
+    for (Request* r : s->active) {
+      const int p = r->precision == EB_PRECISION_MIXED ? 0 : 1;
+      const int32_t steps = static_cast<int32_t>(std::min<int64_t>(K, r->n_steps - r->steps_done));
+      for (size_t b = 0; b < r->bins.size(); ++b) {
+        if ((pass == 0) != (r->bin_pair[b] != 0)) continue;
+        const int halves = r->bin_pair[b] ? 2 : 1;
+        const int32_t W = r->bin_count[b], h = (W + 1) / 2;
+        for (int k = 0; k < halves; ++k) {
+          eb::ServeCta& c = s->h_cta[parity][p][n_cta[p]++];
+          c.start = r->bins[b] * kBin + (k == 1 ? h : 0);
+          c.count = halves == 1 ? W : (k == 0 ? h : W - h);
+          c.steps = steps;
+          c.dt = r->dt;
+          c.half_dt = 0.5 * r->dt;
+          for (int d = 0; d < 3; ++d) c.gravity[d] = r->gravity[d];
+          c.flags = request_flags(*r);
+          c.pair = halves == 2 ? 1u : 0u;
+        }
+      }
+      damped[p] = damped[p] || r->damped;
     }
-    damped[p] = damped[p] || r->damped;
-  }
+  for (int p = 0; p < 2; ++p)
+    if (n_cta[p] % 2) {
+      eb::ServeCta& c = s->h_cta[parity][p][n_cta[p]++];
+      std::memset(&c, 0, sizeof(c));  // no slots, no steps: returns at once
+    }
   if (n_cta[0] + n_cta[1] > 0) {
     eb::StepArgs a{};
     a.stride = s->stride;
@@ -732,7 +817,7 @@ EB_API eb_status eb_server_get_stats(const eb_server* s, eb_server_stats* out) {
   out->completed = s->n_completed;
   out->fallbacks = s->n_fallbacks;
   out->bins_total = s->n_bins;
-  out->bins_used = s->n_bins - static_cast<int64_t>(s->free_bins.size());
+  out->bins_used = s->n_bins - s->bins.free_bins();
   out->ticks = s->ticks;
   out->element_steps = s->element_steps;
   return EB_OK;

@@ -83,11 +83,12 @@ typedef enum eb_precision {
                                            kernel launches */
 #define EB_FLAG_STEP_BUCKETED 0x20u    /* always use the per-size-bucket
                                            resident plan (rods of at most 263
-                                           elements and rods of 264 to 519 in
-                                           separate launches, each with its
-                                           fastest configuration) when the
-                                           batch has rods of both sizes and
-                                           none longer */
+                                           elements, of 264 to 519 and of 520
+                                           to 1039 in separate launches, each
+                                           with its fastest configuration)
+                                           when the batch has rods of two
+                                           sizes, or rods of 520 to 1039
+                                           elements, and none longer */
 
 typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
@@ -313,10 +314,13 @@ EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
 
 /* The step plan chosen by the first eb_step: mode 1 = streaming kernel,
  * 2 = resident kernel with block configuration `config`, 3 = resident kernel
- * per size bucket (rods of at most 263 elements with configuration config % 4,
- * rods of 264 to 519 with config / 4, one launch each); probe_ms[0] is the
- * streaming probe time, probe_ms[1 + c] configuration c's on the whole batch,
- * probe_ms[5 + 4 b + c] configuration c's on bucket b alone (up to count). */
+ * per size bucket, one launch per bucket that holds rods: bucket 0 (rods of
+ * at most 263 elements) with configuration config % 4, bucket 1 (264 to 519)
+ * with (config / 4) % 4, bucket 2 (520 to 1039 elements, each rod on a
+ * cluster of two CTAs) with config / 16 (0: 512, 1: 256 threads per CTA).
+ * probe_ms[0] is the streaming probe time, probe_ms[1 + c] configuration c's
+ * on the whole batch, probe_ms[5 + 4 b + c] configuration c's on bucket b
+ * alone (up to count entries; untimed entries are 0). */
 EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* config, float* probe_ms,
                               int32_t count);
 

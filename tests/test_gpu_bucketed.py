@@ -33,7 +33,7 @@ def test_bucketed_plan_matches_oracle_and_resident_plan():
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, 300)
     plan = sim.step_plan()
     assert plan["mode"] == "bucketed"
-    c_short, c_long = plan["config"] % 4, plan["config"] // 4
+    c_short, c_long = plan["config"] % 4, (plan["config"] // 4) % 4
     assert plan["probe_ms"][5 + c_short] > 0.0 and plan["probe_ms"][9 + c_long] > 0.0
     assert c_long in (0, 1)  # the long bucket needs the 520-slot configurations
     # the oracle's FP64 parity bounds
@@ -79,9 +79,10 @@ def test_bucketed_mixed_precision_tip_error():
     assert np.all(np.isfinite(err)) and err.max() <= TIP_TOL, err.max()
 
 
-@pytest.mark.parametrize("n_range,mode", [((8, 200), ("resident", "streaming")), ((300, 700), ("streaming",))])
+@pytest.mark.parametrize("n_range,mode", [((8, 200), ("resident", "streaming")), ((900, 1200), ("streaming",))])
 def test_bucketed_flag_falls_back_when_plan_does_not_apply(n_range, mode):
-    # one bucket only, or rods longer than 519 elements: the usual plan
+    # one bucket of single-CTA rods only, or rods longer than 1039 elements:
+    # the usual plan
     wl = W.uneven_batch(n_rods=4, seed=3, n_range=n_range)
     sim = wl.build(step_mode="bucketed")
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, 4)

@@ -52,7 +52,8 @@ def test_mixed_with_damper_clamp_gravity_short_run():
 
 
 def test_mixed_rods_too_long_fall_back_to_fp64_streaming():
-    wl = W.uneven_batch(n_rods=3, seed=5, n_range=(600, 700))
+    # longer than a CTA pair holds (1039 elements)
+    wl = W.uneven_batch(n_rods=3, seed=5, n_range=(1100, 1200))
     sim = wl.build(precision="mixed")
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, 4)
     assert sim.step_plan()["mode"] == "streaming"

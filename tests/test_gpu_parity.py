@@ -208,10 +208,11 @@ def test_tile_and_rod_boundaries(lengths):
     assert within(errs, bounds), (errs, bounds)
     _, _, errs, bounds = _run_pair(wl, 200, reference_rounding=True, window=256)
     assert within(errs, bounds), (errs, bounds)
-    # resident kernel where every rod fits (falls back to streaming otherwise)
+    # resident kernel where every rod fits one CTA; rods of 520 to 1039
+    # elements run on CTA pairs in the per-size-bucket plan
     sim, _, errs, bounds = _run_pair(wl, 200, step_mode="resident")
     assert within(errs, bounds), (errs, bounds)
-    assert sim.step_plan()["mode"] == ("resident" if max(lengths) + 1 <= 520 else "streaming")
+    assert sim.step_plan()["mode"] == ("resident" if max(lengths) + 1 <= 520 else "bucketed")
 
 
 def test_energy_matches_oracle():

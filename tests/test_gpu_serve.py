@@ -136,7 +136,7 @@ def test_serve_error_paths(eb):
         srv.submit(rods, -1.0, 10)
     with pytest.raises(EbError):
         srv.submit(rods, dt, 0)
-    long_rod = eb.StraightRod(n_elements=600, material=eb.Material(1000.0, 1e6, 1e6 / 3), radius=0.01, length=1.0)
+    long_rod = eb.StraightRod(n_elements=1040, material=eb.Material(1000.0, 1e6, 1e6 / 3), radius=0.01, length=1.0)
     with pytest.raises(EbError):
         srv.submit([long_rod], dt, 10)
     srv.close()
