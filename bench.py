@@ -377,7 +377,9 @@ def _serve_request(eb, W, rng):
 
 def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
     """Poisson arrivals at `rate` requests/s for `seconds`, then up to
-    `drain_s` more seconds; latency = completion seen - scheduled arrival."""
+    `drain_s` more seconds; latency = completion seen - scheduled arrival.
+    The requests are generated before the clock starts (building them is the
+    client's work, not the server's)."""
     from elasticapp_b200.server import Server
 
     srv = Server(precision="mixed", hbm_budget_bytes=budget)
@@ -388,14 +390,16 @@ def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
         if t >= seconds:
             break
         arrivals.append(t)
+    requests = [_serve_request(eb, W, np.random.Generator(np.random.PCG64(seed * 1000003 + i)))
+                for i in range(len(arrivals))]
     arrival_of, lat, work = {}, [], 0.0
     nxt = 0
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         while nxt < len(arrivals) and arrivals[nxt] <= now:
-            rng = np.random.Generator(np.random.PCG64(seed * 1000003 + nxt))
-            rods, vel, dt, steps, elems = _serve_request(eb, W, rng)
+            rods, vel, dt, steps, elems = requests[nxt]
+            requests[nxt] = None
             rid = srv.submit(rods, dt, steps, gravity=(0.0, 0.0, -9.81), clamp=True, damper=(0.1, 0.1),
                              velocities=vel)
             arrival_of[rid] = arrivals[nxt]
@@ -420,7 +424,9 @@ def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
             "p99_latency_s": float(np.nanpercentile(lat, 99)), "elapsed_s": elapsed,
             "value": st["element_steps"] / elapsed, "unit": UNIT,
             "offered_element_steps_per_s": work / max(seconds, 1e-9), "ticks": int(st["ticks"]),
-            "bins_total": int(st["bins_total"])}
+            "bins_total": int(st["bins_total"]), "kernel_seconds": st["kernel_seconds"],
+            "gpu_busy_frac": st["kernel_seconds"] / elapsed,
+            "kernel_element_steps_per_s": st["element_steps"] / max(st["kernel_seconds"], 1e-9)}
 
 
 def serving_section(eb, W, args, capacity_hint):

@@ -105,7 +105,7 @@ class EbCompletion(ctypes.Structure):
 class EbServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("queued", "active", "finishing", "completed", "fallbacks",
                                                "bins_total", "bins_used", "ticks")] + \
-               [("element_steps", ctypes.c_double)]
+               [("element_steps", ctypes.c_double), ("kernel_seconds", ctypes.c_double)]
 
 
 EB_SERVER_FORCE_FALLBACK = 0x1

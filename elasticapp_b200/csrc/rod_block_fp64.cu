@@ -461,7 +461,7 @@ cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start
 cudaError_t launch_rod_block_fp64_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
                                         bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  return launch_block_cfg<520, 256, true, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+  return launch_block_cfg<520, 512, true, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
 }
 
 // Rod pairs on gathered CTAs: CTAs 2i and 2i + 1 own the two halves of one

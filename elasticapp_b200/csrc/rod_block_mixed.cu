@@ -571,7 +571,7 @@ cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_star
 cudaError_t launch_rod_block_mixed_serve(const StepArgs& args, const ServeCta* serve, int n_ctas, int n_steps,
                                          bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  return launch_mixed_cfg<520, 256, 1, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
+  return launch_mixed_cfg<520, 512, 1, true, false, true>(args, nullptr, n_ctas, n_steps, damped, stream, serve);
 }
 
 // Rod pairs on gathered CTAs (see launch_rod_block_fp64_pairs).

@@ -58,6 +58,7 @@ constexpr int64_t kBin = 520;                 // slots per bin (one CTA)
 constexpr int64_t kPairSlots = 2 * kBin;      // a rod longer than a bin: two adjacent bins (a CTA pair)
 constexpr int64_t kRodsPerBin = kBin / 3;     // a rod takes at least 3 slots
 constexpr size_t kArenaBytes = size_t(1) << 30;  // pinned result arena
+constexpr size_t kUploadBytes = size_t(1) << 28;  // pinned staging of admitted requests' initial data
 using Clock = std::chrono::steady_clock;
 
 eb_status fail(eb_status st, const std::string& m) {
@@ -230,9 +231,18 @@ struct eb_server {
   eb::ServeCta* h_cta[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   cudaEvent_t tick_event[2] = {nullptr, nullptr};
   bool tick_pending[2] = {false, false};
+  // timing of each parity's step launches, summed when the tick is done
+  cudaEvent_t launch_t0[2] = {nullptr, nullptr}, launch_t1[2] = {nullptr, nullptr};
+  bool launch_timed[2] = {false, false};
+  double kernel_seconds = 0.0;
   int cur = 0;
   int64_t ticks = 0;
   Ring arena;
+  // pinned staging of initial data: copies from pageable memory would wait
+  // for the stream (the running ticks) before each admission
+  Ring upload;
+  std::deque<cudaEvent_t> upload_events;  // one per live upload allocation, in order
+  std::vector<cudaEvent_t> spare_events;
   BinPool bins;
   RangeAlloc rod_ids;
   int64_t next_id = 1;
@@ -262,38 +272,53 @@ void server_free(eb_server* s) {
     if (kv.second->event) cudaEventDestroy(kv.second->event);
   for (auto& e : s->tick_event)
     if (e) cudaEventDestroy(e);
+  for (int p = 0; p < 2; ++p) {
+    if (s->launch_t0[p]) cudaEventDestroy(s->launch_t0[p]);
+    if (s->launch_t1[p]) cudaEventDestroy(s->launch_t1[p]);
+  }
   if (s->arena.base) cudaFreeHost(s->arena.base);
+  if (s->upload.base) cudaFreeHost(s->upload.base);
+  for (cudaEvent_t e : s->upload_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : s->spare_events) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
-// Placement units of the request: each rod longer than a bin on its own bin
-// pair, the others packed next-fit into single bins.
+// Placement units of the request, best fit decreasing: rods in order of
+// decreasing length; a rod longer than a bin opens a bin pair (1040 slots,
+// run by a CTA pair, which may split any rod of the unit); a shorter rod goes
+// to the unit with the least room that still holds it, else opens a single
+// bin.
 void pack(Request& r) {
   r.bins.clear();
   r.bin_count.clear();
   r.bin_pair.clear();
   r.rod_bin.assign(r.rods.size(), 0);
   r.rod_off.assign(r.rods.size(), 0);
-  int64_t used = kBin, open = -1;
-  for (size_t k = 0; k < r.rods.size(); ++k) {
+  std::vector<size_t> order(r.rods.size());
+  for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t a, size_t b) { return r.rods[a].n_elements > r.rods[b].n_elements; });
+  std::multimap<int64_t, int64_t> room;  // free slots -> unit
+  for (size_t k : order) {
     const int64_t w = r.rods[k].n_elements + 1;
-    if (w > kBin) {
-      r.rod_bin[k] = static_cast<int64_t>(r.bin_count.size());
-      r.rod_off[k] = 0;
-      r.bin_count.push_back(static_cast<int32_t>(w));
-      r.bin_pair.push_back(1);
-      continue;
+    int64_t u = -1;
+    if (w <= kBin) {
+      auto it = room.lower_bound(w);
+      if (it != room.end()) {
+        u = it->second;
+        room.erase(it);
+      }
     }
-    if (open < 0 || used + w > kBin) {
-      open = static_cast<int64_t>(r.bin_count.size());
+    if (u < 0) {
+      u = static_cast<int64_t>(r.bin_count.size());
       r.bin_count.push_back(0);
-      r.bin_pair.push_back(0);
-      used = 0;
+      r.bin_pair.push_back(w > kBin ? 1 : 0);
     }
-    r.rod_bin[k] = open;
-    r.rod_off[k] = used;
-    used += w;
-    r.bin_count[open] = static_cast<int32_t>(used);
+    r.rod_bin[k] = u;
+    r.rod_off[k] = r.bin_count[u];
+    r.bin_count[u] += static_cast<int32_t>(w);
+    const int64_t left = (r.bin_pair[u] ? kPairSlots : kBin) - r.bin_count[u];
+    if (left >= 3) room.emplace(left, u);  // a rod takes at least 3 slots
   }
 }
 
@@ -311,30 +336,94 @@ uint32_t request_flags(const Request& r) {
   return f;
 }
 
-// Copy the request's initial rods into its bins and compute its initial energy.
+// Space in the pinned staging ring: take back the staging of uploads that
+// have landed, and wait for the oldest one while the ring is full.
+eb_status upload_alloc(eb_server* s, size_t bytes, size_t* off) {
+  auto take_oldest = [&]() {
+    s->spare_events.push_back(s->upload_events.front());
+    s->upload_events.pop_front();
+    s->upload.free_oldest();
+  };
+  while (!s->upload_events.empty()) {
+    const cudaError_t q = cudaEventQuery(s->upload_events.front());
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return fail(EB_ERR_CUDA, std::string("upload event: ") + cudaGetErrorString(q));
+    take_oldest();
+  }
+  while (!s->upload.alloc(bytes, off)) {
+    if (s->upload_events.empty())
+      return fail(EB_ERR_OUT_OF_MEMORY, "request's initial data larger than the staging buffer");
+    SV_CUDA(cudaEventSynchronize(s->upload_events.front()));
+    take_oldest();
+  }
+  return EB_OK;
+}
+
+// Copy the request's initial rods into its bins (through pinned staging, so
+// the copies queue behind the running ticks instead of waiting for them) and
+// compute its initial energy.
 eb_status place(eb_server* s, Request& r) {
   const int64_t S = s->stride;
-  std::vector<std::vector<double>> st(r.bin_count.size()), pr(r.bin_count.size());
-  std::vector<std::vector<uint32_t>> mt(r.bin_count.size());
-  for (size_t b = 0; b < r.bin_count.size(); ++b) {
-    const int64_t c = r.bin_count[b];
-    st[b].assign(static_cast<size_t>(eb::kStateFields * c), 0.0);
-    pr[b].assign(static_cast<size_t>(eb::kParamFields * c), 0.0);
-    mt[b].assign(static_cast<size_t>(c), 0u);
+  const size_t nu = r.bin_count.size(), nr = r.rods.size();
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  std::vector<size_t> ust(nu), upr(nu), umt(nu);
+  size_t bytes = 0;
+  for (size_t b = 0; b < nu; ++b) {
+    const size_t c = static_cast<size_t>(r.bin_count[b]);
+    ust[b] = bytes;
+    bytes += up(c * eb::kStateFields * sizeof(double));
+    upr[b] = bytes;
+    bytes += up(c * eb::kParamFields * sizeof(double));
+    umt[b] = bytes;
+    bytes += up(c * sizeof(uint32_t));
   }
-  std::vector<eb::RodInfo> info(r.rods.size());
-  std::vector<int64_t> rstart(r.rods.size());
-  std::vector<int32_t> rn(r.rods.size());
+  const size_t uinfo = bytes;
+  bytes += up(nr * sizeof(eb::RodInfo));
+  const size_t ustart = bytes;
+  bytes += up(nr * sizeof(int64_t));
+  const size_t un = bytes;
+  bytes += up(nr * sizeof(int32_t));
+  size_t base_off = 0;
+  if (eb_status st = upload_alloc(s, bytes, &base_off)) return st;
+  unsigned char* base = s->upload.base + base_off;
+  std::vector<double*> st(nu), pr(nu);
+  std::vector<uint32_t*> mt(nu);
+  for (size_t b = 0; b < nu; ++b) {
+    st[b] = reinterpret_cast<double*>(base + ust[b]);
+    pr[b] = reinterpret_cast<double*>(base + upr[b]);
+    mt[b] = reinterpret_cast<uint32_t*>(base + umt[b]);
+  }
+  eb::RodInfo* info = reinterpret_cast<eb::RodInfo*>(base + uinfo);
+  int64_t* rstart = reinterpret_cast<int64_t*>(base + ustart);
+  int32_t* rn = reinterpret_cast<int32_t*>(base + un);
+  // the staging space is reused once this event has passed (recorded on
+  // every path, so the ring's allocations and the events stay paired)
+  auto close_upload = [&]() -> eb_status {
+    cudaEvent_t ev = nullptr;
+    if (!s->spare_events.empty()) {
+      ev = s->spare_events.back();
+      s->spare_events.pop_back();
+    } else {
+      SV_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    s->upload_events.push_back(ev);
+    SV_CUDA(cudaEventRecord(ev, s->stream));
+    return EB_OK;
+  };
   size_t voff = 0;
   for (size_t k = 0; k < r.rods.size(); ++k) {
     eb::HostRodData h;
-    if (eb_status e = eb::host_straight_rod(r.rods[k], h)) return e;
+    if (eb_status e = eb::host_straight_rod(r.rods[k], h)) {
+      close_upload();
+      return e;
+    }
     const int64_t n = h.n, W = n + 1, b = r.rod_bin[k], o = r.rod_off[k], c = r.bin_count[b];
     if (!r.velocities.empty()) {
       for (int d = 0; d < 3; ++d)
         for (int64_t j = 0; j <= n; ++j) h.state[(eb::kStV + d) * W + j] = r.velocities[voff + d * W + j];
       voff += static_cast<size_t>(3 * W);
     }
+    // (a unit's rods fill its slots [0, c) without gaps: every staged entry is written)
     for (int f = 0; f < eb::kStateFields; ++f)
       std::memcpy(&st[b][f * c + o], &h.state[f * W], W * sizeof(double));
     for (int f = 0; f < eb::kParamFields; ++f)
@@ -367,17 +456,16 @@ eb_status place(eb_server* s, Request& r) {
   for (size_t b = 0; b < r.bin_count.size(); ++b) {
     const int64_t c = r.bin_count[b], g0 = r.bins[b] * kBin;
     const size_t pitch = static_cast<size_t>(S) * sizeof(double), w = static_cast<size_t>(c) * sizeof(double);
-    SV_CUDA(cudaMemcpy2DAsync(s->state[s->cur] + g0, pitch, st[b].data(), w, w, eb::kStateFields,
+    SV_CUDA(cudaMemcpy2DAsync(s->state[s->cur] + g0, pitch, st[b], w, w, eb::kStateFields,
                               cudaMemcpyHostToDevice, s->stream));
-    SV_CUDA(cudaMemcpy2DAsync(s->par + g0, pitch, pr[b].data(), w, w, eb::kParamFields, cudaMemcpyHostToDevice,
+    SV_CUDA(cudaMemcpy2DAsync(s->par + g0, pitch, pr[b], w, w, eb::kParamFields, cudaMemcpyHostToDevice,
                               s->stream));
-    SV_CUDA(cudaMemcpyAsync(s->meta + g0, mt[b].data(), c * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    SV_CUDA(cudaMemcpyAsync(s->meta + g0, mt[b], c * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   }
-  const size_t nr = r.rods.size();
-  SV_CUDA(cudaMemcpyAsync(s->rods + r.rod0, info.data(), nr * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
-  SV_CUDA(cudaMemcpyAsync(s->rod_start + r.rod0, rstart.data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice,
-                          s->stream));
-  SV_CUDA(cudaMemcpyAsync(s->rod_n + r.rod0, rn.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+  SV_CUDA(cudaMemcpyAsync(s->rods + r.rod0, info, nr * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
+  SV_CUDA(cudaMemcpyAsync(s->rod_start + r.rod0, rstart, nr * sizeof(int64_t), cudaMemcpyHostToDevice, s->stream));
+  SV_CUDA(cudaMemcpyAsync(s->rod_n + r.rod0, rn, nr * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+  if (eb_status st = close_upload()) return st;
   const double g[3] = {(r.options & EB_REQUEST_GRAVITY) ? r.gravity[0] : 0.0,
                        (r.options & EB_REQUEST_GRAVITY) ? r.gravity[1] : 0.0,
                        (r.options & EB_REQUEST_GRAVITY) ? r.gravity[2] : 0.0};
@@ -609,8 +697,13 @@ EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** ou
                           static_cast<size_t>(n_bins + 2) * sizeof(eb::ServeCta), cudaHostAllocDefault);
     }
   if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&s->arena.base), kArenaBytes, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&s->upload.base), kUploadBytes, cudaHostAllocDefault);
   for (auto& ev : s->tick_event)
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  for (int p = 0; p < 2; ++p) {
+    if (e == cudaSuccess) e = cudaEventCreate(&s->launch_t0[p]);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->launch_t1[p]);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
     const std::string msg = std::string("server allocation: ") + cudaGetErrorString(e);
@@ -618,6 +711,7 @@ EB_API eb_status eb_server_create(const eb_server_config* config, eb_server** ou
     return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA, msg);
   }
   s->arena.cap = kArenaBytes;
+  s->upload.cap = kUploadBytes;
   s->bins.init(n_bins);
   s->rod_ids.init(s->rod_cap);
   *out = s.release();
@@ -685,6 +779,12 @@ EB_API eb_status eb_server_tick(eb_server* s, int64_t* in_flight) {
   if (s->tick_pending[parity]) {
     SV_CUDA(cudaEventSynchronize(s->tick_event[parity]));
     s->tick_pending[parity] = false;
+    if (s->launch_timed[parity]) {
+      float ms = 0.0f;
+      SV_CUDA(cudaEventElapsedTime(&ms, s->launch_t0[parity], s->launch_t1[parity]));
+      s->kernel_seconds += 1e-3 * ms;
+      s->launch_timed[parity] = false;
+    }
   }
   if (eb_status st = poll_events(s, false)) return st;
   if (eb_status st = admit(s)) return st;
@@ -734,11 +834,16 @@ EB_API eb_status eb_server_tick(eb_server* s, int64_t* in_flight) {
       if (!n_cta[p]) continue;
       SV_CUDA(cudaMemcpyAsync(s->d_cta[parity][p], s->h_cta[parity][p], n_cta[p] * sizeof(eb::ServeCta),
                               cudaMemcpyHostToDevice, s->stream));
+      if (!s->launch_timed[parity]) {
+        SV_CUDA(cudaEventRecord(s->launch_t0[parity], s->stream));
+        s->launch_timed[parity] = true;
+      }
       if (p == 0)
         SV_CUDA(eb::launch_rod_block_mixed_serve(a, s->d_cta[parity][p], n_cta[p], K, damped[p], s->stream));
       else
         SV_CUDA(eb::launch_rod_block_fp64_serve(a, s->d_cta[parity][p], n_cta[p], K, damped[p], s->stream));
     }
+    if (s->launch_timed[parity]) SV_CUDA(cudaEventRecord(s->launch_t1[parity], s->stream));
     s->cur ^= 1;
     std::vector<Request*> still;
     for (Request* r : s->active) {
@@ -820,6 +925,7 @@ EB_API eb_status eb_server_get_stats(const eb_server* s, eb_server_stats* out) {
   out->bins_used = s->n_bins - s->bins.free_bins();
   out->ticks = s->ticks;
   out->element_steps = s->element_steps;
+  out->kernel_seconds = s->kernel_seconds;
   return EB_OK;
 }
 

@@ -392,6 +392,7 @@ typedef struct eb_completion {
 typedef struct eb_server_stats {
   int64_t queued, active, finishing, completed, fallbacks, bins_total, bins_used, ticks;
   double element_steps;
+  double kernel_seconds; /* device time of the ticks' step launches that have completed */
 } eb_server_stats;
 
 EB_API eb_status eb_server_create(const eb_server_config* config, struct eb_server** out);
