@@ -156,6 +156,9 @@ SIGNATURES = {
                           ctypes.c_int64], ctypes.c_int),
     "eb_server_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
     "eb_server_get_stats": ([ctypes.c_void_p, _P(EbServerStats)], ctypes.c_int),
+    "eb_snapshot_size": ([_sim, _P(ctypes.c_uint64)], ctypes.c_int),
+    "eb_snapshot_save": ([_sim, ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
+    "eb_snapshot_load": ([_sim, ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
     "eb_partition_rods": ([_P(ctypes.c_int64), ctypes.c_int64, ctypes.c_int32, _P(ctypes.c_int32)], ctypes.c_int),
     "eb_box_pairs_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                               _P(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),

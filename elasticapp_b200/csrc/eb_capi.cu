@@ -1603,6 +1603,124 @@ EB_API eb_status eb_energy(eb_sim* s, double* out, int64_t count) {
   return check_device_status(s);
 }
 
+// ---- snapshots ------------------------------------------------------------
+// Layout: SnapshotHeader, n per rod (int64), the current state rows
+// (kStateFields x n_slots doubles), the parameter rows (kParamFields x
+// n_slots doubles), the per-rod constraint and forcing table (RodInfo per
+// rod).  The configuration hash covers what must match for a load: the
+// rods' sizes and models, contact membership, precision, stepper,
+// environment flags and gravity.
+namespace {
+struct SnapshotHeader {
+  char magic[8];
+  uint32_t version;
+  uint32_t sim_flags;
+  int64_t n_rods;
+  int64_t n_slots;
+  uint64_t config_hash;
+  double gravity[3];
+};
+constexpr char kSnapshotMagic[8] = {'E', 'B', 'S', 'N', 'A', 'P', '0', '1'};
+
+uint64_t snapshot_hash(const eb_sim* s) {
+  uint64_t h = 1469598103934665603ull;  // FNV-1a over the configuration words
+  auto mix = [&](uint64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      h ^= (v >> (8 * b)) & 0xffu;
+      h *= 1099511628211ull;
+    }
+  };
+  mix(static_cast<uint64_t>(s->cfg.precision));
+  mix(static_cast<uint64_t>(s->cfg.stepper));
+  mix(s->sim_flags);
+  for (const RodHost& r : s->rods) {
+    mix(static_cast<uint64_t>(r.n));
+    mix(static_cast<uint64_t>(r.model));
+    mix(static_cast<uint64_t>(static_cast<int64_t>(r.contact_material)));
+  }
+  return h;
+}
+
+uint64_t snapshot_bytes(const eb_sim* s) {
+  const uint64_t nr = s->rods.size(), ns = static_cast<uint64_t>(s->n_slots);
+  return sizeof(SnapshotHeader) + nr * sizeof(int64_t) +
+         ns * (eb::kStateFields + eb::kParamFields) * sizeof(double) + nr * sizeof(eb::RodInfo);
+}
+}  // namespace
+
+EB_API eb_status eb_snapshot_size(const eb_sim* s, uint64_t* bytes) {
+  if (check_sim(s) || !bytes) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "a snapshot needs a finalized simulator");
+  *bytes = snapshot_bytes(s);
+  return EB_OK;
+}
+
+EB_API eb_status eb_snapshot_save(eb_sim* s, void* buffer, uint64_t bytes) {
+  if (check_sim(s) || !buffer) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "a snapshot needs a finalized simulator");
+  if (bytes != snapshot_bytes(s)) return fail(EB_ERR_INVALID_ARGUMENT, "buffer size differs from eb_snapshot_size");
+  if (eb_status st = set_device(s)) return st;
+  unsigned char* p = static_cast<unsigned char*>(buffer);
+  SnapshotHeader h{};
+  std::memcpy(h.magic, kSnapshotMagic, 8);
+  h.version = 1;
+  h.sim_flags = s->sim_flags;
+  h.n_rods = static_cast<int64_t>(s->rods.size());
+  h.n_slots = s->n_slots;
+  h.config_hash = snapshot_hash(s);
+  for (int d = 0; d < 3; ++d) h.gravity[d] = s->gravity[d];
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  for (const RodHost& r : s->rods) {
+    std::memcpy(p, &r.n, sizeof(int64_t));
+    p += sizeof(int64_t);
+  }
+  const size_t pitch = static_cast<size_t>(s->stride) * sizeof(double);
+  const size_t w = static_cast<size_t>(s->n_slots) * sizeof(double);
+  EB_CUDA(cudaMemcpy2DAsync(p, w, s->d_state[s->cur], pitch, w, eb::kStateFields, cudaMemcpyDeviceToHost,
+                            s->stream));
+  p += w * eb::kStateFields;
+  EB_CUDA(cudaMemcpy2DAsync(p, w, s->d_param, pitch, w, eb::kParamFields, cudaMemcpyDeviceToHost, s->stream));
+  p += w * eb::kParamFields;
+  EB_CUDA(cudaMemcpyAsync(p, s->d_rods, s->rods.size() * sizeof(eb::RodInfo), cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_status(s);
+}
+
+EB_API eb_status eb_snapshot_load(eb_sim* s, const void* buffer, uint64_t bytes) {
+  if (check_sim(s) || !buffer) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "loading a snapshot needs a finalized simulator");
+  if (bytes < sizeof(SnapshotHeader)) return fail(EB_ERR_INVALID_ARGUMENT, "not a snapshot (too short)");
+  const unsigned char* p = static_cast<const unsigned char*>(buffer);
+  SnapshotHeader h;
+  std::memcpy(&h, p, sizeof(h));
+  if (std::memcmp(h.magic, kSnapshotMagic, 8) != 0 || h.version != 1)
+    return fail(EB_ERR_INVALID_ARGUMENT, "not a snapshot of this format");
+  if (bytes != snapshot_bytes(s) || h.n_rods != static_cast<int64_t>(s->rods.size()) || h.n_slots != s->n_slots ||
+      h.config_hash != snapshot_hash(s) || h.sim_flags != s->sim_flags ||
+      std::memcmp(h.gravity, s->gravity, sizeof(h.gravity)) != 0)
+    return fail(EB_ERR_INVALID_ARGUMENT, "the snapshot was taken from a differently configured simulator");
+  p += sizeof(h);
+  for (const RodHost& r : s->rods) {
+    int64_t n = 0;
+    std::memcpy(&n, p, sizeof(n));
+    p += sizeof(int64_t);
+    if (n != r.n) return fail(EB_ERR_INVALID_ARGUMENT, "the snapshot's rods differ from this simulator's");
+  }
+  if (eb_status st = set_device(s)) return st;
+  const size_t pitch = static_cast<size_t>(s->stride) * sizeof(double);
+  const size_t w = static_cast<size_t>(s->n_slots) * sizeof(double);
+  EB_CUDA(cudaMemcpy2DAsync(s->d_state[s->cur], pitch, p, w, w, eb::kStateFields, cudaMemcpyHostToDevice,
+                            s->stream));
+  p += w * eb::kStateFields;
+  EB_CUDA(cudaMemcpy2DAsync(s->d_param, pitch, p, w, w, eb::kParamFields, cudaMemcpyHostToDevice, s->stream));
+  p += w * eb::kParamFields;
+  EB_CUDA(cudaMemcpyAsync(s->d_rods, p, s->rods.size() * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  s->damper_dt = -1.0;  // the damper factors are refreshed for the next step's dt
+  return check_device_status(s);
+}
+
 EB_API eb_status eb_get_stream(const eb_sim* s, void** stream) {
   if (check_sim(s) || !stream) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
   *stream = static_cast<void*>(s->stream);

@@ -398,3 +398,34 @@ class Simulator:
     def set_batch(self, name: str, values: np.ndarray) -> None:
         a = np.ascontiguousarray(values, dtype=np.float64).ravel()
         L.call("eb_set_field_batch", self._h, L.FIELD_ID[name], L.EB_LAYOUT_PER_ROD, _dptr(a), a.size)
+
+    # -- snapshots and dumps ---------------------------------------------------
+    def snapshot(self) -> bytes:
+        """Device state, parameters and per-rod settings as one buffer (see
+        eb_snapshot_save); restore() loads it into this or an identically
+        configured simulator."""
+        n = ctypes.c_uint64()
+        L.call("eb_snapshot_size", self._h, ctypes.byref(n))
+        buf = ctypes.create_string_buffer(n.value)
+        L.call("eb_snapshot_save", self._h, buf, n.value)
+        return buf.raw
+
+    def restore(self, snapshot: bytes) -> None:
+        data = bytes(snapshot)
+        L.call("eb_snapshot_load", self._h, data, len(data))
+
+    def save(self, path) -> None:
+        with open(path, "wb") as f:
+            f.write(self.snapshot())
+
+    def load(self, path) -> None:
+        with open(path, "rb") as f:
+            self.restore(f.read())
+
+    def dump_rods(self, path, fields=("Position", "Velocity", "Director", "AngularVelocity")) -> None:
+        """Per-rod arrays of the given variables in one numpy archive, keys
+        ``rod<k>/<Variable>`` (the per-rod datasets the reference writes to
+        HDF5 in Simulator/IO/H5/Systems/CosseratRods/CosseratRod.hpp; HDF5
+        itself is not available here)."""
+        arrays = {f"rod{k}/{name}": ref.get(name) for k, ref in enumerate(self.rods) for name in fields}
+        np.savez(path, **arrays)

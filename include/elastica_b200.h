@@ -312,6 +312,19 @@ EB_API eb_status eb_energy(struct eb_sim* sim, double* out, int64_t count);
  * callers that order their own work or timing events against it. */
 EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
 
+/* --- snapshots (checkpoint / restart) --------------------------------------
+ * The reference serialises a finalized simulator (its systems' variables and
+ * modules) into an archive and loads it into an identically configured one
+ * (elastica/Simulator/Interface/Simulator/Serialize.hpp:19-92).  Here a
+ * snapshot is one host buffer: a header, the rods' sizes, the device state and
+ * parameter arrays and the per-rod constraint and forcing table.  Loading
+ * needs a finalized simulator built with the same rods (sizes, models,
+ * contact membership), precision, stepper and environment; anything else is
+ * EB_ERR_INVALID_ARGUMENT.  The time is the caller's (eb_step's t). */
+EB_API eb_status eb_snapshot_size(const struct eb_sim* sim, uint64_t* bytes);
+EB_API eb_status eb_snapshot_save(struct eb_sim* sim, void* buffer, uint64_t bytes);
+EB_API eb_status eb_snapshot_load(struct eb_sim* sim, const void* buffer, uint64_t bytes);
+
 /* The step plan chosen by the first eb_step: mode 1 = streaming kernel,
  * 2 = resident kernel with block configuration `config`, 3 = resident kernel
  * per size bucket, one launch per bucket that holds rods: bucket 0 (rods of
