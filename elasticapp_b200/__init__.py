@@ -6,9 +6,9 @@ built in-tree by ``python -m elasticapp_b200.build`` and there is no CPU
 fallback.
 """
 from .simulator import (AnalyticalLinearDamper, Clamp, CollisionSystem, ContactMaterial, CosseratRod,
-                        CosseratRodWithoutDamping, EndTorque, GravityField, Material, PEFRL, PositionVerlet, RodRef,
-                        Simulator, StraightRod)
+                        CosseratRodWithoutDamping, EndTorque, FreeJoint, GravityField, HingeJoint, Material, PEFRL,
+                        PositionVerlet, RodRef, Simulator, StraightRod)
 from . import _lib
 
 __all__ = ["AnalyticalLinearDamper", "Clamp", "CollisionSystem", "ContactMaterial", "CosseratRod", "CosseratRodWithoutDamping", "EndTorque",
-           "GravityField", "Material", "PEFRL", "PositionVerlet", "RodRef", "Simulator", "StraightRod", "_lib"]
+           "FreeJoint", "GravityField", "HingeJoint", "Material", "PEFRL", "PositionVerlet", "RodRef", "Simulator", "StraightRod", "_lib"]

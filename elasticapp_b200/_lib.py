@@ -108,6 +108,14 @@ class EbServerStats(ctypes.Structure):
                [("element_steps", ctypes.c_double), ("kernel_seconds", ctypes.c_double)]
 
 
+class EbJoint(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("stiffness", ctypes.c_double),
+                ("damping", ctypes.c_double), ("rotational_stiffness", ctypes.c_double),
+                ("normal", ctypes.c_double * 3)]
+
+
+EB_JOINT_FREE = 0
+EB_JOINT_HINGE = 1
 EB_SERVER_FORCE_FALLBACK = 0x1
 EB_REQUEST_CLAMP = 0x1
 EB_REQUEST_DAMPER = 0x2
@@ -140,6 +148,8 @@ SIGNATURES = {
     "eb_add_rod_contact": ([_sim, ctypes.c_int64, ctypes.c_int32], ctypes.c_int),
     "eb_add_contact_plane": ([_sim, _P(ctypes.c_double), _P(ctypes.c_double), ctypes.c_int32], ctypes.c_int),
     "eb_contact_pairs": ([_sim, _P(ctypes.c_int64), ctypes.c_int64, _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_connect": ([_sim, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _P(EbJoint)],
+                   ctypes.c_int),
     "eb_finalize": ([_sim], ctypes.c_int),
     "eb_step": ([_sim, _P(ctypes.c_double), ctypes.c_double, ctypes.c_int64], ctypes.c_int),
     "eb_synchronize": ([_sim], ctypes.c_int),

@@ -30,10 +30,12 @@ SOURCES = [
     # candidate pairs bit-identical to a scalar FP64 evaluation
     ("contact.o", "contact.cu", ["--fmad=false"]),
     ("box_pairs_noalloc.o", "box_pairs_noalloc.cu", []),
+    # joint loads rounded as written, like the CPU restatement
+    ("connection.o", "connection.cu", ["--fmad=false"]),
     ("serve.o", "serve.cu", []),
     ("partition.o", "partition.cu", []),
 ]
-HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h", "eb_host.h"]
+HEADERS = ["eb_internal.h", "rod_math.cuh", "bulk_copy.cuh", "contact.h", "eb_host.h", "joint.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -20,6 +21,7 @@
 #include "contact.h"
 #include "eb_host.h"
 #include "eb_internal.h"
+#include "joint.h"
 
 namespace eb {
 cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream);
@@ -146,6 +148,22 @@ struct ContactDevice {
   bool evaluated = false;
 };
 
+// a connection as added, and its device side
+struct JointHost {
+  int64_t rod_a, index_a, rod_b, index_b;
+  eb_joint joint;
+};
+
+struct JointDevice {
+  bool on = false;
+  eb::JointDev* joints = nullptr;
+  double* out = nullptr;
+  int64_t *force_slot = nullptr, *force_off = nullptr, *torque_slot = nullptr, *torque_off = nullptr;
+  int32_t *force_src = nullptr, *torque_src = nullptr;
+  int64_t n_force = 0, n_torque = 0;
+  double* loads = nullptr;  // 6 x stride: node force rows 0-2, element torque rows 3-5 (lab frame)
+};
+
 }  // namespace
 
 struct eb_sim {
@@ -197,6 +215,9 @@ struct eb_sim {
   std::vector<eb_contact_material> materials;
   std::vector<eb::ContactPlane> planes;
   ContactDevice contact;
+  // connections
+  std::vector<JointHost> joints;
+  JointDevice jd;
 };
 
 namespace {
@@ -358,6 +379,14 @@ void host_free(eb_sim* s) {
   for (auto* p : s->d_cta_start)
     if (p) cudaFree(p);
   s->d_cta_start.clear();
+  {
+    JointDevice& j = s->jd;
+    void* p[] = {j.joints, j.out, j.force_slot, j.force_off, j.torque_slot, j.torque_off, j.force_src, j.torque_src,
+                 j.loads};
+    for (void* q : p)
+      if (q) cudaFree(q);
+    j = JointDevice{};
+  }
   for (auto& b : s->buckets) {
     for (int c = 0; c < 4; ++c) {
       if (b.d_off[c]) cudaFree(b.d_off[c]);
@@ -878,6 +907,118 @@ EB_API eb_status eb_add_contact_plane(eb_sim* s, const double point[3], const do
   return EB_OK;
 }
 
+namespace {
+
+// Device tables of the connections: one entry per joint and, per loaded
+// slot, the joints acting on it in connection order (rod a's share first).
+eb_status setup_joints(eb_sim* s) {
+  JointDevice& j = s->jd;
+  if (s->joints.empty()) return EB_OK;
+  const int64_t S = s->stride;
+  std::vector<eb::JointDev> dev;
+  std::map<int64_t, std::vector<int32_t>> fsrc, tsrc;
+  for (size_t c = 0; c < s->joints.size(); ++c) {
+    const JointHost& h = s->joints[c];
+    eb::JointDev d{};
+    d.node_a = s->offsets[h.rod_a] + h.index_a + 1;
+    d.node_b = s->offsets[h.rod_b] + h.index_b;
+    d.kind = h.joint.kind == EB_JOINT_HINGE ? eb::kJointHinge : eb::kJointFree;
+    d.k = h.joint.stiffness;
+    d.nu = h.joint.damping;
+    d.k_rot = h.joint.rotational_stiffness;
+    for (int k = 0; k < 3; ++k) d.normal[k] = h.joint.normal[k];
+    dev.push_back(d);
+    const int32_t id = static_cast<int32_t>(2 * c);
+    fsrc[d.node_a].push_back(id);
+    fsrc[d.node_b].push_back(id | 1);
+    if (d.kind == eb::kJointHinge) {
+      tsrc[s->offsets[h.rod_a] + h.index_a].push_back(id | 1);
+      tsrc[d.node_b].push_back(id);
+    }
+  }
+  auto csr = [](const std::map<int64_t, std::vector<int32_t>>& m, std::vector<int64_t>& slot,
+                std::vector<int64_t>& off, std::vector<int32_t>& src) {
+    off.push_back(0);
+    for (const auto& kv : m) {
+      slot.push_back(kv.first);
+      src.insert(src.end(), kv.second.begin(), kv.second.end());
+      off.push_back(static_cast<int64_t>(src.size()));
+    }
+  };
+  std::vector<int64_t> fslot, foff, tslot, toff;
+  std::vector<int32_t> fs, ts;
+  csr(fsrc, fslot, foff, fs);
+  csr(tsrc, tslot, toff, ts);
+  auto up = [&](auto** p, const auto& v) -> cudaError_t {
+    const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(v[0]);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    if (e == cudaSuccess && !v.empty())
+      e = cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, s->stream);
+    return e;
+  };
+  EB_CUDA(up(&j.joints, dev));
+  EB_CUDA(up(&j.force_slot, fslot));
+  EB_CUDA(up(&j.force_off, foff));
+  EB_CUDA(up(&j.force_src, fs));
+  EB_CUDA(up(&j.torque_slot, tslot));
+  EB_CUDA(up(&j.torque_off, toff));
+  EB_CUDA(up(&j.torque_src, ts));
+  EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&j.out), dev.size() * 6 * sizeof(double)));
+  EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&j.loads), static_cast<size_t>(6 * S) * sizeof(double)));
+  EB_CUDA(cudaMemsetAsync(j.loads, 0, static_cast<size_t>(6 * S) * sizeof(double), s->stream));
+  j.n_force = static_cast<int64_t>(fslot.size());
+  j.n_torque = static_cast<int64_t>(tslot.size());
+  j.on = true;
+  return EB_OK;
+}
+
+eb::JointArgs joint_args(eb_sim* s) {
+  const JointDevice& j = s->jd;
+  eb::JointArgs a{};
+  a.n_joints = static_cast<int32_t>(s->joints.size());
+  a.joints = j.joints;
+  a.out = j.out;
+  a.stride = s->stride;
+  a.meta = s->d_meta;
+  a.rods = s->d_rods;
+  a.n_force_slots = j.n_force;
+  a.force_slot = j.force_slot;
+  a.force_off = j.force_off;
+  a.force_src = j.force_src;
+  a.n_torque_slots = j.n_torque;
+  a.torque_slot = j.torque_slot;
+  a.torque_off = j.torque_off;
+  a.torque_src = j.torque_src;
+  a.joint_force = j.loads;
+  a.joint_torque = j.loads + 3 * s->stride;
+  return a;
+}
+
+}  // namespace
+
+EB_API eb_status eb_connect(eb_sim* s, int64_t rod_a, int64_t index_a, int64_t rod_b, int64_t index_b,
+                            const eb_joint* joint) {
+  if (check_sim(s) || !joint) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add connections after finalize");
+  const int64_t nr = static_cast<int64_t>(s->rods.size());
+  if (rod_a < 0 || rod_a >= nr || rod_b < 0 || rod_b >= nr) return fail(EB_ERR_NOT_FOUND, "unknown rod");
+  if (joint->kind != EB_JOINT_FREE && joint->kind != EB_JOINT_HINGE)
+    return fail(EB_ERR_INVALID_ARGUMENT, "unknown joint kind");
+  const int64_t na = s->rods[rod_a].n, nb = s->rods[rod_b].n;
+  // force on node index_a + 1 of rod a and node index_b of rod b; the hinge
+  // also loads element index_a of rod a and element index_b of rod b
+  if (index_a < 0 || index_a >= na) return fail(EB_ERR_INVALID_ARGUMENT, "index_a must name an element of rod a");
+  if (index_b < 0 || index_b > nb || (joint->kind == EB_JOINT_HINGE && index_b >= nb))
+    return fail(EB_ERR_INVALID_ARGUMENT, "index_b must name a node (an element for a hinge) of rod b");
+  const double vals[] = {joint->stiffness, joint->damping, joint->rotational_stiffness, joint->normal[0],
+                         joint->normal[1], joint->normal[2]};
+  for (double v : vals)
+    if (!std::isfinite(v)) return fail(EB_ERR_INVALID_ARGUMENT, "joint parameters must be finite");
+  if (s->joints.size() >= (size_t(1) << 30)) return fail(EB_ERR_UNSUPPORTED, "too many connections");
+  s->joints.push_back({rod_a, index_a, rod_b, index_b, *joint});
+  return EB_OK;
+}
+
 EB_API eb_status eb_finalize(eb_sim* s) {
   if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
   if (s->finalized) return fail(EB_ERR_INVALID_STATE, "already finalized");
@@ -945,6 +1086,10 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   EB_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(uint32_t), s->stream));
   s->cur = 0;
   if (eb_status st = setup_contact(s)) {
+    host_free(s);
+    return st;
+  }
+  if (eb_status st = setup_joints(s)) {
     host_free(s);
     return st;
   }
@@ -1265,7 +1410,7 @@ eb_status plan_steps(eb_sim* s, double dt) {
   // contact needs a global exchange every step, PEFRL four force evaluations
   // a step: the streaming kernel
   const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
-                            s->contact.on || s->cfg.stepper == EB_STEPPER_PEFRL;
+                            s->contact.on || s->jd.on || s->cfg.stepper == EB_STEPPER_PEFRL;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -1396,19 +1541,33 @@ eb::ContactArgs contact_args(eb_sim* s, double dt) {
 // Steps with the collision system, in chunks: the chunk's starting state is
 // kept, and a chunk whose candidate pairs overflowed the partner buffer is
 // run again from it with a larger buffer.
+// Streaming steps with external loads evaluated at every force evaluation's
+// drifted state: the collision system (in chunks of kContactChunk steps,
+// rerun with a larger pair buffer on overflow) and/or the connections.
 eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
   ContactDevice& c = s->contact;
+  const bool contact = c.on;
   const size_t state_bytes = static_cast<size_t>(eb::kStateFields * s->stride) * sizeof(double);
   eb::StepArgs a = step_args(s, dt);
-  a.contact_force = c.loads;
-  a.contact_torque = c.loads + 3 * s->stride;
+  if (contact) {
+    a.contact_force = c.loads;
+    a.contact_torque = c.loads + 3 * s->stride;
+  }
+  eb::JointArgs ja{};
+  if (s->jd.on) {
+    ja = joint_args(s);
+    a.joint_force = ja.joint_force;
+    a.joint_torque = ja.joint_torque;
+  }
   int64_t done = 0;
   int regrowths = 0;
   while (done < n_steps) {
-    const int64_t k = std::min<int64_t>(kContactChunk, n_steps - done);
+    const int64_t k = contact ? std::min<int64_t>(kContactChunk, n_steps - done) : n_steps - done;
     const int c0 = s->cur;
-    EB_CUDA(cudaMemcpyAsync(c.backup, s->d_state[c0], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
-    eb::ContactArgs ca = contact_args(s, dt);
+    if (contact)
+      EB_CUDA(cudaMemcpyAsync(c.backup, s->d_state[c0], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+    eb::ContactArgs ca{};
+    if (contact) ca = contact_args(s, dt);
     const Substep* sub;
     const int ns = substeps(s, &sub);
     for (int64_t i = 0; i < k; ++i) {
@@ -1420,14 +1579,26 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
           a.drift_post = sub[j].post * dt;
           ca.half_dt = a.drift_pre;
         }
-        ca.state = s->d_state[s->cur];
-        EB_CUDA(eb::launch_contact(ca, s->stream, &s->launches));
+        if (contact) {
+          ca.state = s->d_state[s->cur];
+          EB_CUDA(eb::launch_contact(ca, s->stream, &s->launches));
+        }
+        if (s->jd.on) {
+          ja.state = s->d_state[s->cur];
+          ja.pre = a.drift_pre;
+          EB_CUDA(eb::launch_joints(ja, s->stream));
+          s->launches += 2;
+        }
         a.in = s->d_state[s->cur];
         a.out = s->d_state[s->cur ^ 1];
         EB_CUDA(launch_streaming(s, a, diag && done + i == n_steps - 1 && j == ns - 1));
         s->cur ^= 1;
         ++s->launches;
       }
+    }
+    if (!contact) {
+      done += k;
+      continue;
     }
     uint32_t st = 0;
     unsigned long long req = 0;
@@ -1478,7 +1649,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (s->plan_mode == 0)
     if (eb_status st = plan_steps(s, dt)) return st;
   const bool diag = s->d_diag != nullptr;
-  if (s->contact.on) {
+  if (s->contact.on || s->jd.on) {
     if (eb_status st = step_with_contact(s, dt, n_steps, diag)) return st;
     if (time)
       for (int64_t k = 0; k < n_steps; ++k) {
@@ -1608,8 +1779,8 @@ EB_API eb_status eb_energy(eb_sim* s, double* out, int64_t count) {
 // (kStateFields x n_slots doubles), the parameter rows (kParamFields x
 // n_slots doubles), the per-rod constraint and forcing table (RodInfo per
 // rod).  The configuration hash covers what must match for a load: the
-// rods' sizes and models, contact membership, precision, stepper,
-// environment flags and gravity.
+// rods' sizes and models, contact membership, the connections, precision,
+// stepper, environment flags and gravity.
 namespace {
 struct SnapshotHeader {
   char magic[8];
@@ -1637,6 +1808,13 @@ uint64_t snapshot_hash(const eb_sim* s) {
     mix(static_cast<uint64_t>(r.n));
     mix(static_cast<uint64_t>(r.model));
     mix(static_cast<uint64_t>(static_cast<int64_t>(r.contact_material)));
+  }
+  for (const JointHost& j : s->joints) {
+    mix(static_cast<uint64_t>(j.rod_a));
+    mix(static_cast<uint64_t>(j.index_a));
+    mix(static_cast<uint64_t>(j.rod_b));
+    mix(static_cast<uint64_t>(j.index_b));
+    mix(static_cast<uint64_t>(j.joint.kind));
   }
   return h;
 }

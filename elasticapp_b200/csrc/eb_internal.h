@@ -108,6 +108,10 @@ struct StepArgs {
   // element slot), or nullptr without a collision system
   const double* contact_force;
   const double* contact_torque;
+  // connection loads of this step (lab frame, 3 x stride each): forces per
+  // node slot, torques per element slot; or nullptr without connections
+  const double* joint_force;
+  const double* joint_torque;
 };
 
 // Rods longer than one CTA's capacity run on a pair of CTAs (a thread-block

@@ -275,13 +275,18 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   D3 Fe{0.0, 0.0, 0.0};
   if (a.sim_flags & kSimGravity)
     Fe = {0.0 + a.gravity[0] * m, 0.0 + a.gravity[1] * m, 0.0 + a.gravity[2] * m};
-  if (kContact) {
+  if (kContact && a.contact_force) {
     // collision system after gravity: the element before the node, then the
     // element at the node, each adding half its capsule force
     // (Systems/Customization/CosseratRods/Transfer/Common.hpp:32-55)
     const double* __restrict__ cf = a.contact_force;
     if (!(meta & kFirst)) Fe = {Fe.x + 0.5 * cf[g - 1], Fe.y + 0.5 * cf[S + g - 1], Fe.z + 0.5 * cf[2 * S + g - 1]};
     if (meta & kElem) Fe = {Fe.x + 0.5 * cf[g], Fe.y + 0.5 * cf[S + g], Fe.z + 0.5 * cf[2 * S + g]};
+  }
+  if (kContact && a.joint_force) {
+    // connections after the collision system
+    const double* __restrict__ jf = a.joint_force;
+    Fe = {Fe.x + jf[g], Fe.y + jf[S + g], Fe.z + jf[2 * S + g]};
   }
   const double inv_m = 1.0 / m;
   const D3 acc = {(F.x + Fe.x) * inv_m, (F.y + Fe.y) * inv_m, (F.z + Fe.z) * inv_m};
@@ -301,10 +306,15 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       T = {T.x - c * w.x, T.y - c * w.y, T.z - c * w.z};
     }
     D3 Te{0.0, 0.0, 0.0};
-    if (kContact) {
+    if (kContact && a.contact_torque) {
       // the capsule torque recast into the material frame: Q tau
       const double* __restrict__ ct = a.contact_torque;
       Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
+    }
+    if (kContact && a.joint_torque) {
+      // the connections' torque (summed in the lab frame), recast the same way
+      const double* __restrict__ jt = a.joint_torque;
+      Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
     }
     if ((meta & kLastElem) && (rflags & kRodEndTorque)) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
@@ -412,7 +422,8 @@ cudaError_t launch_window_c(const StepArgs& args, bool diag, bool damped, cudaSt
 
 template <int W, int MinBlocks>
 cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if (args.contact_force && args.contact_torque)
+  // the external-load variant: collision system and/or connections
+  if ((args.contact_force && args.contact_torque) || (args.joint_force && args.joint_torque))
     return launch_window_c<W, MinBlocks, true>(args, diag, damped, stream);
   return launch_window_c<W, MinBlocks, false>(args, diag, damped, stream);
 }

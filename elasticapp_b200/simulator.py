@@ -140,6 +140,60 @@ class CollisionSystem:
 
 
 @dataclass
+class FreeJoint:
+    """Translational spring (stiffness) and dashpot along the separation
+    (damping) between node index_a + 1 of rod a and node index_b of rod b
+    (the force rule of examples/hinge_joint/HingeJointCaseStudy.cpp:116-136)."""
+
+    def __init__(self, stiffness: float, damping: float = 0.0):
+        self.stiffness, self.damping = float(stiffness), float(damping)
+
+    def to_c(self) -> L.EbJoint:
+        j = L.EbJoint()
+        j.kind, j.stiffness, j.damping = L.EB_JOINT_FREE, self.stiffness, self.damping
+        return j
+
+
+class HingeJoint(FreeJoint):
+    """FreeJoint plus the rotational spring that resists the component of rod
+    b's element index_b along `normal` (HingeJointCaseStudy.cpp:137-150)."""
+
+    def __init__(self, stiffness: float, damping: float, rotational_stiffness: float, normal):
+        super().__init__(stiffness, damping)
+        self.rotational_stiffness = float(rotational_stiffness)
+        self.normal = tuple(float(v) for v in normal)
+
+    def to_c(self) -> L.EbJoint:
+        j = super().to_c()
+        j.kind = L.EB_JOINT_HINGE
+        j.rotational_stiffness = self.rotational_stiffness
+        for k in range(3):
+            j.normal[k] = self.normal[k]
+        return j
+
+
+class _Connect:
+    """simulator.connect(rod_a, index_a).to(rod_b, index_b).using(joint), the
+    reference's connect(rod_a, at(i)).to(rod_b, at(j)).with(generator)."""
+
+    def __init__(self, sim, rod_a, index_a):
+        self.sim, self.rod_a, self.index_a = sim, rod_a, int(index_a)
+        self.rod_b = self.index_b = None
+
+    def to(self, rod_b, index_b: int) -> "_Connect":
+        self.rod_b, self.index_b = rod_b, int(index_b)
+        return self
+
+    def using(self, joint: FreeJoint) -> None:
+        if self.rod_b is None:
+            raise TypeError("connect(...).to(rod, index) first")
+        j = joint.to_c()
+        L.call("eb_connect", self.sim._h, self.rod_a.id, self.index_a, self.rod_b.id, self.index_b,
+               ctypes.byref(j))
+
+    with_ = using
+
+
 class PositionVerlet:
     """Time/SymplecticSteppers/Algorithms/PositionVerlet.hpp:49-88."""
 
@@ -269,6 +323,9 @@ class Simulator:
     # -- modules ---------------------------------------------------------------
     def constrain(self, rod: RodRef) -> _At:
         return _At(self, rod, "constrain")
+
+    def connect(self, rod_a: RodRef, index_a: int) -> _Connect:
+        return _Connect(self, rod_a, index_a)
 
     def force(self, rod: RodRef) -> _At:
         return _At(self, rod, "force")

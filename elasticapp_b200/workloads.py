@@ -44,7 +44,7 @@ class Workload:
     seed: int
     rods: list  # StraightRod
     model: type = CosseratRodWithoutDamping
-    clamp: bool = True
+    clamp: bool | list = True                 # every rod, or per rod
     damper: tuple | None = (0.1, 0.1)
     gravity: tuple | None = (0.0, 0.0, -9.81)
     end_torque: np.ndarray | None = None      # (n_rods, 3) lab frame
@@ -55,6 +55,7 @@ class Workload:
     contact_materials: list | None = None     # ContactMaterial per material id
     contact_rod_material: list | None = None  # per rod material id (-1: none)
     planes: list | None = None                # (point, normal, material id)
+    connections: list | None = None           # (rod_a, index_a, rod_b, index_b, FreeJoint or HingeJoint)
 
     @property
     def n_elements(self) -> np.ndarray:
@@ -79,7 +80,7 @@ class Workload:
                 ref.set("Velocity", self.velocities[k])
             if self.rest_curvature is not None:
                 ref.set("ReferenceCurvature", self.rest_curvature[k])
-            if self.clamp:
+            if self.clamp if isinstance(self.clamp, bool) else self.clamp[k]:
                 sim.constrain(ref).at(0).using(Clamp())
             if self.damper is not None:
                 sim.constrain(ref).using(AnalyticalLinearDamper(*self.damper))
@@ -94,6 +95,8 @@ class Workload:
                     sim.add_contact(ref, ids[mat])
             for point, normal, mat in (self.planes or []):
                 sim.emplace_plane(point, normal, ids[mat])
+        for ra, ia, rb, ib, joint in (self.connections or []):
+            sim.connect(refs[ra], ia).to(refs[rb], ib).using(joint)
         sim.finalize()
         return sim
 
@@ -117,6 +120,27 @@ def _normals(rng, directions):
                 out[i] = c / np.linalg.norm(c)
                 break
     return out
+
+
+def hinge_chain(n_links: int = 2, n_elements: int = 10, seed: int = 1006, n_steps: int = 20_000) -> Workload:
+    """Links end to end along +z with the hinge-joint example's parameters
+    (examples/hinge_joint/HingeJointCaseStudy.cpp: rho 1750, E 3e7, G 2e7,
+    r 0.007, L 0.2, damping rate 0.015, hinge k 1e5, nu 0, k_rot 5e3 about
+    normal x direction); the first link clamped at its base.  In place of the
+    example's time-dependent tip force (a user-written rule) the chain sags
+    under gravity along -y from seeded node velocities N(0, 1e-3^2)."""
+    from .simulator import CosseratRod, HingeJoint
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L, n = 0.2, n_elements
+    rods = [StraightRod(n_elements=n, material=Material(1750.0, 3e7, 2e7), radius=0.007, length=L,
+                        origin=(0.0, 0.0, k * L), direction=(0.0, 0.0, 1.0), normal=(0.0, 1.0, 0.0),
+                        force_damping_rate=0.015, torque_damping_rate=0.015) for k in range(n_links)]
+    roll = (1.0, 0.0, 0.0)  # normal x direction
+    joints = [(k, n - 1, k + 1, 0, HingeJoint(1e5, 0.0, 5e3, roll)) for k in range(n_links - 1)]
+    vel = [rng.normal(0.0, 1e-3, size=(3, n + 1)) for _ in range(n_links)]
+    return Workload("hinge_chain", seed, rods, model=CosseratRod, clamp=[k == 0 for k in range(n_links)],
+                    damper=None, gravity=(0.0, -9.81, 0.0), velocities=vel, dt=1e-5, n_steps=n_steps,
+                    connections=joints)
 
 
 def cantilever(n_elements: int = 100, seed: int = 1001) -> Workload:

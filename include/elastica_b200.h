@@ -283,6 +283,36 @@ EB_API eb_status eb_add_rod_contact(struct eb_sim* sim, int64_t rod, int32_t mat
  * (PlanePrimitive, Simulator/Environments/Primitives/PlanePrimitive.cpp:60-130). */
 EB_API eb_status eb_add_contact_plane(struct eb_sim* sim, const double point[3], const double normal[3],
                                       int32_t material_id);
+/* --- connections (joints) between rods --------------------------------------
+ * The reference joins two rods with simulator->connect(rod_a, at(i)).to(rod_b,
+ * at(j)).with(generator), the generator holding a user-written force and
+ * torque rule applied among the pre-dynamic updates
+ * (elastica/Simulator/Connections/Connection.hpp, MakeConnection.hpp).  The
+ * rules here are built in, those of the reference's hinge-joint example
+ * (examples/hinge_joint/HingeJointCaseStudy.cpp:96-150) with its indices:
+ *   every joint: d = x_b[j] - x_a[i + 1], u = d / |d| (0 for d = 0),
+ *     F = k d - nu ((v_b[j] - v_a[i + 1]) . u) u; node i + 1 of rod a gains F,
+ *     node j of rod b loses it;
+ *   EB_JOINT_HINGE also: l = x_b[j + 1] - x_b[j], f = -k_rot (l . n) n,
+ *     tau = l x f; element i of rod a loses Q_a tau, element j of rod b gains
+ *     Q_b tau (material frame).
+ * i must name an element of rod a; j a node of rod b (an element for a
+ * hinge).  Connections are evaluated at every force evaluation's drifted
+ * state (as the collision system), after gravity and contact; several
+ * connections on one node or element are summed in the order they were
+ * added.  A simulator with connections steps on the streaming kernel. */
+typedef enum eb_joint_kind { EB_JOINT_FREE = 0, EB_JOINT_HINGE = 1 } eb_joint_kind;
+typedef struct eb_joint {
+  int32_t kind;                /* eb_joint_kind */
+  int32_t reserved;
+  double stiffness;            /* k */
+  double damping;              /* nu, along the separation */
+  double rotational_stiffness; /* k_rot (hinge) */
+  double normal[3];            /* n (hinge): the direction the hinge resists */
+} eb_joint;
+EB_API eb_status eb_connect(struct eb_sim* sim, int64_t rod_a, int64_t index_a, int64_t rod_b, int64_t index_b,
+                            const eb_joint* joint);
+
 /* Candidate pairs of the last step's contact evaluation: pairs[2 k], pairs[2 k + 1]
  * = (a, b), a < b, sorted; a capsule's id is its element slot (rod r's element
  * i is eb_slot_offsets()[r] + i) and plane p is eb_slot_count() + p.  Writes
@@ -319,7 +349,8 @@ EB_API eb_status eb_get_stream(const struct eb_sim* sim, void** stream);
  * snapshot is one host buffer: a header, the rods' sizes, the device state and
  * parameter arrays and the per-rod constraint and forcing table.  Loading
  * needs a finalized simulator built with the same rods (sizes, models,
- * contact membership), precision, stepper and environment; anything else is
+ * contact membership), connections, precision, stepper and environment;
+ * anything else is
  * EB_ERR_INVALID_ARGUMENT.  The time is the caller's (eb_step's t). */
 EB_API eb_status eb_snapshot_size(const struct eb_sim* sim, uint64_t* bytes);
 EB_API eb_status eb_snapshot_save(struct eb_sim* sim, void* buffer, uint64_t bytes);

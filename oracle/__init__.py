@@ -94,6 +94,9 @@ def lib():
         for name in ("orc_fine_capsule_capsule", "orc_fine_capsule_plane"):
             getattr(_lib, name).argtypes = [_P, _P, _P]
         _lib.orc_fine_pair_loads.argtypes = [_P, _P, _P, _P]
+        _lib.orc_step_loads.argtypes = [ctypes.POINTER(_OrcRods), ctypes.POINTER(_OrcContact),
+                                        ctypes.POINTER(_OrcConnections), ctypes.c_double, ctypes.c_int64,
+                                        ctypes.c_int]
     return _lib
 
 
@@ -270,6 +273,53 @@ class ContactSpec:
         c.capsule_force = self.capsule_force.ctypes.data_as(_P)
         c.capsule_torque = self.capsule_torque.ctypes.data_as(_P)
         return c
+
+
+_I64 = ctypes.POINTER(ctypes.c_int64)
+
+
+class _OrcConnections(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("rod_a", _I64), ("index_a", _I64), ("rod_b", _I64), ("index_b", _I64),
+                ("kind", ctypes.POINTER(ctypes.c_int32)), ("k", _P), ("nu", _P), ("k_rot", _P), ("normal", _P)]
+
+
+class ConnectionSpec:
+    """Connections for the oracle, in order: (rod_a, index_a, rod_b, index_b,
+    kind (0 free, 1 hinge), k, nu, k_rot, normal(3))."""
+
+    def __init__(self, connections):
+        c = list(connections)
+        self.n = len(c)
+        col = lambda i, dt: np.ascontiguousarray([x[i] for x in c] or [0], dtype=dt)
+        self.rod_a, self.index_a = col(0, np.int64), col(1, np.int64)
+        self.rod_b, self.index_b = col(2, np.int64), col(3, np.int64)
+        self.kind = col(4, np.int32)
+        self.k, self.nu, self.k_rot = col(5, np.float64), col(6, np.float64), col(7, np.float64)
+        self.normal = np.ascontiguousarray(np.array([x[8] for x in c] or [[0.0, 0.0, 0.0]],
+                                                    dtype=np.float64).reshape(-1))
+
+    def _struct(self):
+        s = _OrcConnections()
+        s.n = self.n
+        s.rod_a, s.index_a = self.rod_a.ctypes.data_as(_I64), self.index_a.ctypes.data_as(_I64)
+        s.rod_b, s.index_b = self.rod_b.ctypes.data_as(_I64), self.index_b.ctypes.data_as(_I64)
+        s.kind = self.kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        s.k, s.nu, s.k_rot = self.k.ctypes.data_as(_P), self.nu.ctypes.data_as(_P), self.k_rot.ctypes.data_as(_P)
+        s.normal = self.normal.ctypes.data_as(_P)
+        return s
+
+
+def loads_step(rods: RodArrays, contact: "ContactSpec | None", connections: ConnectionSpec | None, dt,
+               n_steps=1, n_threads=0):
+    """PositionVerlet steps with the collision system and/or connections
+    (orc_step_loads)."""
+    s = rods._struct()
+    c = contact._struct(rods.n_slots) if contact is not None else None
+    j = connections._struct() if connections is not None else None
+    rc = lib().orc_step_loads(ctypes.byref(s), ctypes.byref(c) if c is not None else None,
+                              ctypes.byref(j) if j is not None else None, float(dt), int(n_steps), int(n_threads))
+    if rc != 0:
+        raise RuntimeError("orc_step_loads failed")
 
 
 def contact_step(rods: RodArrays, spec: ContactSpec, dt, n_steps=1, n_threads=0):

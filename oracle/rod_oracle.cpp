@@ -201,8 +201,11 @@ void clamp_values(const OrcRods& R, int64_t r) {
 // cf, ct: capsule contact force and torque (lab frame, per element slot,
 // 3*S) transferred to the rod as in
 // Systems/Customization/CosseratRods/Transfer/Common.hpp:32-55, or NULL.
+// nf, nt: connection loads (lab frame; node forces and element torques,
+// 3*S each), added after the contact loads, or NULL.
 void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, double* alpha,
-                      const double* cf = nullptr, const double* ct = nullptr) {
+                      const double* cf = nullptr, const double* ct = nullptr, const double* nf = nullptr,
+                      const double* nt = nullptr) {
   const int64_t S = R.n_slots, o = R.offset[r], n = R.offset[r + 1] - o - 1;
   const Field x{R.x, S}, v{R.v, S}, w{R.w, S};
   sc.resize(n);
@@ -352,6 +355,7 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
       if (j > 0) fe = {fe.x + 0.5 * cf[s - 1], fe.y + 0.5 * cf[S + s - 1], fe.z + 0.5 * cf[2 * S + s - 1]};
       if (j < n) fe = {fe.x + 0.5 * cf[s], fe.y + 0.5 * cf[S + s], fe.z + 0.5 * cf[2 * S + s]};
     }
+    if (nf) fe = {fe.x + nf[s], fe.y + nf[S + s], fe.z + nf[2 * S + s]};
     const V3 f = getv(sc.fl, j);
     const double im = 1.0 / m;  // InvMass, WithRodKinematics.hpp:411-424
     const V3 a = {(f.x + fe.x) * im, (f.y + fe.y) * im, (f.z + fe.z) * im};
@@ -367,6 +371,13 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
       double q[9];
       load_q(R.Q, S, s, q);
       const V3 tc = matvec(q, {ct[s], ct[S + s], ct[2 * S + s]});
+      te = {te.x + tc.x, te.y + tc.y, te.z + tc.z};
+    }
+    if (nt) {
+      // the connections' torque, summed in the lab frame, recast the same way
+      double q[9];
+      load_q(R.Q, S, s, q);
+      const V3 tc = matvec(q, {nt[s], nt[S + s], nt[2 * S + s]});
       te = {te.x + tc.x, te.y + tc.y, te.z + tc.z};
     }
     if (i == n - 1) te = {te.x + tend.x, te.y + tend.y, te.z + tend.z};
@@ -958,6 +969,74 @@ int check_contact(const OrcRods& R, const OrcContact* C) {
   return 0;
 }
 
+// ---- connections between rods -------------------------------------------
+// The joints of the reference's hinge-joint example
+// (examples/hinge_joint/HingeJointCaseStudy.cpp:96-150), connecting rod a at
+// index i to rod b at index j:
+//   force:  d = x_b[j] - x_a[i + 1];  F = k d - nu ((v_b[j] - v_a[i + 1]) . u) u,
+//           u = d / |d| (Blaze's normalize: d times 1/|d|, or d times 0 for
+//           |d| = 0);  rod a's node i + 1 gains F, rod b's node j loses it;
+//   torque (hinge only): l = x_b[j + 1] - x_b[j];  f = -k_rot (l . n) n;
+//           tau = l x f;  rod a's element i loses Q_a tau, rod b's element j
+//           gains Q_b tau (material frame).
+// Loads are summed per slot in connection order, each connection adding to
+// rod a before rod b; torques are summed in the lab frame and recast by the
+// element's directors in compute_dynamics.
+void connection_loads(const OrcRods& R, const OrcConnections& C, double* nf, double* nt) {
+  const int64_t S = R.n_slots;
+  std::fill(nf, nf + 3 * S, 0.0);
+  std::fill(nt, nt + 3 * S, 0.0);
+  const Field x{R.x, S}, v{R.v, S};
+  auto add = [&](double* a, int64_t s, V3 f, bool minus) {
+    if (minus) {
+      a[s] = a[s] - f.x;
+      a[S + s] = a[S + s] - f.y;
+      a[2 * S + s] = a[2 * S + s] - f.z;
+    } else {
+      a[s] = a[s] + f.x;
+      a[S + s] = a[S + s] + f.y;
+      a[2 * S + s] = a[2 * S + s] + f.z;
+    }
+  };
+  for (int64_t c = 0; c < C.n; ++c) {
+    const int64_t na = R.offset[C.rod_a[c]] + C.index_a[c] + 1, nb = R.offset[C.rod_b[c]] + C.index_b[c];
+    const V3 d = sub(x.get(nb), x.get(na));
+    const double k = C.k[c], nu = C.nu[c];
+    const V3 fel = {k * d.x, k * d.y, k * d.z};
+    const double len = std::sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+    const double il = len != 0.0 ? 1.0 / len : len;
+    const V3 u = {d.x * il, d.y * il, d.z * il};
+    const V3 dv = sub(v.get(nb), v.get(na));
+    const double vr = dv.x * u.x + dv.y * u.y + dv.z * u.z;
+    const V3 vel = {vr * u.x, vr * u.y, vr * u.z};
+    const double mnu = -nu;
+    const V3 F = {fel.x + mnu * vel.x, fel.y + mnu * vel.y, fel.z + mnu * vel.z};
+    add(nf, na, F, false);
+    add(nf, nb, F, true);
+    if (C.kind[c] == 1) {
+      const V3 l = sub(x.get(nb + 1), x.get(nb));
+      const V3 n = {C.normal[3 * c], C.normal[3 * c + 1], C.normal[3 * c + 2]};
+      const double s = (-C.k_rot[c]) * (l.x * n.x + l.y * n.y + l.z * n.z);
+      const V3 f = {s * n.x, s * n.y, s * n.z};
+      const V3 tau = {l.y * f.z - l.z * f.y, l.z * f.x - l.x * f.z, l.x * f.y - l.y * f.x};
+      add(nt, na - 1, tau, true);
+      add(nt, nb, tau, false);
+    }
+  }
+}
+
+int check_connections(const OrcRods& R, const OrcConnections* C) {
+  if (!C) return 0;
+  for (int64_t c = 0; c < C->n; ++c) {
+    const int64_t ra = C->rod_a[c], rb = C->rod_b[c];
+    if (ra < 0 || ra >= R.n_rods || rb < 0 || rb >= R.n_rods) return -1;
+    const int64_t na = R.offset[ra + 1] - R.offset[ra] - 1, nb = R.offset[rb + 1] - R.offset[rb] - 1;
+    if (C->index_a[c] < 0 || C->index_a[c] >= na || C->index_b[c] < 0) return -1;
+    if (C->kind[c] == 1 ? C->index_b[c] >= nb : C->index_b[c] > nb) return -1;
+  }
+  return 0;
+}
+
 // positions after a drift of c and the clamp's value constraint (a copy)
 std::vector<double> drifted_positions(const OrcRods& R, double c) {
   const int64_t S = R.n_slots;
@@ -1007,17 +1086,28 @@ extern "C" int orc_step(const OrcRods* rods, double dt, int64_t n_steps, int n_t
 
 extern "C" int orc_step_contact(const OrcRods* rods, const OrcContact* contact, double dt, int64_t n_steps,
                                 int n_threads) {
+  if (!contact) return -1;
+  return orc_step_loads(rods, contact, nullptr, dt, n_steps, n_threads);
+}
+
+extern "C" int orc_step_loads(const OrcRods* rods, const OrcContact* contact, const OrcConnections* conns,
+                              double dt, int64_t n_steps, int n_threads) {
   if (check(rods) != 0) return -1;
   const OrcRods& R = *rods;
-  if (check_contact(R, contact) != 0) return -1;
-  const OrcContact& C = *contact;
+  if (contact && check_contact(R, contact) != 0) return -1;
+  if (check_connections(R, conns) != 0) return -1;
+  const bool has_conn = conns && conns->n > 0;
 #ifdef _OPENMP
   const int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
 #else
   const int nt = 1;
 #endif
   const int64_t S = R.n_slots;
-  std::vector<double> cf(3 * S, 0.0), ct(3 * S, 0.0);
+  std::vector<double> cf(3 * S, 0.0), ct(3 * S, 0.0), jf, jt;  // contact; connection loads
+  if (has_conn) {
+    jf.assign(3 * S, 0.0);
+    jt.assign(3 * S, 0.0);
+  }
   ContactWorld W;
   std::vector<int64_t> pairs;
   for (int64_t step = 0; step < n_steps; ++step) {
@@ -1030,13 +1120,17 @@ extern "C" int orc_step_contact(const OrcRods* rods, const OrcContact* contact, 
       kinematic_half(R, r, dt);
       clamp_values(R, r);
     }
-    build_capsules(R, C, W, R.x);
-    pairs_grid(R, W, pairs);
-    contact_loads(R, C, W, pairs, cf.data(), ct.data(), nt);
-    if (step == n_steps - 1 && C.capsule_force && C.capsule_torque) {
-      std::copy(cf.begin(), cf.end(), C.capsule_force);
-      std::copy(ct.begin(), ct.end(), C.capsule_torque);
+    if (contact) {
+      const OrcContact& C = *contact;
+      build_capsules(R, C, W, R.x);
+      pairs_grid(R, W, pairs);
+      contact_loads(R, C, W, pairs, cf.data(), ct.data(), nt);
+      if (step == n_steps - 1 && C.capsule_force && C.capsule_torque) {
+        std::copy(cf.begin(), cf.end(), C.capsule_force);
+        std::copy(ct.begin(), ct.end(), C.capsule_torque);
+      }
     }
+    if (has_conn) connection_loads(R, *conns, jf.data(), jt.data());
 #ifdef _OPENMP
 #pragma omp parallel num_threads(nt)
 #endif
@@ -1050,7 +1144,9 @@ extern "C" int orc_step_contact(const OrcRods* rods, const OrcContact* contact, 
         const int64_t n = R.offset[r + 1] - R.offset[r] - 1;
         acc.assign(3 * (n + 1), 0.0);
         alpha.assign(3 * (n + 1), 0.0);
-        compute_dynamics(R, r, sc, acc.data(), alpha.data(), cf.data(), ct.data());
+        compute_dynamics(R, r, sc, acc.data(), alpha.data(), contact ? cf.data() : nullptr,
+                         contact ? ct.data() : nullptr, has_conn ? jf.data() : nullptr,
+                         has_conn ? jt.data() : nullptr);
         if (step == n_steps - 1) write_diagnostics(R, r, sc, acc.data(), alpha.data());
         dynamic_update(R, r, dt, sc, acc.data(), alpha.data());
         kinematic_half(R, r, dt);

@@ -122,6 +122,33 @@ typedef struct OrcContact {
 int orc_step_contact(const OrcRods* rods, const OrcContact* contact, double dt, int64_t n_steps,
                      int n_threads);
 
+/* ---- connections (joints) between rods -----------------------------------
+ * Connection c joins rod_a at index_a to rod_b at index_b with the joint of
+ * the reference's hinge-joint example: kind 0 = translational spring (k) and
+ * dashpot along the separation (nu) between node index_a + 1 of rod a and
+ * node index_b of rod b; kind 1 adds the rotational spring (k_rot) that
+ * penalises the component of rod b's element index_b along `normal`, as a
+ * torque on element index_a of rod a and element index_b of rod b. */
+typedef struct OrcConnections {
+  int64_t n;
+  const int64_t* rod_a;
+  const int64_t* index_a;
+  const int64_t* rod_b;
+  const int64_t* index_b;
+  const int32_t* kind;
+  const double* k;
+  const double* nu;
+  const double* k_rot;
+  const double* normal; /* 3 * n */
+} OrcConnections;
+
+/* PositionVerlet steps with the collision system (contact, may be NULL) and
+ * the connections (may be NULL) evaluated at the drifted state of every
+ * dynamic substep; external loads in the order gravity, contact,
+ * connections (forces) and contact, connections, end torque (torques). */
+int orc_step_loads(const OrcRods* rods, const OrcContact* contact, const OrcConnections* connections, double dt,
+                   int64_t n_steps, int n_threads);
+
 /* Capsules of the current state after a kinematic drift of half_dt (0: as
  * is) and the clamp's value constraint, the way one step would build them:
  * out[k*S + s] for k = 0..14 = centre(3), length, radius, axis(3), AABB

@@ -31,7 +31,7 @@ def oracle_from_workload(wl, damped: bool = False, diagnostics: bool = False):
             rods.set_rod("v", r, wl.velocities[r])
         if wl.rest_curvature is not None:
             rods.set_rod("rest_kappa", r, wl.rest_curvature[r])
-        if wl.clamp:
+        if wl.clamp if isinstance(wl.clamp, bool) else wl.clamp[r]:
             rods.clamp[r] = 1
             rods.clamp_x[3 * r:3 * r + 3] = init["x"][:, 0]
             rods.clamp_Q[9 * r:9 * r + 9] = init["Q"][:, :, 0].ravel()
@@ -136,6 +136,40 @@ def oracle_spread_contact(wl, n_steps):
         p = oracle_from_workload(wl)
         p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
         oracle.contact_step(p, contact_spec(wl), wl.dt, n_steps)
+        for name, k, place in STATE_FIELDS:
+            spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
+    return base, spread
+
+
+def connection_spec(wl):
+    """The oracle's description of a workload's connections (None if none)."""
+    from elasticapp_b200.simulator import HingeJoint
+    if not wl.connections:
+        return None
+    rows = []
+    for ra, ia, rb, ib, j in wl.connections:
+        hinge = isinstance(j, HingeJoint)
+        rows.append((ra, ia, rb, ib, 1 if hinge else 0, j.stiffness, j.damping,
+                     j.rotational_stiffness if hinge else 0.0, j.normal if hinge else (0.0, 0.0, 0.0)))
+    return oracle.ConnectionSpec(rows)
+
+
+def loads_step(rods, wl, n_steps):
+    oracle.loads_step(rods, contact_spec(wl), connection_spec(wl), wl.dt, n_steps)
+
+
+def oracle_spread_loads(wl, n_steps):
+    """oracle_spread for a workload with connections and/or contact
+    (orc_step_loads)."""
+    from elasticapp_b200.simulator import CosseratRod
+    damped = wl.model is CosseratRod
+    base = oracle_from_workload(wl, damped=damped)
+    loads_step(base, wl, n_steps)
+    spread = {name: 0.0 for name, _, _ in STATE_FIELDS}
+    for key in ("x", "Q"):
+        p = oracle_from_workload(wl, damped=damped)
+        p.arrays[key] = np.nextafter(p.arrays[key], np.inf)
+        loads_step(p, wl, n_steps)
         for name, k, place in STATE_FIELDS:
             spread[name] = max(spread[name], max_rel_error_per_rod(p.comp(k), base.comp(k), wl.n_elements, place))
     return base, spread
