@@ -562,26 +562,37 @@ def main(argv=None) -> int:
 
     # ---- end to end through the public API with host buffers: each cycle
     # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE
-    # steps and reads the state back (the reference's run_for + communicate)
-    S = sim.n_slots()
+    # steps and reads the state back (the reference's run_for + communicate),
+    # on a simulator with the default plan (chosen by timing at its first
+    # step, which runs untimed before the cycles)
     names = ("Position", "Velocity", "Director", "AngularVelocity")
     ncomp = {"Position": 3, "Velocity": 3, "Director": 9, "AngularVelocity": 3}
-    host = {n: torch.empty((ncomp[n], S), dtype=torch.float64, pin_memory=True).numpy() for n in names}
-    for n in names:
-        sim.get_slots(n, out=host[n])
+    e2e_plan = None
+    if args.e2e_cycles > 0:
+        esim = wl.build(device=local)
+        estream = torch.cuda.ExternalStream(esim.stream_handle(), device=torch.device("cuda", local))
+        S = esim.n_slots()
+        host = {n: torch.empty((ncomp[n], S), dtype=torch.float64, pin_memory=True).numpy() for n in names}
+        for n in names:
+            esim.get_slots(n, out=host[n])
+        te = esim.step(eb.PositionVerlet(), 0.0, wl.dt, E2E_STEPS_PER_CYCLE)
+        e2e_plan = esim.step_plan()["mode"]
+    else:
+        esim, estream, S = sim, stream, sim.n_slots()
+        host = {n: np.zeros((ncomp[n], S)) for n in names}
     bytes_cycle = sum(8 * ncomp[n] * S for n in names)
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    e0.record(estream)
     for _ in range(max(args.e2e_cycles, 0)):
         for n in names:
-            sim.set_slots(n, host[n])
-        t = sim.step(eb.PositionVerlet(), t, wl.dt, E2E_STEPS_PER_CYCLE)
+            esim.set_slots(n, host[n])
+        te = esim.step(eb.PositionVerlet(), te, wl.dt, E2E_STEPS_PER_CYCLE)
         for n in names:
-            sim.get_slots(n, out=host[n])
-    e1.record(stream)
+            esim.get_slots(n, out=host[n])
+    e1.record(estream)
     torch.cuda.synchronize()
     barrier()
     e2e_ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
@@ -590,6 +601,8 @@ def main(argv=None) -> int:
     e2e_value = (total_elems * E2E_STEPS_PER_CYCLE * args.e2e_cycles / (float(e2e_ms.item()) / 1e3)
                  if args.e2e_cycles > 0 else None)
     finite = all(np.isfinite(host[n]).all() for n in names)
+    if esim is not sim:
+        esim.close()
 
     # ---- the resident (batched) form of the same step on the same workload
     batched = None
@@ -663,7 +676,7 @@ def main(argv=None) -> int:
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cycle,
                     "d2h_bytes_per_step": bytes_cycle, "steps_per_e2e_step": E2E_STEPS_PER_CYCLE,
-                    "cycles": args.e2e_cycles},
+                    "cycles": args.e2e_cycles, "plan": e2e_plan},
             "gpu_launches": launches,
             "clocks": clock_info,
             "state_finite": bool(finite),

@@ -708,9 +708,9 @@ EB_API eb_status eb_set_field(eb_sim* s, int64_t rod, int32_t field, const doubl
   if (fi->kind == kState) {
     // keep the other ping-pong buffer consistent for the unused slot entries
     double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi->offset) * s->stride;
-    EB_CUDA(cudaMemcpy2DAsync(other + s->offsets[rod], s->stride * sizeof(double), values,
-                              per * sizeof(double), per * sizeof(double), fi->ncomp,
-                              cudaMemcpyHostToDevice, s->stream));
+    EB_CUDA(cudaMemcpy2DAsync(other + s->offsets[rod], s->stride * sizeof(double), base + s->offsets[rod],
+                              s->stride * sizeof(double), per * sizeof(double), fi->ncomp,
+                              cudaMemcpyDeviceToDevice, s->stream));
   }
   EB_CUDA(cudaStreamSynchronize(s->stream));
   return EB_OK;
@@ -762,8 +762,10 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
     if (to_device) {
       EB_CUDA(cudaMemcpy2DAsync(base, pitch, host, w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
       if (fi.kind == kState) {
+        // the other ping-pong buffer gets the same values on the device (its
+        // entries that no step writes must match), not by a second upload
         double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi.offset) * s->stride;
-        EB_CUDA(cudaMemcpy2DAsync(other, pitch, host, w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+        EB_CUDA(cudaMemcpy2DAsync(other, pitch, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToDevice, s->stream));
       }
     } else {
       EB_CUDA(cudaMemcpy2DAsync(host, w, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToHost, s->stream));
@@ -797,7 +799,7 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
   EB_CUDA(cudaMemcpy2DAsync(base, pitch, tmp.data(), w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
   if (fi.kind == kState) {
     double* other = s->d_state[s->cur ^ 1] + static_cast<int64_t>(fi.offset) * s->stride;
-    EB_CUDA(cudaMemcpy2DAsync(other, pitch, tmp.data(), w, w, fi.ncomp, cudaMemcpyHostToDevice, s->stream));
+    EB_CUDA(cudaMemcpy2DAsync(other, pitch, base, pitch, w, fi.ncomp, cudaMemcpyDeviceToDevice, s->stream));
   }
   EB_CUDA(cudaStreamSynchronize(s->stream));
   return EB_OK;
@@ -1356,11 +1358,37 @@ cudaError_t launch_bucket(eb_sim* s, eb::StepArgs& a, int b, int config, int ste
                                           s->any_damped, s->stream);
 }
 
+// Predicted time of kProbeSteps steps of a resident launch sequence when it
+// runs in launches of `chunk` steps: runs of kProbeSteps and 3 kProbeSteps
+// steps (after a warm-up) give the per-step cost and the fixed cost of a
+// launch (staging the state and writing it back), so a probe of a few steps
+// does not charge a 128-step launch with its staging eight times over.
+extern "C++" {
+template <class Launch>
+eb_status time_resident(eb_sim* s, cudaEvent_t e0, cudaEvent_t e1, int chunk, Launch launch, float* ms_out) {
+  float t[2] = {0.0f, 0.0f};
+  const int steps[2] = {kProbeSteps, 3 * kProbeSteps};
+  EB_CUDA(launch(kProbeSteps));  // warm-up
+  for (int i = 0; i < 2; ++i) {
+    EB_CUDA(cudaEventRecord(e0, s->stream));
+    EB_CUDA(launch(steps[i]));
+    EB_CUDA(cudaEventRecord(e1, s->stream));
+    EB_CUDA(cudaEventSynchronize(e1));
+    EB_CUDA(cudaEventElapsedTime(&t[i], e0, e1));
+  }
+  const float per = std::max(0.0f, (t[1] - t[0]) / static_cast<float>(steps[1] - steps[0]));
+  const float fixed = std::max(0.0f, t[0] - per * static_cast<float>(steps[0]));
+  *ms_out = per * kProbeSteps + fixed * static_cast<float>(kProbeSteps) / static_cast<float>(std::max(1, chunk));
+  return EB_OK;
+}
+}  // extern "C++"
+
 // Per-size-bucket plan: when the batch has rods of two or more buckets, or
 // rods of 520 to 1039 elements (and none longer), time every configuration on
 // each bucket alone for kProbeSteps steps into the spare buffer; *total_ms =
 // the sum of the buckets' best times, or -1 when the plan does not apply.
-eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cudaEvent_t e1, float* total_ms) {
+eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cudaEvent_t e1, int chunk,
+                        float* total_ms) {
   *total_ms = -1.0f;
   for (const auto& r : s->rods)
     if (bucket_of(r.n + 1) < 0) return EB_OK;
@@ -1376,14 +1404,9 @@ eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cud
     const int n_cfg = b == 2 ? kPairConfigs : eb::block_config_count();
     for (int c = 0; c < n_cfg; ++c) {
       if (!s->buckets[b].d_off[b == 2 ? 0 : c]) continue;
-      for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
-        EB_CUDA(cudaEventRecord(e0, s->stream));
-        EB_CUDA(launch_bucket(s, a, b, c, kProbeSteps));
-        EB_CUDA(cudaEventRecord(e1, s->stream));
-        EB_CUDA(cudaEventSynchronize(e1));
-      }
       float ms = 0.0f;
-      EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (eb_status st = time_resident(s, e0, e1, chunk, [&](int k) { return launch_bucket(s, a, b, c, k); }, &ms))
+        return st;
       s->plan_ms[5 + 4 * b + c] = ms;
       if (s->bucket_config[b] < 0 || ms < best) {
         best = ms;
@@ -1406,7 +1429,9 @@ int bucket_plan_config(const eb_sim* s) {
 // Choose between the streaming kernel and the resident configurations by
 // timing each for kProbeSteps steps from the current state into the spare
 // buffer (the current state is left untouched).
-eb_status plan_steps(eb_sim* s, double dt) {
+// chunk: steps per resident launch the first call would run (its step count,
+// at most kResidentChunk); the resident probes are compared at that length.
+eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   // contact needs a global exchange every step, PEFRL four force evaluations
   // a step: the streaming kernel
   const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
@@ -1438,7 +1463,7 @@ eb_status plan_steps(eb_sim* s, double dt) {
   bool bucket_done = false;
   if (s->cfg.flags & EB_FLAG_STEP_BUCKETED) {
     bucket_done = true;
-    if (eb_status st = probe_buckets(s, a, e0, e1, &bucket_ms)) return st;
+    if (eb_status st = probe_buckets(s, a, e0, e1, chunk, &bucket_ms)) return st;
     if (bucket_ms >= 0.0f) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -1454,18 +1479,19 @@ eb_status plan_steps(eb_sim* s, double dt) {
   for (int c = -1; c < eb::block_config_count(); ++c) {
     if (c >= 0 && !s->d_cta_start[c]) continue;
     if (c < 0 && force_resident) continue;
-    for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
-      EB_CUDA(cudaEventRecord(e0, s->stream));
-      if (c < 0) {
-        for (int k = 0; k < kProbeSteps; ++k) EB_CUDA(launch_streaming(s, a, false));
-      } else {
-        EB_CUDA(launch_resident(s, a, c, kProbeSteps));
-      }
-      EB_CUDA(cudaEventRecord(e1, s->stream));
-      EB_CUDA(cudaEventSynchronize(e1));
-    }
     float ms = 0.0f;
-    EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (c < 0) {
+      for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
+        EB_CUDA(cudaEventRecord(e0, s->stream));
+        for (int k = 0; k < kProbeSteps; ++k) EB_CUDA(launch_streaming(s, a, false));
+        EB_CUDA(cudaEventRecord(e1, s->stream));
+        EB_CUDA(cudaEventSynchronize(e1));
+      }
+      EB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    } else if (eb_status st = time_resident(s, e0, e1, chunk, [&](int k) { return launch_resident(s, a, c, k); },
+                                            &ms)) {
+      return st;
+    }
     s->plan_ms[c + 1] = ms;
     if (best_cfg == -1 && best_mode == 1 && best == 0.0f) {
       best = ms;
@@ -1480,7 +1506,7 @@ eb_status plan_steps(eb_sim* s, double dt) {
   if (best_mode == 2 && best_cfg < 0) best_mode = 1;
   // per size bucket: keep the best pair if it beats the plans above
   if (!bucket_done) {
-    if (eb_status st = probe_buckets(s, a, e0, e1, &bucket_ms)) return st;
+    if (eb_status st = probe_buckets(s, a, e0, e1, chunk, &bucket_ms)) return st;
     // (mixed precision: the streaming kernel was not timed, so any bucket
     // plan beats the FP64 fallback)
     const bool have_best = best_cfg >= 0 || !force_resident;
@@ -1647,7 +1673,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     s->damper_dt = dt;
   }
   if (s->plan_mode == 0)
-    if (eb_status st = plan_steps(s, dt)) return st;
+    if (eb_status st = plan_steps(s, dt, static_cast<int>(std::min<int64_t>(n_steps, kResidentChunk)))) return st;
   const bool diag = s->d_diag != nullptr;
   if (s->contact.on || s->jd.on) {
     if (eb_status st = step_with_contact(s, dt, n_steps, diag)) return st;

@@ -362,9 +362,12 @@ EB_API eb_status eb_snapshot_load(struct eb_sim* sim, const void* buffer, uint64
  * at most 263 elements) with configuration config % 4, bucket 1 (264 to 519)
  * with (config / 4) % 4, bucket 2 (520 to 1039 elements, each rod on a
  * cluster of two CTAs) with config / 16 (0: 512, 1: 256 threads per CTA).
- * probe_ms[0] is the streaming probe time, probe_ms[1 + c] configuration c's
- * on the whole batch, probe_ms[5 + 4 b + c] configuration c's on bucket b
- * alone (up to count entries; untimed entries are 0). */
+ * probe_ms[0] is the time of 8 streaming steps; probe_ms[1 + c] the predicted
+ * time of 8 steps of configuration c on the whole batch, and probe_ms[5 + 4 b
+ * + c] on bucket b alone, when run in launches of the first eb_step call's
+ * step count (at most 128): resident runs of 8 and 24 steps separate the
+ * per-step cost from the launch's fixed staging cost (up to count entries;
+ * untimed entries are 0). */
 EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* config, float* probe_ms,
                               int32_t count);
 
