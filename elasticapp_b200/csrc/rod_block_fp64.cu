@@ -13,7 +13,8 @@
 // per-slot data lives in shared-memory rows, so any thread count works.
 //
 // Step structure: the same substeps as the streaming kernel, including both
-// half drifts of every step.  (Merging the second half drift of step k with
+// half drifts of every step, in two phases with one barrier after each (see
+// the step loop).  (Merging the second half drift of step k with
 // the first of step k+1 into one full drift is not an identity here: the
 // reference normalises the rotation axis by theta + 1e-14, so one update by
 // dt differs from two by dt/2 by ~1e-14 per step, which the stiff rod modes
@@ -192,50 +193,62 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
 
   const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
 
-  for (int step = 0; step < n_steps; ++step) {
-    // ---- drift: half on the first step; afterwards the merged full drift,
-    // or (kSplit) the first half drift, the second half of the previous step
-    // having been applied at the end of its update phase
-    const double c = (step == 0 || kSplit) ? hdt : dt;
-    for (int s = tid; s < count; s += kThreads) {
-      const uint32_t meta = meta_s[s];
-      const D3 v = R.get3(bV, s);
-      D3 x = R.get3(bX, s);
-      x = {x.x + c * v.x, x.y + c * v.y, x.z + c * v.z};
-      double q[9];
-      if (meta & kElem) {
+  // drift of slot s by c (x += c v, Q <- exp(-c [w]x) Q), then, with
+  // `clamp`, the clamp's value constraint on a clamped rod's first slot
+  auto drift = [&](int s, uint32_t meta, double c, bool clamp) {
+    const D3 v = R.get3(bV, s);
+    D3 x = R.get3(bX, s);
+    x = {x.x + c * v.x, x.y + c * v.y, x.z + c * v.z};
+    double q[9];
+    if (meta & kElem) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
-        const D3 w = R.get3(bW, s);
-        so3_update_fast(q, c * w.x, c * w.y, c * w.z);
-      }
-      if (any_rod && (meta & kFirst)) {
-        const RodInfo& ri = a.rods[meta >> kRodShift];
-        if (ri.flags & kRodClamp) {
-          x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+      for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
+      const D3 w = R.get3(bW, s);
+      so3_update_fast(q, c * w.x, c * w.y, c * w.z);
+    }
+    if (clamp && any_rod && (meta & kFirst)) {
+      const RodInfo& ri = a.rods[meta >> kRodShift];
+      if (ri.flags & kRodClamp) {
+        x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
 #pragma unroll
-          for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
-        }
-      }
-      R.put3(bX, s, x);
-      if (meta & kElem) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
+        for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
       }
     }
-    sync_neighbours();
+    R.put3(bX, s, x);
+    if (meta & kElem) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
+    }
+  };
+  // length of element s, rounded as written (so the copy a Voronoi point
+  // recomputes for its next element equals the element's own)
+  auto elem_length = [&](int s) -> double {
+    const D3 dx = nb3(bX, s + 1) - nb3(bX, s);
+    return sqrt(__fma_rn(dx.z, dx.z, __fma_rn(dx.y, dx.y, __dmul_rn(dx.x, dx.x))));
+  };
 
-    // ---- element geometry, internal stress, element-local torque terms
+  // ---- first half drift of the first step and the clamp's value constraint
+  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], hdt, true);
+  sync_neighbours();
+
+  // Two phases per step, one barrier after each: (1) element s (geometry,
+  // strain, stress, element-local torque terms) and Voronoi point s
+  // (curvature and couple, with the next element's length recomputed rather
+  // than exchanged); (2) loads, torques, kick and rate constraints, then the
+  // second half drift of this step and the first half drift of the next
+  // (kept apart: merging them into one rotation is not an identity under the
+  // 1e-14 axis guard).
+  for (int step = 0; step < n_steps; ++step) {
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       D3 f{0.0, 0.0, 0.0}, tl{0.0, 0.0, 0.0};
       double l = 1.0, e = 1.0;
+      double q[9];
       if (meta & kElem) {
-        double q[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
         const D3 dx = nb3(bX, s + 1) - R.get3(bX, s);
-        l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
+        l = elem_length(s);
         const double il = 1.0 / l;
         const D3 t = {dx.x * il, dx.y * il, dx.z * il};
         const double l0 = R.at(bL0, s);
@@ -254,27 +267,17 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
         const double rate = dot(t, dv) / (e * l0);
         tl = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
       }
-      R.at(bL, s) = l;
       R.at(bE, s) = e;
       R.put3(bF, s, f);
       R.put3(bTl, s, tl);
-    }
-    sync_neighbours();
-
-    // ---- Voronoi curvature and couple
-    for (int s = tid; s < count; s += kThreads) {
-      const uint32_t meta = meta_s[s];
       D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
       if (meta & kVor) {
-        double qc[9], qn[9];
+        double qn[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          qc[k] = R.at(bQ + k, s);
-          qn[k] = nb(bQ + k, s + 1);
-        }
+        for (int k = 0; k < 9; ++k) qn[k] = nb(bQ + k, s + 1);
         const double D0 = R.at(bD0, s);
-        const D3 kappa = inv_rotate_divide_fast(qc, qn, D0);
-        const double eps = 0.5 * (R.at(bL, s) + nb(bL, s + 1)) / D0;
+        const D3 kappa = inv_rotate_divide_fast(q, qn, D0);
+        const double eps = 0.5 * (l + elem_length(s + 1)) / D0;
         const double ic = 1.0 / (eps * eps * eps);
         const D3 dk = kappa - R.get3(bKap0, s);
         const D3 B = R.get3(bBend, s);
@@ -344,27 +347,19 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       }
       R.put3(bV, s, v);
       if (meta & kElem) R.put3(bW, s, w);
-      if (kSplit && step + 1 < n_steps) {
-        // second half drift of this step, own slot only
-        D3 x = R.get3(bX, s);
-        R.put3(bX, s, D3{x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z});
-        if (meta & kElem) {
-          double q[9];
-#pragma unroll
-          for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
-          so3_update_fast(q, hdt * w.x, hdt * w.y, hdt * w.z);
-#pragma unroll
-          for (int k = 0; k < 9; ++k) R.at(bQ + k, s) = q[k];
+      if (step + 1 < n_steps) {
+        if (kSplit) {
+          drift(s, meta, hdt, false);  // second half of this step, own slot
+          drift(s, meta, hdt, true);   // first half of the next
+        } else {
+          drift(s, meta, dt, true);
         }
       }
     }
-    // the next step's drift reads only its own slot; a pair's partner must
-    // not leave (and free its rows) while this CTA still reads them
-    if (step + 1 < n_steps) {
-      __syncthreads();
-    } else {
-      sync_neighbours();
-    }
+    // the next phase reads the neighbours' drifted state; for a pair, the
+    // partner must also not leave (and free its rows) while this CTA still
+    // reads them
+    sync_neighbours();
   }
 
   // ---- final half drift and write-back
