@@ -7,9 +7,10 @@
 // element-step falls by the number of steps per launch and the step becomes
 // arithmetic-bound.
 //
-// Work list: CTA c owns the consecutive slots [cta_start[c], cta_start[c+1]),
-// always a whole number of rods (the host packs rods into CTAs of at most
-// kCap slots).  Every phase loops its threads over the CTA's slots; all
+// Work list: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),
+// always whole rods (the host packs rods best fit decreasing into CTAs of at
+// most kCap slots; serving launches read consecutive slot ranges from a CTA
+// table instead).  Every phase loops its threads over the CTA's slots; all
 // per-slot data lives in shared-memory rows, so any thread count works.
 //
 // Step structure: the same substeps as the streaming kernel, including both
@@ -438,16 +439,8 @@ int block_config_capacity(int config) {
   return (config >= 0 && config < kNumConfigs) ? kBlockConfigs[config][0] : 0;
 }
 
-cudaError_t launch_rod_block_fp64(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
-                                  int config, bool damped, cudaStream_t stream) {
-  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  switch (config) {
-    case 0: return launch_block_cfg<520, 512, true>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 1: return launch_block_cfg<520, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 2: return launch_block_cfg<264, 256, true>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 3: return launch_block_cfg<264, 288, true>(args, cta_start, n_ctas, n_steps, damped, stream);
-    default: return cudaErrorInvalidValue;
-  }
+int block_config_threads(int config) {
+  return (config >= 0 && config < kNumConfigs) ? kBlockConfigs[config][1] : 0;
 }
 
 // Serving launches (see launch_rod_block_mixed_serve): 520-slot CTAs in a

@@ -548,21 +548,6 @@ cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int
 
 }  // namespace
 
-cudaError_t launch_rod_block_mixed(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps,
-                                   int config, bool damped, cudaStream_t stream) {
-  if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
-  // the same capacities as the FP64 resident configurations (0/1: 520 slots,
-  // 2/3: 264 slots); 376 B of shared memory per slot allows two CTAs per SM
-  // at 264 slots
-  switch (config) {
-    case 0: return launch_mixed_cfg<520, 512, 1>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 1: return launch_mixed_cfg<520, 256, 1>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 2: return launch_mixed_cfg<264, 256, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
-    case 3: return launch_mixed_cfg<264, 288, 2>(args, cta_start, n_ctas, n_steps, damped, stream);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 // Serving launches: CTA c runs serve[c] (its request's slot range, time step,
 // environment and min(n_steps, serve[c].steps) steps); 520-slot CTAs.
 // A cluster launch (n_ctas even) in which entries 2i and 2i + 1 may hold the
@@ -585,8 +570,10 @@ cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* ct
   }
 }
 
-// Gathered CTAs: CTA c owns the slots gmap[cta_start[c] .. cta_start[c + 1]),
-// whole rods in slot order (the per-size-bucket plans).
+// Resident launches: CTA c owns the slots gmap[cta_start[c] .. cta_start[c +
+// 1]), whole rods (the host packs them best fit decreasing).  The same
+// capacities as the FP64 resident configurations (0/1: 520 slots, 2/3: 264
+// slots); 376 B of shared memory per slot allows two CTAs per SM at 264.
 cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
                                           int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
