@@ -56,6 +56,12 @@ namespace {
 
 constexpr int64_t kBin = 520;                 // slots per bin (one CTA)
 constexpr int64_t kPairSlots = 2 * kBin;      // a rod longer than a bin: two adjacent bins (a CTA pair)
+// Packing fills a bin to at most 512 slots and a bin pair to 1024: the
+// serving CTAs run 512 threads, and one slot more gives some threads a
+// second round in every phase.  A single rod longer than that fills its unit
+// alone.
+constexpr int64_t kBinFill = 512;
+constexpr int64_t kPairFill = 2 * kBinFill;
 constexpr int64_t kRodsPerBin = kBin / 3;     // a rod takes at least 3 slots
 constexpr size_t kArenaBytes = size_t(1) << 30;  // pinned result arena
 constexpr size_t kUploadBytes = size_t(1) << 28;  // pinned staging of admitted requests' initial data
@@ -286,8 +292,8 @@ void server_free(eb_server* s) {
 // Placement units of the request, best fit decreasing: rods in order of
 // decreasing length; a rod longer than a bin opens a bin pair (1040 slots,
 // run by a CTA pair, which may split any rod of the unit); a shorter rod goes
-// to the unit with the least room that still holds it, else opens a single
-// bin.
+// to the unit with the least room (below the fill limits above) that still
+// holds it, else opens a single bin.
 void pack(Request& r) {
   r.bins.clear();
   r.bin_count.clear();
@@ -302,7 +308,7 @@ void pack(Request& r) {
   for (size_t k : order) {
     const int64_t w = r.rods[k].n_elements + 1;
     int64_t u = -1;
-    if (w <= kBin) {
+    if (w <= kBinFill) {
       auto it = room.lower_bound(w);
       if (it != room.end()) {
         u = it->second;
@@ -317,7 +323,7 @@ void pack(Request& r) {
     r.rod_bin[k] = u;
     r.rod_off[k] = r.bin_count[u];
     r.bin_count[u] += static_cast<int32_t>(w);
-    const int64_t left = (r.bin_pair[u] ? kPairSlots : kBin) - r.bin_count[u];
+    const int64_t left = (r.bin_pair[u] ? kPairFill : kBinFill) - r.bin_count[u];
     if (left >= 3) room.emplace(left, u);  // a rod takes at least 3 slots
   }
 }
