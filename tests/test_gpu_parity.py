@@ -186,10 +186,14 @@ def test_explicitly_damped_rods_vs_oracle(step_mode):
     assert within(errs, bounds), (errs, bounds)
 
 
-@pytest.mark.parametrize("lengths", [[1000], [255, 1, 300], [2, 2, 2, 2, 2], [254], [255], [256], [600, 2, 511]])
+@pytest.mark.parametrize("lengths", [[1000], [255, 1, 300], [2, 2, 2, 2, 2], [254], [255], [256], [600, 2, 511],
+                                     [511, 512, 519, 2, 7, 250, 261]])
 def test_tile_and_rod_boundaries(lengths):
     """Rods that span several 256-slot tiles, end exactly on tile edges, or
-    are minimal (2 elements).  A length of 1 in the list is replaced by 2."""
+    are minimal (2 elements); rods that fill a resident CTA's 512-slot packing
+    limit exactly (511 elements), pass it (512) or fill its 520-slot capacity
+    (519), beside short rods the packing puts into the remainders.  A length
+    of 1 in the list is replaced by 2."""
     lengths = [max(2, n) for n in lengths]
     rng = np.random.default_rng(len(lengths) * 1000 + sum(lengths))
     rods = []
