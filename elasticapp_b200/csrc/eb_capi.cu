@@ -599,7 +599,7 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
   if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.stepper != EB_STEPPER_PEFRL)
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown time stepper");
   if (cfg.stepper == EB_STEPPER_PEFRL && cfg.precision == EB_PRECISION_MIXED)
-    return fail(EB_ERR_UNSUPPORTED, "PEFRL runs on the FP64 streaming kernel only");
+    return fail(EB_ERR_UNSUPPORTED, "PEFRL runs in FP64 only");
   if (cfg.flags & ~static_cast<uint32_t>(EB_FLAG_RECORD_DIAGNOSTICS | EB_FLAG_REFERENCE_ROUNDING |
                                           EB_FLAG_STEP_STREAMING | EB_FLAG_STEP_RESIDENT | EB_FLAG_CUDA_GRAPH |
                                           EB_FLAG_STEP_BUCKETED))
@@ -1252,6 +1252,20 @@ const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0},
                            {1.0 - 2.0 * (kPefrlChi + kPefrlXi), kPefrlLambda, 0.0},
                            {kPefrlChi, 0.5 * (1.0 - 2.0 * kPefrlLambda), kPefrlXi}};
 
+int substeps(const eb_sim* s, const Substep** table);
+
+// the substep table of the simulator's stepper, for the resident kernels
+void set_substeps(const eb_sim* s, eb::StepArgs& a) {
+  const Substep* sub;
+  const int ns = substeps(s, &sub);
+  a.n_sub = ns;
+  for (int j = 0; j < ns; ++j) {
+    a.sub_pre[j] = sub[j].pre;
+    a.sub_kick[j] = sub[j].kick;
+  }
+  a.sub_post = sub[ns - 1].post;
+}
+
 int substeps(const eb_sim* s, const Substep** table) {
   if (s->cfg.stepper == EB_STEPPER_PEFRL) {
     *table = kPefrl;
@@ -1480,7 +1494,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   // contact needs a global exchange every step, PEFRL four force evaluations
   // a step: the streaming kernel
   const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
-                            s->contact.on || s->jd.on || s->cfg.stepper == EB_STEPPER_PEFRL;
+                            s->contact.on || s->jd.on;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -1500,6 +1514,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   EB_CUDA(cudaEventCreate(&e0));
   EB_CUDA(cudaEventCreate(&e1));
   eb::StepArgs a = step_args(s, dt);
+  set_substeps(s, a);  // the resident kernels take the stepper's substeps
   a.in = s->d_state[s->cur];
   a.out = s->d_state[s->cur ^ 1];
   float best = 0.0f;
@@ -1730,6 +1745,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     return EB_OK;
   }
   eb::StepArgs a = step_args(s, dt);
+  set_substeps(s, a);  // the resident kernels take the stepper's substeps
   int64_t done = 0;
   if (s->plan_mode == 2 || s->plan_mode == 3) {
     // resident kernel in chunks; the last step of a call that records

@@ -102,6 +102,13 @@ struct StepArgs {
   double drift_pre;
   double kick;
   double drift_post;
+  // substeps of one step for the resident kernels, in units of dt: the drift
+  // before each force evaluation, each kick, and the drift after the last
+  // kick; n_sub 0 or 1 means PositionVerlet (0.5, 1, 0.5), 4 is PEFRL
+  int32_t n_sub;
+  double sub_pre[4];
+  double sub_kick[4];
+  double sub_post;
   double gravity[3];
   uint32_t sim_flags;   // kSim* below
   // capsule contact loads of this step (lab frame, 3 x stride each, per

@@ -228,18 +228,27 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
     return sqrt(__fma_rn(dx.z, dx.z, __fma_rn(dx.y, dx.y, __dmul_rn(dx.x, dx.x))));
   };
 
-  // ---- first half drift of the first step and the clamp's value constraint
-  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], hdt, true);
+  // Substeps: PositionVerlet (drift dt/2, kick dt, drift dt/2), or PEFRL's
+  // four kicks with their drifts (StepArgs::sub_*, in units of dt; serving
+  // launches are PositionVerlet).
+  const bool pefrl = !kServe && a.n_sub > 1;
+  const int nsub = pefrl ? a.n_sub : 1;
+
+  // ---- first drift of the first step and the clamp's value constraint
+  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], pefrl ? a.sub_pre[0] * dt : hdt, true);
   sync_neighbours();
 
-  // Two phases per step, one barrier after each: (1) element s (geometry,
-  // strain, stress, element-local torque terms) and Voronoi point s
-  // (curvature and couple, with the next element's length recomputed rather
-  // than exchanged); (2) loads, torques, kick and rate constraints, then the
-  // second half drift of this step and the first half drift of the next
-  // (kept apart: merging them into one rotation is not an identity under the
-  // 1e-14 axis guard).
-  for (int step = 0; step < n_steps; ++step) {
+  // Two phases per force evaluation, one barrier after each: (1) element s
+  // (geometry, strain, stress, element-local torque terms) and Voronoi point
+  // s (curvature and couple, with the next element's length recomputed
+  // rather than exchanged); (2) loads, torques, kick and rate constraints,
+  // then the drift before the next force evaluation (after the last kick of
+  // a step: its closing drift and the next step's first, kept apart: merging
+  // them into one rotation is not an identity under the 1e-14 axis guard).
+  for (int step = 0; step < n_steps; ++step)
+  for (int sub = 0; sub < nsub; ++sub) {
+    const double kc = pefrl ? a.sub_kick[sub] : 1.0;  // this kick, in units of dt
+    const double kdt = pefrl ? kc * dt : dt;
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       D3 f{0.0, 0.0, 0.0}, tl{0.0, 0.0, 0.0};
@@ -305,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       }
       if (flags & kSimGravity) F = F + D3{gvec[0] * m, gvec[1] * m, gvec[2] * m};
       const double im = 1.0 / m;
-      v = {v.x + dt * (F.x * im), v.y + dt * (F.y * im), v.z + dt * (F.z * im)};
+      v = {v.x + kdt * (F.x * im), v.y + kdt * (F.y * im), v.z + kdt * (F.z * im)};
       D3 w{0.0, 0.0, 0.0};
       const RodInfo* ri = any_rod ? a.rods + (meta >> kRodShift) : nullptr;
       if (meta & kElem) {
@@ -329,13 +338,13 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
           T = T + matvec(q, D3{ri->end_torque[0], ri->end_torque[1], ri->end_torque[2]});
         }
         const D3 ji = R.get3(bJinv, s);
-        w = {w.x + dt * (ji.x * T.x * e), w.y + dt * (ji.y * T.y * e), w.z + dt * (ji.z * T.z * e)};
+        w = {w.x + kdt * (ji.x * T.x * e), w.y + kdt * (ji.y * T.y * e), w.z + kdt * (ji.z * T.z * e)};
         if (any_rod && (ri->flags & kRodDamper)) {
           const double mn = nb(bMass, s + 1);
           double em = 0.5 * (m + mn);
           if (first) em += 0.5 * m;
           if (meta & kLastElem) em += 0.5 * mn;
-          const double y = -ri->damper_r * em * dt * e;
+          const double y = -ri->damper_r * em * kdt * e;
           w = {w.x * exp(y * ji.x), w.y * exp(y * ji.y), w.z * exp(y * ji.z)};
         }
       }
@@ -344,12 +353,18 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
           v = D3{0.0, 0.0, 0.0};
           w = D3{0.0, 0.0, 0.0};
         }
-        if (ri->flags & kRodDamper) v = scale(v, ri->damper_t);
+        // exp(-nu_t dt) for a kick of dt; a fractional kick scales the exponent
+        if (ri->flags & kRodDamper) v = scale(v, kc == 1.0 ? ri->damper_t : exp(log(ri->damper_t) * kc));
       }
       R.put3(bV, s, v);
       if (meta & kElem) R.put3(bW, s, w);
-      if (step + 1 < n_steps) {
-        if (kSplit) {
+      if (sub + 1 < nsub) {
+        drift(s, meta, a.sub_pre[sub + 1] * dt, true);  // before the next force evaluation
+      } else if (step + 1 < n_steps) {
+        if (pefrl) {
+          drift(s, meta, a.sub_post * dt, false);  // closing drift of this step, own slot
+          drift(s, meta, a.sub_pre[0] * dt, true);  // first drift of the next
+        } else if (kSplit) {
           drift(s, meta, hdt, false);  // second half of this step, own slot
           drift(s, meta, hdt, true);   // first half of the next
         } else {
@@ -363,13 +378,14 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
     sync_neighbours();
   }
 
-  // ---- final half drift and write-back
+  // ---- closing drift of the last step and write-back
+  const double fin = pefrl ? a.sub_post * dt : hdt;
   for (int s = tid; s < count; s += kThreads) {
     const uint32_t meta = meta_s[s];
     const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
     const D3 v = R.get3(bV, s);
     D3 x = R.get3(bX, s);
-    x = {x.x + hdt * v.x, x.y + hdt * v.y, x.z + hdt * v.z};
+    x = {x.x + fin * v.x, x.y + fin * v.y, x.z + fin * v.z};
     a.out[kStX * S + g] = x.x;
     a.out[(kStX + 1) * S + g] = x.y;
     a.out[(kStX + 2) * S + g] = x.z;
@@ -381,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
 #pragma unroll
       for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
       const D3 w = R.get3(bW, s);
-      so3_update_fast(q, hdt * w.x, hdt * w.y, hdt * w.z);
+      so3_update_fast(q, fin * w.x, fin * w.y, fin * w.z);
 #pragma unroll
       for (int k = 0; k < 9; ++k) a.out[(kStQ + k) * S + g] = q[k];
       a.out[kStW * S + g] = w.x;

@@ -76,7 +76,8 @@ typedef enum eb_precision {
                                            128 steps per launch) when the rods
                                            fit; by default the first eb_step
                                            times both and keeps the faster */
-#define EB_FLAG_CUDA_GRAPH 0x10u       /* streaming steps (without contact)
+#define EB_FLAG_CUDA_GRAPH 0x10u       /* streaming steps (without contact or
+                                           connections)
                                            replayed from a captured CUDA graph
                                            of 32 steps: one graph launch
                                            instead of 32 (128 with PEFRL)
@@ -107,7 +108,9 @@ typedef struct eb_config {
  * xi = 0.1786178958448091, lambda = -0.2123418310626054,
  * chi = -0.06626458266981849, value constraints after every drift and rate
  * constraints after every kick (the damper's factors for the kick's share of
- * dt).  PEFRL runs on the FP64 streaming kernel. */
+ * dt).  PEFRL runs in FP64, on the streaming kernel (four launches a step)
+ * or on the resident kernels (four force evaluations a step on chip), as the
+ * step plan chooses. */
 typedef enum eb_stepper { EB_STEPPER_POSITION_VERLET = 0, EB_STEPPER_PEFRL = 1 } eb_stepper;
 
 /* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and

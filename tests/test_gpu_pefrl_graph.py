@@ -1,9 +1,10 @@
 """PEFRL and CUDA-graph replay on the GPU.
 
-* PEFRL on the streaming kernel against the oracle's PEFRL (the reference
-  declares the stepper without implementing it): the FP64 parity rule after
-  200 steps with clamp, damper and gravity, and fourth-order convergence on
-  free rods.
+* PEFRL on the streaming kernel (four launches a step) and on the resident
+  kernel (four force evaluations a step on chip) against the oracle's PEFRL
+  (the reference declares the stepper without implementing it): the FP64
+  parity rule after 200 steps with clamp, damper and gravity, and
+  fourth-order convergence on free rods.
 * Steps replayed from a captured CUDA graph give bit-identical states to
   the same steps launched one by one, for PositionVerlet and PEFRL, with a
   recorded last step, and after a change of dt (a new capture).
@@ -28,29 +29,52 @@ def W():
     return workloads
 
 
-def test_pefrl_parity_with_oracle(eb, W):
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_pefrl_parity_with_oracle(eb, W, step_mode):
     wl = W.uneven_batch(n_rods=12, seed=7, n_range=(20, 90))
     steps = 200
     base, spread = oracle_spread(wl, steps, stepper="pefrl")
     bounds = parity_bounds(spread)
-    sim = wl.build(stepper=eb.PEFRL())
+    sim = wl.build(stepper=eb.PEFRL(), step_mode=step_mode)
     sim.step(eb.PEFRL(), 0.0, wl.dt, steps)
     want = state_slots(base)
     for name, place in (("Position", 0), ("Velocity", 0), ("Director", 1), ("AngularVelocity", 1)):
         err = max_rel_error_per_rod(sim.get_slots(name), want[name], wl.n_elements, place)
         assert err <= bounds[name], (name, err, bounds[name])
-    assert sim.step_plan()["mode"] == "streaming"
+    assert sim.step_plan()["mode"] == step_mode
     sim.close()
 
 
-def test_pefrl_fourth_order_on_gpu(eb, W):
+def test_pefrl_resident_long_rods_and_chunks(eb, W):
+    """PEFRL on the bucketed resident plan (rods on CTA pairs included), in
+    chunks that split launches differently, against the streaming kernel."""
+    wl = W.uneven_batch(n_rods=6, seed=12, n_range=(100, 900))
+    a = wl.build(stepper=eb.PEFRL(), step_mode="bucketed")
+    b = wl.build(stepper=eb.PEFRL(), step_mode="bucketed")
+    ref = wl.build(stepper=eb.PEFRL(), step_mode="streaming")
+    a.step(eb.PEFRL(), 0.0, wl.dt, 300)
+    for k in (130, 170):
+        b.step(eb.PEFRL(), 0.0, wl.dt, k)
+    ref.step(eb.PEFRL(), 0.0, wl.dt, 300)
+    assert a.step_plan()["mode"] == "bucketed"
+    for name in ("Position", "Director", "Velocity", "AngularVelocity"):
+        assert np.array_equal(a.get_slots(name), b.get_slots(name)), name
+    for name in ("Position", "Director"):
+        x, y = a.get_slots(name), ref.get_slots(name)
+        assert np.max(np.abs(x - y)) <= 1e-10 * max(1.0, np.max(np.abs(y))), name
+    for s in (a, b, ref):
+        s.close()
+
+
+@pytest.mark.parametrize("step_mode", ["streaming", "resident"])
+def test_pefrl_fourth_order_on_gpu(eb, W, step_mode):
     wl = W.uneven_batch(n_rods=4, seed=3, n_range=(20, 40))
     wl.damper = None
     wl.clamp = False
     horizon = 800 * wl.dt
 
     def run(f):
-        sim = wl.build(stepper=eb.PEFRL())
+        sim = wl.build(stepper=eb.PEFRL(), step_mode=step_mode)
         dt = wl.dt * f
         sim.step(eb.PEFRL(), 0.0, dt, int(round(horizon / dt)))
         x = sim.get_slots("Position").copy()
