@@ -632,6 +632,31 @@ def main(argv=None) -> int:
                    "kernel": "rod_block_fp64 (whole rods resident in shared memory, up to 128 steps per launch)"}
         bsim.close()
         sim = None
+        # the same batch with PEFRL (four force evaluations a step): the
+        # default plan against the streaming kernel (four launches a step)
+        pefrl = {}
+        for mode in ("auto", "streaming"):
+            psim = wl.build(device=local, stepper=eb.PEFRL(), step_mode=mode)
+            tp = psim.step(eb.PEFRL(), 0.0, wl.dt, 128)  # plan + warm-up
+            pstream = torch.cuda.ExternalStream(psim.stream_handle(), device=torch.device("cuda", local))
+            n_p = 128 if mode == "auto" else 32
+            barrier()
+            torch.cuda.synchronize()
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            p0.record(pstream)
+            tp = psim.step(eb.PEFRL(), tp, wl.dt, n_p)
+            p1.record(pstream)
+            torch.cuda.synchronize()
+            barrier()
+            pms = torch.tensor([p0.elapsed_time(p1)], device="cuda")
+            if pg is not None:
+                pg.all_reduce(pms, op=pg.ReduceOp.MAX)
+            pefrl[mode] = {"value": total_elems * n_p / (float(pms.item()) / 1e3), "steps": n_p,
+                           "ms_per_step": float(pms.item()) / n_p, "plan": psim.step_plan()["mode"]}
+            psim.close()
+        batched["pefrl"] = {"unit": UNIT, "force_evaluations_per_step": 4, "default_plan": pefrl["auto"],
+                            "streaming": pefrl["streaming"]}
 
     # ---- mixed precision: the mixed batch on the FP64 streaming drop-in and
     # on the mixed-precision resident kernel, tip positions compared

@@ -1243,9 +1243,9 @@ eb_status build_block_worklists(eb_sim* s) {
 struct Substep {
   double pre, kick, post;
 };
-constexpr double kPefrlXi = 0.1786178958448091;
-constexpr double kPefrlLambda = -0.2123418310626054;
-constexpr double kPefrlChi = -0.06626458266981849;
+using eb::kPefrlChi;
+using eb::kPefrlLambda;
+using eb::kPefrlXi;
 const Substep kVerlet[1] = {{0.5, 1.0, 0.5}};
 const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0},
                            {kPefrlChi, kPefrlLambda, 0.0},
@@ -1254,16 +1254,10 @@ const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0},
 
 int substeps(const eb_sim* s, const Substep** table);
 
-// the substep table of the simulator's stepper, for the resident kernels
+// the stepper's force evaluations per step, for the resident kernels
 void set_substeps(const eb_sim* s, eb::StepArgs& a) {
   const Substep* sub;
-  const int ns = substeps(s, &sub);
-  a.n_sub = ns;
-  for (int j = 0; j < ns; ++j) {
-    a.sub_pre[j] = sub[j].pre;
-    a.sub_kick[j] = sub[j].kick;
-  }
-  a.sub_post = sub[ns - 1].post;
+  a.n_sub = substeps(s, &sub);
 }
 
 int substeps(const eb_sim* s, const Substep** table) {
@@ -1541,9 +1535,19 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
     if (c < 0 && force_resident) continue;
     float ms = 0.0f;
     if (c < 0) {
+      // whole steps: one launch per substep (four for PEFRL)
+      const Substep* sub;
+      const int ns = substeps(s, &sub);
       for (int rep = 0; rep < 2; ++rep) {  // first repetition warms up
         EB_CUDA(cudaEventRecord(e0, s->stream));
-        for (int k = 0; k < kProbeSteps; ++k) EB_CUDA(launch_streaming(s, a, false));
+        for (int k = 0; k < kProbeSteps; ++k)
+          for (int j = 0; j < ns; ++j) {
+            eb::StepArgs b = a;
+            b.drift_pre = sub[j].pre * dt;
+            b.kick = sub[j].kick * dt;
+            b.drift_post = sub[j].post * dt;
+            EB_CUDA(launch_streaming(s, b, false));
+          }
         EB_CUDA(cudaEventRecord(e1, s->stream));
         EB_CUDA(cudaEventSynchronize(e1));
       }

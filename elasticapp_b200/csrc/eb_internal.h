@@ -102,13 +102,9 @@ struct StepArgs {
   double drift_pre;
   double kick;
   double drift_post;
-  // substeps of one step for the resident kernels, in units of dt: the drift
-  // before each force evaluation, each kick, and the drift after the last
-  // kick; n_sub 0 or 1 means PositionVerlet (0.5, 1, 0.5), 4 is PEFRL
+  // force evaluations per step for the resident kernels: 0 or 1 is
+  // PositionVerlet, 4 is PEFRL (coefficients below)
   int32_t n_sub;
-  double sub_pre[4];
-  double sub_kick[4];
-  double sub_post;
   double gravity[3];
   uint32_t sim_flags;   // kSim* below
   // capsule contact loads of this step (lab frame, 3 x stride each, per
@@ -126,6 +122,13 @@ struct StepArgs {
 // slots, the right CTA the rest, and neighbour reads across the split go to
 // the partner's shared memory.
 constexpr int kPairMaxSlots = 1040;  // two 520-slot halves
+
+// PEFRL (Omelyan, Mryglod and Folk, Comput. Phys. Commun. 146 (2002)
+// 188-202): drifts xi, chi, 1 - 2 (chi + xi), chi, xi around the kicks
+// (1 - 2 lambda) / 2, lambda, lambda, (1 - 2 lambda) / 2, in units of dt.
+constexpr double kPefrlXi = 0.1786178958448091;
+constexpr double kPefrlLambda = -0.2123418310626054;
+constexpr double kPefrlChi = -0.06626458266981849;
 
 // Per-CTA work of the serving launches (resident kernels): the CTA's slot
 // range, its step count for this launch and the time step and environment of

@@ -108,7 +108,9 @@ __device__ __forceinline__ int param_row(int f) {
 // kPair: cluster launch of CTA pairs; with kServe, CTAs 2i and 2i + 1 form a
 // pair when both serve entries say so and run the same step count, and are
 // single CTAs otherwise; without kServe every cluster is a pair
-template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false, bool kPair = false>
+// kPefrl: PEFRL's four force evaluations a step (PositionVerlet otherwise)
+template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false, bool kPair = false,
+          bool kPefrl = false>
 __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
                                                                     int n_steps_launch, const ServeCta* serve,
                                                                     const int32_t* gmap) {
@@ -229,13 +231,17 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   };
 
   // Substeps: PositionVerlet (drift dt/2, kick dt, drift dt/2), or PEFRL's
-  // four kicks with their drifts (StepArgs::sub_*, in units of dt; serving
-  // launches are PositionVerlet).
-  const bool pefrl = !kServe && a.n_sub > 1;
-  const int nsub = pefrl ? a.n_sub : 1;
+  // four kicks with their drifts (in units of dt; compile-time constants)
+  constexpr int nsub = kPefrl ? 4 : 1;
+  auto pefrl_pre = [](int j) -> double {  // drift before force evaluation j
+    return j == 0 ? kPefrlXi : (j == 2 ? 1.0 - 2.0 * (kPefrlChi + kPefrlXi) : kPefrlChi);
+  };
+  auto pefrl_kick = [](int j) -> double {
+    return (j == 0 || j == 3) ? 0.5 * (1.0 - 2.0 * kPefrlLambda) : kPefrlLambda;
+  };
 
   // ---- first drift of the first step and the clamp's value constraint
-  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], pefrl ? a.sub_pre[0] * dt : hdt, true);
+  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], kPefrl ? kPefrlXi * dt : hdt, true);
   sync_neighbours();
 
   // Two phases per force evaluation, one barrier after each: (1) element s
@@ -247,8 +253,8 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   // them into one rotation is not an identity under the 1e-14 axis guard).
   for (int step = 0; step < n_steps; ++step)
   for (int sub = 0; sub < nsub; ++sub) {
-    const double kc = pefrl ? a.sub_kick[sub] : 1.0;  // this kick, in units of dt
-    const double kdt = pefrl ? kc * dt : dt;
+    const double kc = kPefrl ? pefrl_kick(sub) : 1.0;  // this kick, in units of dt
+    const double kdt = kPefrl ? kc * dt : dt;
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       D3 f{0.0, 0.0, 0.0}, tl{0.0, 0.0, 0.0};
@@ -359,11 +365,11 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
       R.put3(bV, s, v);
       if (meta & kElem) R.put3(bW, s, w);
       if (sub + 1 < nsub) {
-        drift(s, meta, a.sub_pre[sub + 1] * dt, true);  // before the next force evaluation
+        drift(s, meta, pefrl_pre(sub + 1) * dt, true);  // before the next force evaluation
       } else if (step + 1 < n_steps) {
-        if (pefrl) {
-          drift(s, meta, a.sub_post * dt, false);  // closing drift of this step, own slot
-          drift(s, meta, a.sub_pre[0] * dt, true);  // first drift of the next
+        if (kPefrl) {
+          drift(s, meta, kPefrlXi * dt, false);  // closing drift of this step, own slot
+          drift(s, meta, kPefrlXi * dt, true);   // first drift of the next
         } else if (kSplit) {
           drift(s, meta, hdt, false);  // second half of this step, own slot
           drift(s, meta, hdt, true);   // first half of the next
@@ -379,7 +385,7 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
   }
 
   // ---- closing drift of the last step and write-back
-  const double fin = pefrl ? a.sub_post * dt : hdt;
+  const double fin = kPefrl ? kPefrlXi * dt : hdt;
   for (int s = tid; s < count; s += kThreads) {
     const uint32_t meta = meta_s[s];
     const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
@@ -435,6 +441,11 @@ cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int
       return cudaGetLastError();
     }
   };
+  if constexpr (!kServe) {  // serving launches are PositionVerlet
+    if (args.n_sub > 1)
+      return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair, true>)
+                    : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair, true>);
+  }
   return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair>)
                 : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair>);
 }
