@@ -7,6 +7,7 @@ snapshot; object files go to ``elasticapp_b200/_build/`` (git-ignored).
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -68,7 +69,7 @@ def _stale(target: str, deps: list[str]) -> bool:
 def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "elastica_b200.h")]
-    objs = []
+    objs, cmds = [], []
     for oname, src, extra in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, oname)
@@ -79,7 +80,13 @@ def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True) 
                 cmd += ["-Xptxas", "-v"]
             if not quiet:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # the translation units compile independently: one nvcc per core
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
+        for done in pool.map(lambda c: subprocess.run(c, check=False), cmds):
+            if done.returncode != 0:
+                raise subprocess.CalledProcessError(done.returncode, done.args)
     if force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + host_compiler() + ["-shared", "-cudart", "static", "-o", LIB] + objs
         if not quiet:
