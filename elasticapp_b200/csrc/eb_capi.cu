@@ -200,15 +200,18 @@ struct eb_sim {
     int n_ctas[4] = {0, 0, 0, 0};
     int64_t rods = 0;
   };
-  Bucket buckets[3];
-  int bucket_config[3] = {-1, -1, -1};
+  // bucket 3: buckets 0 and 1 packed together (used in their place when
+  // faster; built when the batch also has pair rods)
+  Bucket buckets[4];
+  int bucket_config[4] = {-1, -1, -1, -1};
+  bool bucket_merged = false;
   // whole-batch resident plan, per block configuration (or null): CTA c owns
   // the slots d_gmap[d_cta_start[c] .. d_cta_start[c + 1]); configurations
   // packed the same way share their lists
   std::vector<int64_t*> d_cta_start;
   std::vector<int32_t*> d_gmap;
   std::vector<int> n_ctas;
-  float plan_ms[16] = {0};
+  float plan_ms[20] = {0};
   // captured streaming steps: per starting buffer parity, for graph_dt
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double graph_dt[2] = {0.0, 0.0};
@@ -1347,10 +1350,19 @@ int bucket_of(int64_t w) {
 
 eb_status build_bucket_worklists(eb_sim* s) {
   if (s->buckets[0].rods + s->buckets[1].rods + s->buckets[2].rods > 0) return EB_OK;  // built already
-  for (int b = 0; b < 3; ++b) {
+  int64_t count[3] = {0, 0, 0};
+  for (const auto& r : s->rods) {
+    const int b = bucket_of(r.n + 1);
+    if (b >= 0) ++count[b];
+  }
+  const bool merge = count[0] > 0 && count[1] > 0 && count[2] > 0;
+  for (int b = 0; b < 4; ++b) {
+    if (b == 3 && !merge) continue;
     std::vector<size_t> rods;
-    for (size_t r = 0; r < s->rods.size(); ++r)
-      if (bucket_of(s->rods[r].n + 1) == b) rods.push_back(r);
+    for (size_t r = 0; r < s->rods.size(); ++r) {
+      const int rb = bucket_of(s->rods[r].n + 1);
+      if (rb == b || (b == 3 && (rb == 0 || rb == 1))) rods.push_back(r);
+    }
     s->buckets[b].rods = static_cast<int64_t>(rods.size());
     if (rods.empty()) continue;
     if (b == 2) {
@@ -1449,8 +1461,8 @@ eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cud
   const int used = (s->buckets[0].rods > 0) + (s->buckets[1].rods > 0) + (s->buckets[2].rods > 0);
   if (used < 2 && s->buckets[2].rods == 0) return EB_OK;
   eb::StepArgs a = args;
-  float total = 0.0f;
-  for (int b = 0; b < 3; ++b) {
+  float best_of[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int b = 0; b < 4; ++b) {
     s->bucket_config[b] = -1;
     if (s->buckets[b].rods == 0) continue;
     float best = 0.0f;
@@ -1460,20 +1472,26 @@ eb_status probe_buckets(eb_sim* s, const eb::StepArgs& args, cudaEvent_t e0, cud
       float ms = 0.0f;
       if (eb_status st = time_resident(s, e0, e1, chunk, [&](int k) { return launch_bucket(s, a, b, c, k); }, &ms))
         return st;
-      s->plan_ms[5 + 4 * b + c] = ms;
+      s->plan_ms[b == 3 ? 16 + c : 5 + 4 * b + c] = ms;
       if (s->bucket_config[b] < 0 || ms < best) {
         best = ms;
         s->bucket_config[b] = c;
       }
     }
-    if (s->bucket_config[b] < 0) return EB_OK;
-    total += best;
+    if (s->bucket_config[b] < 0 && b != 3) return EB_OK;
+    best_of[b] = best;
   }
-  *total_ms = total;
+  // buckets 0 and 1 apart, or packed together (bucket 3) when that is faster
+  const float apart = best_of[0] + best_of[1];
+  s->bucket_merged = s->bucket_config[3] >= 0 && best_of[3] < apart;
+  *total_ms = best_of[2] + (s->bucket_merged ? best_of[3] : apart);
   return EB_OK;
 }
 
+// bucket configurations as one number: c0 + 4 c1 + 16 c2, plus 64 (c3 + 1)
+// when buckets 0 and 1 run packed together (c0 = c1 = 0 then)
 int bucket_plan_config(const eb_sim* s) {
+  if (s->bucket_merged) return 16 * std::max(0, s->bucket_config[2]) + 64 * (s->bucket_config[3] + 1);
   int c = 0;
   for (int b = 2; b >= 0; --b) c = 4 * c + std::max(0, s->bucket_config[b]);
   return c;
@@ -1765,8 +1783,9 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
         ++s->launches;
       } else {
         // one launch per size bucket over the same buffers
-        for (int b = 0; b < 3; ++b) {
+        for (int b = 0; b < 4; ++b) {
           if (s->buckets[b].rods == 0) continue;
+          if (s->bucket_merged ? (b == 0 || b == 1) : b == 3) continue;
           EB_CUDA(launch_bucket(s, a, b, s->bucket_config[b], k));
           ++s->launches;
         }
@@ -1838,7 +1857,7 @@ EB_API eb_status eb_step_plan(const eb_sim* s, int32_t* mode, int32_t* config, f
   *mode = s->plan_mode;
   *config = s->plan_config;
   if (probe_ms)
-    for (int i = 0; i < count && i < 16; ++i) probe_ms[i] = s->plan_ms[i];
+    for (int i = 0; i < count && i < 20; ++i) probe_ms[i] = s->plan_ms[i];
   return EB_OK;
 }
 

@@ -412,8 +412,8 @@ class Simulator:
     def step_plan(self) -> dict:
         """The kernel plan chosen by the first step (see eb_step_plan)."""
         mode, cfg = ctypes.c_int32(), ctypes.c_int32()
-        ms = (ctypes.c_float * 16)()
-        L.call("eb_step_plan", self._h, ctypes.byref(mode), ctypes.byref(cfg), ms, 16)
+        ms = (ctypes.c_float * 20)()
+        L.call("eb_step_plan", self._h, ctypes.byref(mode), ctypes.byref(cfg), ms, 20)
         return {"mode": {0: "undecided", 1: "streaming", 2: "resident", 3: "bucketed"}[mode.value], "config": cfg.value,
                 "probe_ms": list(ms)}
 

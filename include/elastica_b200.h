@@ -364,10 +364,13 @@ EB_API eb_status eb_snapshot_load(struct eb_sim* sim, const void* buffer, uint64
  * per size bucket, one launch per bucket that holds rods: bucket 0 (rods of
  * at most 263 elements) with configuration config % 4, bucket 1 (264 to 519)
  * with (config / 4) % 4, bucket 2 (520 to 1039 elements, each rod on a
- * cluster of two CTAs) with config / 16 (0: 512, 1: 256 threads per CTA).
+ * cluster of two CTAs) with (config / 16) % 4 (0: 512, 1: 256 threads per
+ * CTA); config >= 64 means buckets 0 and 1 run packed together, with
+ * configuration config / 64 - 1, because that timed faster.
  * probe_ms[0] is the time of 8 streaming steps; probe_ms[1 + c] the predicted
  * time of 8 steps of configuration c on the whole batch, and probe_ms[5 + 4 b
- * + c] on bucket b alone, when run in launches of the first eb_step call's
+ * + c] on bucket b alone and probe_ms[16 + c] on buckets 0 and 1 together,
+ * when run in launches of the first eb_step call's
  * step count (at most 128): resident runs of 8 and 24 steps separate the
  * per-step cost from the launch's fixed staging cost (up to count entries;
  * untimed entries are 0). */
