@@ -456,7 +456,7 @@ cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int
 // rod a configuration can hold (n + 1 slots).
 namespace {
 // {slots per CTA, threads per CTA}
-constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {288, 288}, {264, 288}};
+constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {288, 288}, {320, 320}};
 constexpr int kNumConfigs = 4;
 }  // namespace
 
@@ -501,7 +501,7 @@ cudaError_t launch_rod_block_fp64_gather(const StepArgs& args, const int64_t* ct
     case 0: return launch_block_cfg<520, 512, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 1: return launch_block_cfg<520, 256, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 2: return launch_block_cfg<288, 288, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
-    case 3: return launch_block_cfg<264, 288, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 3: return launch_block_cfg<320, 320, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -16,9 +16,10 @@
 //
 // FP32 copies of the director and angular velocity are refreshed whenever
 // the FP64 values change, so each is converted once per step, and the
-// divisions of the element math are reciprocal square roots and stored
-// reciprocals: conversions and the special-function unit, not the FP32
-// arithmetic, bound this kernel otherwise.
+// divisions of the element math are reciprocal square roots and rounded
+// reciprocals (the reciprocals of the masses and Voronoi rest lengths are
+// formed each step rather than stored: shared memory per slot, not the
+// arithmetic, sets how many slots an SM holds).
 //
 // Reformulations (mathematically identical; rounding differs):
 //   sigma = (Q t) e - z  =  Q dx / l0 - z         (no normalisation)
@@ -62,12 +63,18 @@ using D3 = Vec3<double>;
 using F3 = Vec3<float>;
 
 // FP64 rows
-enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dDampT = 19, dSig0 = 20, dRowsD = 23 };
+enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dSig0 = 19, dRowsD = 22 };
+// shared-memory rows of FP32 values per slot
+template <bool kDamped>
+constexpr int mixed_rows_f() { return kDamped ? 44 : 42; }
+
 // FP32 rows
 enum MixedRowF : int {
-  fMass = 0, fInvMass = 1, fL0 = 2, fInvL0 = 3, fD0 = 4, fInvD0 = 5, fKap0 = 6, fShear = 9, fBend = 12,
-  fJ = 15, fJinv = 18, fNuF = 21, fNuT = 22,
-  fF = 23, fP = 26, fM = 29, fE = 32, fDampR = 33, fQ = 34, fW = 43, fRowsF = 46
+  fMass = 0, fL0 = 1, fD0 = 2, fKap0 = 3, fShear = 6, fBend = 9, fJ = 12, fJinv = 15,
+  fF = 18, fP = 21, fM = 24, fE = 27, fDampR = 28,
+  fDampC = 29,  // 1 - exp(-nu_t dt) of the rod's analytical damper
+  fQ = 30, fW = 39,
+  fNuF = 42, fNuT = 43  // explicit damping only: the last rows, not allocated for undamped rods
 };
 
 template <int kCap>
@@ -232,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                            const int32_t* gmap) {
   extern __shared__ __align__(128) double smem[];
   const MRows<kCap> R{smem, reinterpret_cast<float*>(smem + dRowsD * kCap)};
-  uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + fRowsF * kCap);
+  uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + mixed_rows_f<kDamped>() * kCap);
   uint32_t* rflag_s = meta_s + kCap;
 
   const int tid = threadIdx.x;
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       dr = static_cast<float>(ri.damper_r);
     }
     rflag_s[s] = rf;
-    R.ad(dDampT, s) = dtc;
+    R.af(fDampC, s) = static_cast<float>(1.0 - dtc);
     R.af(fDampR, s) = dr;
 #pragma unroll 1
     for (int f = 0; f < kStateFields; ++f) R.ad(f, s) = a.in[f * S + g];
@@ -315,7 +322,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     for (int k = 0; k < 3; ++k) R.af(fW + k, s) = static_cast<float>(R.ad(dW + k, s));
     const double il0 = 1.0 / a.par[kL0 * S + g];
     R.ad(dInvL0, s) = il0;
-    R.af(fInvL0, s) = static_cast<float>(il0);
     // the rest strain, with the unit axial strain of sigma = Q dx / l0 - z folded in
     R.ad(dSig0, s) = a.par[kSig0 * S + g];
     R.ad(dSig0 + 1, s) = a.par[(kSig0 + 1) * S + g];
@@ -326,8 +332,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       if (r < 0 || (!kDamped && (f == kNuF || f == kNuT))) continue;
       R.af(r, s) = static_cast<float>(a.par[f * S + g]);
     }
-    R.af(fInvMass, s) = static_cast<float>(1.0 / a.par[kMass * S + g]);
-    R.af(fInvD0, s) = static_cast<float>(1.0 / a.par[kD0 * S + g]);
   }
   __syncthreads();
 
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const float l = l2 * il;
         const F3 t = scale(dxf, il);
         const float l0 = R.af(fL0, s);
-        e = l * R.af(fInvL0, s);
+        e = l * static_cast<float>(il0);
         const float ie = l0 * il;
         const F3 sh = R.f3(fShear, s);
         const F3 nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
@@ -409,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
             ratio = 2.f * asinf(sqrtf(0.5f * y)) * rsqrtf(y * (2.f - y));
           }
           const float D0 = R.af(fD0, s);
-          const float st = 0.5f * ratio * R.af(fInvD0, s);
+          const float st = 0.5f * ratio * __frcp_rn(D0);
           const F3 d1{qf[0], qf[1], qf[2]}, d2{qf[3], qf[4], qf[5]}, d3{qf[6], qf[7], qf[8]};
           const F3 e1{dd[0], dd[1], dd[2]}, e2{dd[3], dd[4], dd[5]}, e3{dd[6], dd[7], dd[8]};
           const F3 skew = {dot(d3, e2) - dot(d2, e3), dot(d1, e3) - dot(d3, e1), dot(d2, e1) - dot(d1, e2)};
@@ -450,7 +454,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         F = {F.x - cf * vf.x, F.y - cf * vf.y, F.z - cf * vf.z};
       }
       if (flags & kSimGravity) F = F + F3{grav.x * m, grav.y * m, grav.z * m};
-      const float im = R.af(fInvMass, s);
+      const float im = __frcp_rn(m);
       v = {v.x + dt * static_cast<double>(F.x * im), v.y + dt * static_cast<double>(F.y * im),
            v.z + dt * static_cast<double>(F.z * im)};
       D3 w{0.0, 0.0, 0.0};
@@ -491,7 +495,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         v = D3{0.0, 0.0, 0.0};
         w = D3{0.0, 0.0, 0.0};
       }
-      if (rf & kRodDamper) v = scale(v, R.ad(dDampT, s));
+      if (rf & kRodDamper) v = scale(v, 1.0 - static_cast<double>(R.af(fDampC, s)));
       R.pd3(dV, s, v);
       if (meta & kElem) {
         R.pd3(dW, s, w);
@@ -516,7 +520,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 template <int kCap, int kThreads, int kMinBlocks, bool kServe = false, bool kGather = false, bool kPair = false>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
-  const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(fRowsF) * kCap * sizeof(float) +
+  const int rows_f = damped ? mixed_rows_f<true>() : mixed_rows_f<false>();
+  const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(rows_f) * kCap * sizeof(float) +
                        2 * size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -573,8 +578,8 @@ cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* ct
 // Resident launches: CTA c owns the slots gmap[cta_start[c] .. cta_start[c +
 // 1]), whole rods (the host packs them best fit decreasing).  The same
 // configurations as the FP64 resident kernel (0/1: 520 slots, 2: 288, 3:
-// 264); 376 B of shared memory per slot allows two CTAs per SM at 288 and
-// 264 slots.
+// 320); 352 B of shared memory per slot (360 with explicit damping) allows
+// two CTAs per SM at 288 and 320 slots.
 cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
                                           int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
@@ -582,7 +587,7 @@ cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* c
     case 0: return launch_mixed_cfg<520, 512, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 1: return launch_mixed_cfg<520, 256, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 2: return launch_mixed_cfg<288, 288, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
-    case 3: return launch_mixed_cfg<264, 288, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 3: return launch_mixed_cfg<320, 320, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     default: return cudaErrorInvalidValue;
   }
 }
