@@ -44,9 +44,8 @@ using D3 = Vec3<double>;
 enum BlockRow : int {
   bX = 0, bV = 3, bQ = 6, bW = 15,  // state (kStateFields rows)
   bMass = 18, bL0 = 19, bD0 = 20, bSig0 = 21, bKap0 = 24, bShear = 27, bBend = 30, bJ = 33, bJinv = 36,
-  bNuF = 39, bNuT = 40,             // explicit damping only
-  bL = 41, bE = 42, bF = 43, bG = 46, bH = 49, bTl = 52,  // per-step exchange rows
-  bRows = 55
+  bE = 39, bF = 40, bG = 43, bH = 46, bTl = 49,  // per-step exchange rows
+  bNuF = 52, bNuT = 53              // explicit damping only: the last rows, not allocated otherwise
 };
 
 template <int kCap>
@@ -109,14 +108,22 @@ __device__ __forceinline__ int param_row(int f) {
 // pair when both serve entries say so and run the same step count, and are
 // single CTAs otherwise; without kServe every cluster is a pair
 // kPefrl: PEFRL's four force evaluations a step (PositionVerlet otherwise)
+// FP64 shared-memory rows per slot
+template <bool kDamped>
+constexpr int block_rows() { return kDamped ? 54 : 52; }
+
+// two CTAs per SM for the CTAs of at most 264 slots (420 B a slot undamped)
+template <int kCap>
+constexpr int block_min_ctas() { return kCap <= 264 ? 2 : 1; }
+
 template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false, bool kPair = false,
           bool kPefrl = false>
-__global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
+__global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
                                                                     int n_steps_launch, const ServeCta* serve,
                                                                     const int32_t* gmap) {
   extern __shared__ __align__(128) double smem[];
   const BRows<kCap> R{smem};
-  uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + bRows * kCap);
+  uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + block_rows<kDamped>() * kCap);
 
   const int tid = threadIdx.x;
   int64_t g0;
@@ -416,7 +423,8 @@ __global__ void __launch_bounds__(kThreads, 1) rod_block_fp64_kernel(const StepA
 template <int kCap, int kThreads, bool kSplit, bool kServe = false, bool kGather = false, bool kPair = false>
 cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
-  const size_t bytes = size_t(bRows) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
+  const size_t bytes =
+      size_t(damped ? block_rows<true>() : block_rows<false>()) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
@@ -456,7 +464,7 @@ cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int
 // rod a configuration can hold (n + 1 slots).
 namespace {
 // {slots per CTA, threads per CTA}
-constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {288, 288}, {320, 320}};
+constexpr int kBlockConfigs[][2] = {{520, 512}, {520, 256}, {264, 256}, {320, 320}};
 constexpr int kNumConfigs = 4;
 }  // namespace
 
@@ -500,7 +508,7 @@ cudaError_t launch_rod_block_fp64_gather(const StepArgs& args, const int64_t* ct
   switch (config) {
     case 0: return launch_block_cfg<520, 512, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 1: return launch_block_cfg<520, 256, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
-    case 2: return launch_block_cfg<288, 288, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 2: return launch_block_cfg<264, 256, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 3: return launch_block_cfg<320, 320, true, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     default: return cudaErrorInvalidValue;
   }

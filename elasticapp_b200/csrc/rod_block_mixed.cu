@@ -577,16 +577,16 @@ cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* ct
 
 // Resident launches: CTA c owns the slots gmap[cta_start[c] .. cta_start[c +
 // 1]), whole rods (the host packs them best fit decreasing).  The same
-// configurations as the FP64 resident kernel (0/1: 520 slots, 2: 288, 3:
+// configurations as the FP64 resident kernel (0/1: 520 slots, 2: 264, 3:
 // 320); 352 B of shared memory per slot (360 with explicit damping) allows
-// two CTAs per SM at 288 and 320 slots.
+// two CTAs per SM at 264 and 320 slots.
 cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
                                           int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
   switch (config) {
     case 0: return launch_mixed_cfg<520, 512, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 1: return launch_mixed_cfg<520, 256, 1, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
-    case 2: return launch_mixed_cfg<288, 288, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
+    case 2: return launch_mixed_cfg<264, 256, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     case 3: return launch_mixed_cfg<320, 320, 2, false, true>(args, cta_start, n_ctas, n_steps, damped, stream, nullptr, gmap);
     default: return cudaErrorInvalidValue;
   }
