@@ -562,9 +562,11 @@ def main(argv=None) -> int:
 
     # ---- end to end through the public API with host buffers: each cycle
     # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE
-    # steps and reads the state back (the reference's run_for + communicate),
-    # on a simulator with the default plan (chosen by timing at its first
-    # step, which runs untimed before the cycles)
+    # steps and reads the state back (the reference's run_for + communicate)
+    # in one eb_step_host_state call, which overlaps the copies of each slot
+    # group with the steps of the others under a resident plan; a simulator
+    # with the default plan (chosen by timing at its first step) and one
+    # exchange (building the slot groups) run untimed before the cycles
     names = ("Position", "Velocity", "Director", "AngularVelocity")
     ncomp = {"Position": 3, "Velocity": 3, "Director": 9, "AngularVelocity": 3}
     e2e_plan = None
@@ -577,6 +579,7 @@ def main(argv=None) -> int:
             esim.get_slots(n, out=host[n])
         te = esim.step(eb.PositionVerlet(), 0.0, wl.dt, E2E_STEPS_PER_CYCLE)
         e2e_plan = esim.step_plan()["mode"]
+        te = esim.step_host_state(eb.PositionVerlet(), te, wl.dt, E2E_STEPS_PER_CYCLE, inputs=host, outputs=host)
     else:
         esim, estream, S = sim, stream, sim.n_slots()
         host = {n: np.zeros((ncomp[n], S)) for n in names}
@@ -587,11 +590,7 @@ def main(argv=None) -> int:
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(estream)
     for _ in range(max(args.e2e_cycles, 0)):
-        for n in names:
-            esim.set_slots(n, host[n])
-        te = esim.step(eb.PositionVerlet(), te, wl.dt, E2E_STEPS_PER_CYCLE)
-        for n in names:
-            esim.get_slots(n, out=host[n])
+        te = esim.step_host_state(eb.PositionVerlet(), te, wl.dt, E2E_STEPS_PER_CYCLE, inputs=host, outputs=host)
     e1.record(estream)
     torch.cuda.synchronize()
     barrier()
@@ -701,7 +700,7 @@ def main(argv=None) -> int:
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_cycle,
                     "d2h_bytes_per_step": bytes_cycle, "steps_per_e2e_step": E2E_STEPS_PER_CYCLE,
-                    "cycles": args.e2e_cycles, "plan": e2e_plan},
+                    "cycles": args.e2e_cycles, "plan": e2e_plan, "call": "eb_step_host_state"},
             "gpu_launches": launches,
             "clocks": clock_info,
             "state_finite": bool(finite),

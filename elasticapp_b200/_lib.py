@@ -108,6 +108,15 @@ class EbServerStats(ctypes.Structure):
                [("element_steps", ctypes.c_double), ("kernel_seconds", ctypes.c_double)]
 
 
+FIELD_NAME_SNAKE = {"Position": "position", "Velocity": "velocity", "Director": "director",
+                    "AngularVelocity": "angular_velocity"}
+
+
+class EbHostState(ctypes.Structure):
+    _fields_ = [(f"{n}_{d}", ctypes.c_void_p) for d in ("in", "out")
+                for n in ("position", "velocity", "director", "angular_velocity")]
+
+
 class EbJoint(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("stiffness", ctypes.c_double),
                 ("damping", ctypes.c_double), ("rotational_stiffness", ctypes.c_double),
@@ -153,6 +162,8 @@ SIGNATURES = {
     "eb_finalize": ([_sim], ctypes.c_int),
     "eb_step": ([_sim, _P(ctypes.c_double), ctypes.c_double, ctypes.c_int64], ctypes.c_int),
     "eb_synchronize": ([_sim], ctypes.c_int),
+    "eb_step_host_state": ([_sim, _P(ctypes.c_double), ctypes.c_double, ctypes.c_int64, _P(EbHostState)],
+                           ctypes.c_int),
     "eb_energy": ([_sim, _P(ctypes.c_double), ctypes.c_int64], ctypes.c_int),
     "eb_get_stream": ([_sim, _P(ctypes.c_void_p)], ctypes.c_int),
     "eb_step_plan": ([_sim, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_float), ctypes.c_int32], ctypes.c_int),

@@ -212,6 +212,22 @@ struct eb_sim {
   std::vector<int32_t*> d_gmap;
   std::vector<int> n_ctas;
   float plan_ms[20] = {0};
+  // host-state exchange (eb_step_host_state) under a resident plan: the rods
+  // split into contiguous slot groups, each packed on its own for the
+  // configuration xconfig, so one group's copies overlap another's launches;
+  // streams: copies in, copies out, launches of even and of odd groups;
+  // events: the start, per group its inputs landed and its steps done, the
+  // four streams' ends
+  struct XGroup {
+    int64_t lo = 0, hi = 0;  // slots [lo, hi)
+    int64_t* d_off = nullptr;
+    int32_t* d_map = nullptr;
+    int n_ctas = 0;
+  };
+  std::vector<XGroup> xgroups;
+  int xconfig = -1;
+  cudaStream_t xs[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> xev;
   // captured streaming steps: per starting buffer parity, for graph_dt
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double graph_dt[2] = {0.0, 0.0};
@@ -399,6 +415,12 @@ void host_free(eb_sim* s) {
       if (q) cudaFree(q);
     j = JointDevice{};
   }
+  for (auto& g : s->xgroups) {
+    if (g.d_off) cudaFree(g.d_off);
+    if (g.d_map) cudaFree(g.d_map);
+  }
+  s->xgroups.clear();
+  s->xconfig = -1;
   for (auto& b : s->buckets) {
     for (int c = 0; c < 4; ++c) {
       if (b.d_off[c]) cudaFree(b.d_off[c]);
@@ -626,7 +648,12 @@ EB_API eb_status eb_sim_destroy(eb_sim* s) {
   if (!s) return EB_OK;
   cudaSetDevice(s->cfg.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  for (cudaStream_t x : s->xs)
+    if (x) cudaStreamSynchronize(x);
   host_free(s);
+  for (cudaEvent_t e : s->xev) cudaEventDestroy(e);
+  for (cudaStream_t x : s->xs)
+    if (x) cudaStreamDestroy(x);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return EB_OK;
@@ -1737,6 +1764,77 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
   return EB_OK;
 }
 
+// the reference builds the damper's exponential constants once for the
+// simulation's dt (AnalyticalLinearDamper.hpp:40-57)
+eb_status damper_for_dt(eb_sim* s, double dt) {
+  if (!(s->sim_flags & eb::kSimDamper) || dt == s->damper_dt) return EB_OK;
+  for (auto& r : s->rods)
+    if (r.info.flags & eb::kRodDamper) r.info.damper_t = std::exp(-r.damper_nu_t * dt);
+  if (eb_status st = upload_rod_table(s)) return st;
+  s->damper_dt = dt;
+  return EB_OK;
+}
+
+// Slot groups of the host-state exchange for the resident configuration of
+// the plan: the rods in order cut into contiguous runs of about equal slot
+// counts, each packed best fit decreasing on its own (a group's CTAs touch
+// only its slots, so its launches need only its copies).  One group per six
+// waves of the configuration's CTAs, at most eight; a single group means no
+// overlap and the exchange runs its copies and steps in sequence.
+eb_status build_exchange_groups(eb_sim* s) {
+  const int c = s->plan_config;
+  if (s->xconfig == c && !s->xgroups.empty()) return EB_OK;
+  for (auto& g : s->xgroups) {
+    if (g.d_off) EB_CUDA(cudaFree(g.d_off));
+    if (g.d_map) EB_CUDA(cudaFree(g.d_map));
+  }
+  s->xgroups.clear();
+  s->xconfig = c;
+  int sms = 0;
+  EB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device));
+  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * pack_fill(c) * 6;
+  const int64_t n_groups = std::min<int64_t>(8, std::max<int64_t>(1, s->n_slots / per_group));
+  if (n_groups < 2 || s->rods.size() < 2) return EB_OK;
+  std::vector<std::vector<size_t>> members(1);
+  std::vector<int64_t> cut(1, 0);
+  for (size_t r = 0; r < s->rods.size(); ++r) {
+    const int64_t j = static_cast<int64_t>(members.size());
+    if (!members.back().empty() && j < n_groups && s->offsets[r] >= j * s->n_slots / n_groups) {
+      members.emplace_back();
+      cut.push_back(s->offsets[r]);
+    }
+    members.back().push_back(r);
+  }
+  cut.push_back(s->n_slots);
+  if (members.size() < 2) return EB_OK;
+  std::vector<int64_t> off;
+  std::vector<int32_t> map;
+  for (size_t g = 0; g < members.size(); ++g) {
+    eb_sim::XGroup X;
+    X.lo = cut[g];
+    X.hi = cut[g + 1];
+    if (!pack_best_fit(s, members[g], c, off, map)) return fail(EB_ERR_INVALID_STATE, "exchange group does not pack");
+    EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&X.d_off), off.size() * sizeof(int64_t)));
+    s->xgroups.push_back(X);  // owned from here on (freed with the simulator)
+    EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&s->xgroups.back().d_map), map.size() * sizeof(int32_t)));
+    EB_CUDA(cudaMemcpyAsync(s->xgroups.back().d_off, off.data(), off.size() * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, s->stream));
+    EB_CUDA(cudaMemcpyAsync(s->xgroups.back().d_map, map.data(), map.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, s->stream));
+    s->xgroups.back().n_ctas = static_cast<int>(off.size() - 1);
+    EB_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  if (!s->xs[0])
+    for (auto& x : s->xs) EB_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+  const size_t n_ev = 2 * s->xgroups.size() + 5;
+  while (s->xev.size() < n_ev) {
+    cudaEvent_t e;
+    EB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    s->xev.push_back(e);
+  }
+  return EB_OK;
+}
+
 }  // namespace
 
 EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
@@ -1746,14 +1844,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (n_steps < 0) return fail(EB_ERR_INVALID_ARGUMENT, "negative step count");
   if (n_steps == 0) return EB_OK;
   if (eb_status st = set_device(s)) return st;
-  if ((s->sim_flags & eb::kSimDamper) && dt != s->damper_dt) {
-    // the reference builds the damper's exponential constants once for the
-    // simulation's dt (AnalyticalLinearDamper.hpp:40-57)
-    for (auto& r : s->rods)
-      if (r.info.flags & eb::kRodDamper) r.info.damper_t = std::exp(-r.damper_nu_t * dt);
-    if (eb_status st = upload_rod_table(s)) return st;
-    s->damper_dt = dt;
-  }
+  if (eb_status st = damper_for_dt(s, dt)) return st;
   if (s->plan_mode == 0)
     if (eb_status st = plan_steps(s, dt, static_cast<int>(std::min<int64_t>(n_steps, kResidentChunk)))) return st;
   const bool diag = s->d_diag != nullptr;
@@ -1810,6 +1901,111 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     }
   }
   return EB_OK;
+}
+
+// The state fields the exchange moves, in eb_host_state's order.
+constexpr int32_t kExchangeFields[4] = {EB_POSITION, EB_VELOCITY, EB_DIRECTOR, EB_ANGULAR_VELOCITY};
+
+EB_API eb_status eb_step_host_state(eb_sim* s, double* time, double dt, int64_t n_steps,
+                                    const eb_host_state* host) {
+  if (check_sim(s) || !host) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s->finalized) return fail(EB_ERR_INVALID_STATE, "finalize before stepping");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(EB_ERR_INVALID_ARGUMENT, "dt must be positive and finite");
+  if (n_steps < 0) return fail(EB_ERR_INVALID_ARGUMENT, "negative step count");
+  const double* in[4] = {host->position_in, host->velocity_in, host->director_in, host->angular_velocity_in};
+  double* out[4] = {host->position_out, host->velocity_out, host->director_out, host->angular_velocity_out};
+  bool any_out = false;
+  for (double* o : out) any_out = any_out || o;
+  if (eb_status st = set_device(s)) return st;
+  // the plan is chosen by the first step; contact, connections and recorded
+  // diagnostics step the whole batch together
+  bool overlap = n_steps > 0 && s->plan_mode == 2 && !s->contact.on && !s->jd.on && !s->d_diag;
+  if (overlap) {
+    if (eb_status st = build_exchange_groups(s)) return st;
+    overlap = !s->xgroups.empty();
+  }
+  if (!overlap) {
+    for (int f = 0; f < 4; ++f)
+      if (in[f])
+        if (eb_status st = batch_copy(s, kExchangeFields[f], EB_LAYOUT_SLOTS, const_cast<double*>(in[f]),
+                                      kFields[kExchangeFields[f]].ncomp * s->n_slots, true))
+          return st;
+    if (eb_status st = eb_step(s, time, dt, n_steps)) return st;
+    for (int f = 0; f < 4; ++f)
+      if (out[f])
+        if (eb_status st = batch_copy(s, kExchangeFields[f], EB_LAYOUT_SLOTS, out[f],
+                                      kFields[kExchangeFields[f]].ncomp * s->n_slots, false))
+          return st;
+    return EB_OK;
+  }
+  if (eb_status st = damper_for_dt(s, dt)) return st;
+  eb::StepArgs a = step_args(s, dt);
+  set_substeps(s, a);
+  const int c = s->plan_config;
+  const int64_t S = s->stride;
+  const size_t pitch = static_cast<size_t>(S) * sizeof(double);
+  const size_t hpitch = static_cast<size_t>(s->n_slots) * sizeof(double);
+  const int64_t chunks = (n_steps + kResidentChunk - 1) / kResidentChunk;
+  const int c0 = s->cur, c1 = static_cast<int>((c0 + chunks) & 1);
+  const size_t G = s->xgroups.size();
+  cudaEvent_t* ev = s->xev.data();  // [0] start, [1, G] inputs landed, [G+1, 2G] steps done, [2G+1, 2G+4] ends
+  EB_CUDA(cudaEventRecord(ev[0], s->stream));
+  for (cudaStream_t x : s->xs) EB_CUDA(cudaStreamWaitEvent(x, ev[0], 0));
+  for (size_t g = 0; g < G; ++g) {
+    const eb_sim::XGroup& X = s->xgroups[g];
+    const size_t w = static_cast<size_t>(X.hi - X.lo) * sizeof(double);
+    cudaStream_t L = s->xs[2 + (g & 1)];
+    // inputs into the current buffer, then the same values into the other
+    // one on the device (as eb_set_field_batch: entries no step writes match)
+    for (int f = 0; f < 4; ++f) {
+      if (!in[f]) continue;
+      const FieldInfo& fi = kFields[kExchangeFields[f]];
+      EB_CUDA(cudaMemcpy2DAsync(s->d_state[c0] + fi.offset * S + X.lo, pitch, in[f] + X.lo, hpitch, w, fi.ncomp,
+                                cudaMemcpyHostToDevice, s->xs[0]));
+    }
+    EB_CUDA(cudaEventRecord(ev[1 + g], s->xs[0]));
+    EB_CUDA(cudaStreamWaitEvent(L, ev[1 + g], 0));
+    for (int f = 0; f < 4; ++f) {
+      if (!in[f]) continue;
+      const FieldInfo& fi = kFields[kExchangeFields[f]];
+      EB_CUDA(cudaMemcpy2DAsync(s->d_state[c0 ^ 1] + fi.offset * S + X.lo, pitch, s->d_state[c0] + fi.offset * S + X.lo,
+                                pitch, w, fi.ncomp, cudaMemcpyDeviceToDevice, L));
+    }
+    int cur = c0;
+    for (int64_t done = 0; done < n_steps;) {
+      const int k = static_cast<int>(std::min<int64_t>(kResidentChunk, n_steps - done));
+      a.in = s->d_state[cur];
+      a.out = s->d_state[cur ^ 1];
+      if (s->cfg.precision == EB_PRECISION_MIXED)
+        EB_CUDA(eb::launch_rod_block_mixed_gather(a, X.d_off, X.d_map, X.n_ctas, k, c, s->any_damped, L));
+      else
+        EB_CUDA(eb::launch_rod_block_fp64_gather(a, X.d_off, X.d_map, X.n_ctas, k, c, s->any_damped, L));
+      ++s->launches;
+      cur ^= 1;
+      done += k;
+    }
+    EB_CUDA(cudaEventRecord(ev[1 + G + g], L));
+    EB_CUDA(cudaStreamWaitEvent(s->xs[1], ev[1 + G + g], 0));
+    for (int f = 0; f < 4; ++f) {
+      if (!out[f]) continue;
+      const FieldInfo& fi = kFields[kExchangeFields[f]];
+      EB_CUDA(cudaMemcpy2DAsync(out[f] + X.lo, hpitch, s->d_state[c1] + fi.offset * S + X.lo, pitch, w, fi.ncomp,
+                                cudaMemcpyDeviceToHost, s->xs[1]));
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    EB_CUDA(cudaEventRecord(ev[1 + 2 * G + k], s->xs[k]));
+    EB_CUDA(cudaStreamWaitEvent(s->stream, ev[1 + 2 * G + k], 0));
+  }
+  s->cur = c1;
+  if (time)
+    for (int64_t k = 0; k < n_steps; ++k) {
+      *time += 0.5 * dt;
+      *time += 0.5 * dt;
+    }
+  if (!any_out) return EB_OK;
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_status(s);
 }
 
 EB_API eb_status eb_contact_pairs(eb_sim* s, int64_t* pairs, int64_t capacity, int64_t* count) {

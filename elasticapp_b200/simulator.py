@@ -395,6 +395,36 @@ class Simulator:
         L.call("eb_step", self._h, ctypes.byref(t), float(dt), int(n_steps))
         return t.value
 
+    _EXCHANGE = ("Position", "Velocity", "Director", "AngularVelocity")
+
+    def step_host_state(self, stepper, time: float, dt: float, n_steps: int, inputs: dict | None = None,
+                        outputs: dict | None = None) -> float:
+        """Set the state from host arrays, step, read it back (eb_step_host_state).
+
+        inputs/outputs map "Position", "Velocity", "Director" and
+        "AngularVelocity" to float64 C-contiguous arrays in the slot layout,
+        shape (ncomp, n_slots); an output may be its input.  The same as
+        set_slots, step and get_slots in sequence; under a resident plan the
+        copies of one slot group overlap the steps of the others (pinned
+        arrays needed for the overlap).
+        """
+        if not isinstance(stepper, self.stepper):
+            raise TypeError(f"this simulator was created for {self.stepper.__name__}")
+        hs = L.EbHostState()
+        S = self.n_slots()
+        for d, arrays in (("in", inputs or {}), ("out", outputs or {})):
+            for name, arr in arrays.items():
+                if name not in self._EXCHANGE:
+                    raise KeyError(f"{name} is not a state field")
+                shape = (L.FIELD_SHAPE[name][1], S)
+                if (not isinstance(arr, np.ndarray) or arr.dtype != np.float64 or arr.shape != shape
+                        or not arr.flags.c_contiguous or (d == "out" and not arr.flags.writeable)):
+                    raise ValueError(f"{name} must be a C-contiguous float64 array of shape {shape}")
+                setattr(hs, f"{L.FIELD_NAME_SNAKE[name]}_{d}", arr.ctypes.data)
+        t = ctypes.c_double(time)
+        L.call("eb_step_host_state", self._h, ctypes.byref(t), float(dt), int(n_steps), ctypes.byref(hs))
+        return t.value
+
     def synchronize(self) -> None:
         L.call("eb_synchronize", self._h)
 

@@ -336,6 +336,33 @@ EB_API eb_status eb_finalize(struct eb_sim* sim);
 EB_API eb_status eb_step(struct eb_sim* sim, double* time, double dt, int64_t n_steps);
 EB_API eb_status eb_synchronize(struct eb_sim* sim);
 
+/* --- one cycle of a host-driven loop: the state set from host memory, then
+ * the reference's CaseStudy run_for and communicate()
+ * (elastica/Utilities/AppSupport/Python/CaseStudyPybind.hpp:40-110).  Uploads
+ * every non-null input (slot layout, ncomp x slot_count doubles, as
+ * eb_set_field_batch with EB_LAYOUT_SLOTS), runs n_steps as eb_step and reads
+ * every non-null output back (as eb_get_field_batch); the result is the same
+ * as those calls in sequence, bit for bit.  An output may be the same buffer
+ * as its input.  Under a resident plan (eb_step_plan mode 2; no contact,
+ * connections or recorded diagnostics) the rods are cut into contiguous slot
+ * groups whose copies overlap the other groups' launches; with pinned host
+ * buffers the cycle then costs about the steps plus one group's copies
+ * instead of the steps plus all copies.  Otherwise, and on the call that
+ * chooses the plan, the copies and steps run in sequence.  Returns once the
+ * outputs are written (asynchronous when there are none). */
+typedef struct eb_host_state {
+  const double* position_in;         /* 3 x slot_count, or NULL */
+  const double* velocity_in;         /* 3 x slot_count, or NULL */
+  const double* director_in;         /* 9 x slot_count, or NULL */
+  const double* angular_velocity_in; /* 3 x slot_count, or NULL */
+  double* position_out;
+  double* velocity_out;
+  double* director_out;
+  double* angular_velocity_out;
+} eb_host_state;
+EB_API eb_status eb_step_host_state(struct eb_sim* sim, double* time, double dt, int64_t n_steps,
+                                    const eb_host_state* host);
+
 /* --- energies (elastica/Systems/CosseratRods/Utility/Energy.hpp:46-141) at
  * the current state: out[4 r + {0,1,2,3}] = translational, rotational,
  * shear/stretch, bend/twist energy of rod r. */
