@@ -213,19 +213,20 @@ struct eb_sim {
   std::vector<int> n_ctas;
   float plan_ms[20] = {0};
   // host-state exchange (eb_step_host_state) under a resident plan: the rods
-  // split into contiguous slot groups, each packed on its own for the
-  // configuration xconfig, so one group's copies overlap another's launches;
-  // streams: copies in, copies out, launches of even and of odd groups;
-  // events: the start, per group its inputs landed and its steps done, the
-  // four streams' ends
+  // split into contiguous slot groups, each packed on its own for the plan
+  // (xplan: mode and configuration it was built for), so one group's copies
+  // overlap another's launches; per group one work list (whole-batch plan,
+  // index 0) or one per size bucket; streams: copies in, copies out,
+  // launches of even and of odd groups; events: the start, per group its
+  // inputs landed and its steps done, the four streams' ends
   struct XGroup {
     int64_t lo = 0, hi = 0;  // slots [lo, hi)
-    int64_t* d_off = nullptr;
-    int32_t* d_map = nullptr;
-    int n_ctas = 0;
+    int64_t* d_off[4] = {nullptr, nullptr, nullptr, nullptr};
+    int32_t* d_map[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n_ctas[4] = {0, 0, 0, 0};
   };
   std::vector<XGroup> xgroups;
-  int xconfig = -1;
+  int64_t xplan = -1;
   cudaStream_t xs[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> xev;
   // captured streaming steps: per starting buffer parity, for graph_dt
@@ -415,12 +416,13 @@ void host_free(eb_sim* s) {
       if (q) cudaFree(q);
     j = JointDevice{};
   }
-  for (auto& g : s->xgroups) {
-    if (g.d_off) cudaFree(g.d_off);
-    if (g.d_map) cudaFree(g.d_map);
-  }
+  for (auto& g : s->xgroups)
+    for (int k = 0; k < 4; ++k) {
+      if (g.d_off[k]) cudaFree(g.d_off[k]);
+      if (g.d_map[k]) cudaFree(g.d_map[k]);
+    }
   s->xgroups.clear();
-  s->xconfig = -1;
+  s->xplan = -1;
   for (auto& b : s->buckets) {
     for (int c = 0; c < 4; ++c) {
       if (b.d_off[c]) cudaFree(b.d_off[c]);
@@ -1775,24 +1777,41 @@ eb_status damper_for_dt(eb_sim* s, double dt) {
   return EB_OK;
 }
 
-// Slot groups of the host-state exchange for the resident configuration of
-// the plan: the rods in order cut into contiguous runs of about equal slot
-// counts, each packed best fit decreasing on its own (a group's CTAs touch
-// only its slots, so its launches need only its copies).  One group per six
-// waves of the configuration's CTAs, at most eight; a single group means no
-// overlap and the exchange runs its copies and steps in sequence.
+// Slot groups of the host-state exchange for the resident plan (mode 2: the
+// whole-batch configuration; mode 3: each size bucket's): the rods in order
+// cut into contiguous runs of about equal slot counts, each packed on its own
+// the way the plan packs the whole batch (a group's CTAs touch only its
+// slots, so its launches need only its copies).  One group per six waves of
+// 512-slot CTAs, at most eight; a single group means no overlap and the
+// exchange runs its copies and steps in sequence.
+eb_status upload_list(eb_sim* s, const std::vector<int64_t>& off, const std::vector<int32_t>& map, int64_t** d_off,
+                      int32_t** d_map) {
+  EB_CUDA(cudaMalloc(reinterpret_cast<void**>(d_off), off.size() * sizeof(int64_t)));
+  EB_CUDA(cudaMalloc(reinterpret_cast<void**>(d_map), map.size() * sizeof(int32_t)));
+  EB_CUDA(cudaMemcpyAsync(*d_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaMemcpyAsync(*d_map, map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  return EB_OK;
+}
+
+// the buckets a bucketed plan launches
+bool bucket_launched(const eb_sim* s, int b) {
+  return s->buckets[b].rods > 0 && !(s->bucket_merged ? (b == 0 || b == 1) : b == 3);
+}
+
 eb_status build_exchange_groups(eb_sim* s) {
-  const int c = s->plan_config;
-  if (s->xconfig == c && !s->xgroups.empty()) return EB_OK;
-  for (auto& g : s->xgroups) {
-    if (g.d_off) EB_CUDA(cudaFree(g.d_off));
-    if (g.d_map) EB_CUDA(cudaFree(g.d_map));
-  }
+  const int64_t plan = 1000 * s->plan_mode + (s->plan_mode == 2 ? s->plan_config : bucket_plan_config(s));
+  if (s->xplan == plan && !s->xgroups.empty()) return EB_OK;
+  for (auto& g : s->xgroups)
+    for (int k = 0; k < 4; ++k) {
+      if (g.d_off[k]) EB_CUDA(cudaFree(g.d_off[k]));
+      if (g.d_map[k]) EB_CUDA(cudaFree(g.d_map[k]));
+    }
   s->xgroups.clear();
-  s->xconfig = c;
+  s->xplan = plan;
   int sms = 0;
   EB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device));
-  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * pack_fill(c) * 6;
+  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * 512 * 6;
   const int64_t n_groups = std::min<int64_t>(8, std::max<int64_t>(1, s->n_slots / per_group));
   if (n_groups < 2 || s->rods.size() < 2) return EB_OK;
   std::vector<std::vector<size_t>> members(1);
@@ -1810,19 +1829,40 @@ eb_status build_exchange_groups(eb_sim* s) {
   std::vector<int64_t> off;
   std::vector<int32_t> map;
   for (size_t g = 0; g < members.size(); ++g) {
-    eb_sim::XGroup X;
+    s->xgroups.emplace_back();  // owned from here on (freed with the simulator)
+    eb_sim::XGroup& X = s->xgroups.back();
     X.lo = cut[g];
     X.hi = cut[g + 1];
-    if (!pack_best_fit(s, members[g], c, off, map)) return fail(EB_ERR_INVALID_STATE, "exchange group does not pack");
-    EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&X.d_off), off.size() * sizeof(int64_t)));
-    s->xgroups.push_back(X);  // owned from here on (freed with the simulator)
-    EB_CUDA(cudaMalloc(reinterpret_cast<void**>(&s->xgroups.back().d_map), map.size() * sizeof(int32_t)));
-    EB_CUDA(cudaMemcpyAsync(s->xgroups.back().d_off, off.data(), off.size() * sizeof(int64_t),
-                            cudaMemcpyHostToDevice, s->stream));
-    EB_CUDA(cudaMemcpyAsync(s->xgroups.back().d_map, map.data(), map.size() * sizeof(int32_t),
-                            cudaMemcpyHostToDevice, s->stream));
-    s->xgroups.back().n_ctas = static_cast<int>(off.size() - 1);
-    EB_CUDA(cudaStreamSynchronize(s->stream));
+    for (int b = 0; b < 4; ++b) {
+      std::vector<size_t> rods;
+      if (s->plan_mode == 2) {
+        if (b > 0) break;
+        rods = members[g];
+      } else {
+        if (!bucket_launched(s, b)) continue;
+        for (size_t r : members[g]) {
+          const int rb = bucket_of(s->rods[r].n + 1);
+          if (rb == b || (b == 3 && (rb == 0 || rb == 1))) rods.push_back(r);
+        }
+      }
+      if (rods.empty()) continue;
+      if (s->plan_mode == 3 && b == 2) {
+        // rod pairs: the first half of each rod's slots on the even CTA
+        off.assign(1, 0);
+        map.clear();
+        for (size_t r : rods) {
+          const int64_t w = s->rods[r].n + 1, h = (w + 1) / 2;
+          for (int64_t k = 0; k < w; ++k) map.push_back(static_cast<int32_t>(s->offsets[r] + k));
+          off.push_back(off.back() + h);
+          off.push_back(off.back() + (w - h));
+        }
+      } else {
+        const int c = s->plan_mode == 2 ? s->plan_config : s->bucket_config[b];
+        if (!pack_best_fit(s, rods, c, off, map)) return fail(EB_ERR_INVALID_STATE, "exchange group does not pack");
+      }
+      if (eb_status st = upload_list(s, off, map, &X.d_off[b], &X.d_map[b])) return st;
+      X.n_ctas[b] = static_cast<int>(off.size() - 1);
+    }
   }
   if (!s->xs[0])
     for (auto& x : s->xs) EB_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
@@ -1833,6 +1873,26 @@ eb_status build_exchange_groups(eb_sim* s) {
     s->xev.push_back(e);
   }
   return EB_OK;
+}
+
+// One resident launch of `steps` steps over slot group X.
+cudaError_t launch_exchange_group(eb_sim* s, eb::StepArgs& a, const eb_sim::XGroup& X, int steps, cudaStream_t L,
+                                  int64_t* launches) {
+  const bool mixed = s->cfg.precision == EB_PRECISION_MIXED;
+  for (int b = 0; b < 4; ++b) {
+    if (X.n_ctas[b] == 0) continue;
+    const int c = s->plan_mode == 2 ? s->plan_config : s->bucket_config[b];
+    cudaError_t e;
+    if (s->plan_mode == 3 && b == 2)
+      e = mixed ? eb::launch_rod_block_mixed_pairs(a, X.d_off[b], X.d_map[b], X.n_ctas[b], steps, c, s->any_damped, L)
+                : eb::launch_rod_block_fp64_pairs(a, X.d_off[b], X.d_map[b], X.n_ctas[b], steps, c, s->any_damped, L);
+    else
+      e = mixed ? eb::launch_rod_block_mixed_gather(a, X.d_off[b], X.d_map[b], X.n_ctas[b], steps, c, s->any_damped, L)
+                : eb::launch_rod_block_fp64_gather(a, X.d_off[b], X.d_map[b], X.n_ctas[b], steps, c, s->any_damped, L);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -1919,7 +1979,7 @@ EB_API eb_status eb_step_host_state(eb_sim* s, double* time, double dt, int64_t 
   if (eb_status st = set_device(s)) return st;
   // the plan is chosen by the first step; contact, connections and recorded
   // diagnostics step the whole batch together
-  bool overlap = n_steps > 0 && s->plan_mode == 2 && !s->contact.on && !s->jd.on && !s->d_diag;
+  bool overlap = n_steps > 0 && (s->plan_mode == 2 || s->plan_mode == 3) && !s->contact.on && !s->jd.on && !s->d_diag;
   if (overlap) {
     if (eb_status st = build_exchange_groups(s)) return st;
     overlap = !s->xgroups.empty();
@@ -1941,7 +2001,6 @@ EB_API eb_status eb_step_host_state(eb_sim* s, double* time, double dt, int64_t 
   if (eb_status st = damper_for_dt(s, dt)) return st;
   eb::StepArgs a = step_args(s, dt);
   set_substeps(s, a);
-  const int c = s->plan_config;
   const int64_t S = s->stride;
   const size_t pitch = static_cast<size_t>(S) * sizeof(double);
   const size_t hpitch = static_cast<size_t>(s->n_slots) * sizeof(double);
@@ -1976,11 +2035,7 @@ EB_API eb_status eb_step_host_state(eb_sim* s, double* time, double dt, int64_t 
       const int k = static_cast<int>(std::min<int64_t>(kResidentChunk, n_steps - done));
       a.in = s->d_state[cur];
       a.out = s->d_state[cur ^ 1];
-      if (s->cfg.precision == EB_PRECISION_MIXED)
-        EB_CUDA(eb::launch_rod_block_mixed_gather(a, X.d_off, X.d_map, X.n_ctas, k, c, s->any_damped, L));
-      else
-        EB_CUDA(eb::launch_rod_block_fp64_gather(a, X.d_off, X.d_map, X.n_ctas, k, c, s->any_damped, L));
-      ++s->launches;
+      EB_CUDA(launch_exchange_group(s, a, X, k, L, &s->launches));
       cur ^= 1;
       done += k;
     }

@@ -343,7 +343,7 @@ EB_API eb_status eb_synchronize(struct eb_sim* sim);
  * eb_set_field_batch with EB_LAYOUT_SLOTS), runs n_steps as eb_step and reads
  * every non-null output back (as eb_get_field_batch); the result is the same
  * as those calls in sequence, bit for bit.  An output may be the same buffer
- * as its input.  Under a resident plan (eb_step_plan mode 2; no contact,
+ * as its input.  Under a resident plan (eb_step_plan mode 2 or 3; no contact,
  * connections or recorded diagnostics) the rods are cut into contiguous slot
  * groups whose copies overlap the other groups' launches; with pinned host
  * buffers the cycle then costs about the steps plus one group's copies

@@ -6,7 +6,8 @@ group's copies overlap the other groups' launches.  The result must be the
 same, bit for bit and in every slot entry, as eb_set_field_batch, eb_step and
 eb_get_field_batch in sequence, for one and several resident chunks, an
 output that is its own input, inputs or outputs left out, and both
-precisions; plans the overlap does not cover take the sequential path."""
+precisions and for the whole-batch and per-size-bucket resident plans; plans
+the overlap does not cover take the sequential path."""
 import numpy as np
 import pytest
 import torch
@@ -74,6 +75,30 @@ def test_exchange_equals_sequential_calls(batch, precision, config, n_steps):
     xch.step(eb.PositionVerlet(), t_x, batch.dt, 3)
     for name in STATE:
         assert np.array_equal(xch.get_slots(name), seq.get_slots(name)), name
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_exchange_bucketed_plan(precision):
+    # rods of all three size buckets (pairs of CTAs for 520-1039 elements),
+    # about 1.6 M slots; the sequential calls and the exchange run on the same
+    # simulator (same bucket configurations) from the same snapshot
+    wl = W.uneven_batch(n_rods=3100, seed=45, n_range=(32, 1000), n_steps=200)
+    sim = planned(wl, precision=precision, step_mode="bucketed")
+    assert sim.step_plan()["mode"] == "bucketed"
+    host = perturbed_state(sim, seed=11)
+    snap = sim.snapshot()
+    for name in STATE:
+        sim.set_slots(name, host[name])
+    t_seq = sim.step(eb.PositionVerlet(), 0.25, wl.dt, 200)
+    want = {name: sim.get_slots(name) for name in STATE}
+    sim.restore(snap)
+    out = {name: pinned(host[name].shape) for name in STATE}
+    before = sim.launch_count()
+    t_x = sim.step_host_state(eb.PositionVerlet(), 0.25, wl.dt, 200, inputs=host, outputs=out)
+    assert sim.launch_count() - before > 2 * 3  # two chunks of at most three bucket launches, per group
+    assert t_x == t_seq
+    for name in STATE:
+        assert np.array_equal(out[name], want[name]), name
 
 
 def test_exchange_in_place_and_partial_fields(batch):
