@@ -101,6 +101,24 @@ def test_exchange_bucketed_plan(precision):
         assert np.array_equal(out[name], want[name]), name
 
 
+def test_exchange_pefrl(batch):
+    # four force evaluations a step on the resident kernel, per slot group
+    seq = batch.build(step_mode="resident", resident_config=1, stepper=eb.PEFRL)
+    xch = batch.build(step_mode="resident", resident_config=1, stepper=eb.PEFRL)
+    for sim in (seq, xch):
+        sim.step(eb.PEFRL(), 0.0, batch.dt, 8)
+        assert sim.step_plan()["mode"] == "resident"
+    host = perturbed_state(seq, seed=5)
+    for name in STATE:
+        seq.set_slots(name, host[name])
+    t_seq = seq.step(eb.PEFRL(), 0.0, batch.dt, 130)
+    out = {name: pinned(host[name].shape) for name in STATE}
+    t_x = xch.step_host_state(eb.PEFRL(), 0.0, batch.dt, 130, inputs=host, outputs=out)
+    assert t_x == t_seq
+    for name in STATE:
+        assert np.array_equal(out[name], seq.get_slots(name)), name
+
+
 def test_exchange_in_place_and_partial_fields(batch):
     seq = planned(batch, step_mode="resident", resident_config=1)
     xch = planned(batch, step_mode="resident", resident_config=1)
