@@ -3,7 +3,8 @@
 //
 // cp.async.bulk moves a contiguous byte range with the Tensor Memory
 // Accelerator; source and destination must be 16-byte aligned and the size a
-// multiple of 16 bytes.  No multicast form is used anywhere.
+// multiple of 16 bytes.  Every copy reads this GPU's own memory into its own
+// CTA's shared memory; no copy is shared across the CTAs of a cluster.
 #pragma once
 
 #include <cstdint>
