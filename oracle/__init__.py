@@ -94,6 +94,8 @@ def lib():
         for name in ("orc_fine_capsule_capsule", "orc_fine_capsule_plane"):
             getattr(_lib, name).argtypes = [_P, _P, _P]
         _lib.orc_fine_pair_loads.argtypes = [_P, _P, _P, _P]
+        _lib.orc_so3_add_assign.argtypes = [_P, _P]
+        _lib.orc_inv_rotate_divide.argtypes = [_P, _P, ctypes.c_double, _P]
         _lib.orc_step_loads.argtypes = [ctypes.POINTER(_OrcRods), ctypes.POINTER(_OrcContact),
                                         ctypes.POINTER(_OrcConnections), ctypes.c_double, ctypes.c_int64,
                                         ctypes.c_int]

@@ -1218,6 +1218,23 @@ void put_contacts(const ContactPoint* pts, int n, double* out) {
 }
 }  // namespace
 
+/* Single-element kernels for the reference's own kernel tests
+ * (tests/Unit/Systems/States/Expressions/SO3/Test_SO3PrimitiveAddAssign.cpp,
+ * tests/Unit/Systems/CosseratRods/Traits/Operations/BlazeBackend/Test_InvRotateDivide_Scalar.cpp):
+ * the same so3_add_assign and inv_rotate_divide the step uses. */
+extern "C" int orc_so3_add_assign(double* q, const double* u) {
+  so3_add_assign(q, {u[0], u[1], u[2]});
+  return 0;
+}
+
+extern "C" int orc_inv_rotate_divide(const double* qc, const double* qn, double span, double* out) {
+  const V3 k = inv_rotate_divide(qc, qn, span);
+  out[0] = k.x;
+  out[1] = k.y;
+  out[2] = k.z;
+  return 0;
+}
+
 extern "C" int orc_fine_capsule_capsule(const double* a, const double* b, double* contacts) {
   ContactPoint pts[2];
   const int n = rod_capsule_contacts(capsule_from_desc(a), capsule_from_desc(b), pts);

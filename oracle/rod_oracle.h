@@ -173,6 +173,14 @@ int orc_fine_capsule_capsule(const double* a, const double* b, double* contacts)
 int orc_fine_capsule_plane(const double* capsule, const double* plane, double* contacts);
 int orc_fine_pair_loads(const double* a, const double* b, const double* pm, double* out);
 
+/* Element kernels of the step, exposed for the reference's kernel tests.
+ * A director matrix is 9 doubles q[3 k + j] = component j of director d_k.
+ * orc_so3_add_assign: q <- exp(-[u]x) q (SO3PrimitiveAddAssign/Scalar.hpp).
+ * orc_inv_rotate_divide: curvature between directors qc and qn divided by
+ * span, out[3] (InvRotateDivide/Scalar.hpp). */
+int orc_so3_add_assign(double* q, const double* u);
+int orc_inv_rotate_divide(const double* qc, const double* qn, double span, double* out);
+
 /* Straight-rod initializer (reference Initializers/detail/Geometry.hpp and the
  * component initialize() chains).  Fills one rod of n elements:
  * x[3*(n+1)], Q[9*n], l0[n], D0[n-1], V[n], radius[n], mass[n+1],

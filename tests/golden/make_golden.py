@@ -12,6 +12,9 @@ tests:
   (undamped rod; 1 rod after 0/1/3/5 steps),
 * ``tests/Unit/Systems/CosseratRods/FullRodTest/Test_PerturbedRod.cpp``
   (state injection round trips for 2 rods).
+* ``tests/Unit/Systems/States/Expressions/SO3/Test_SO3PrimitiveAddAssign.cpp``
+  (the director update from the identity by a fixed rotation vector, applied
+  repeatedly; written to ``so3_add_assign.json``).
 
 This script reads those files as text (nothing is compiled or run) and writes
 ``tests/golden/<name>.json``.  Every number is stored as ``float.hex`` so the
@@ -119,6 +122,42 @@ def parse_file(path: str) -> list[dict]:
     return cases
 
 
+SO3_FILE = "tests/Unit/Systems/States/Expressions/SO3/Test_SO3PrimitiveAddAssign.cpp"
+SO3_EXPECTED = re.compile(r"H_mat (expected_result_(\d))\{(.*?)\};", re.S)
+SO3_DIRECTION = re.compile(r"DH_mat _derivative_data\{(.*?)\};", re.S)
+SO3_ANGLE = re.compile(r"_derivative_data \*= ([0-9.]+) \* M_PI / 180\.0;")
+SO3_TIMES = re.compile(r"Time first\(([0-9.]+)\), second\(([0-9.]+)\)")
+
+
+def parse_so3(path: str) -> dict:
+    """Rotation-vector inputs and the expected directors after 1, 2, 3
+    applications of the SO(3) update.  Each expected tensor is 3 x 3 x 1 in
+    page-major order, i.e. 9 values q[3 k + j] = component j of director d_k."""
+    text = open(path, encoding="utf-8").read()
+
+    def line_of(pos: int) -> int:
+        return text.count("\n", 0, pos) + 1
+
+    expected = []
+    for m in SO3_EXPECTED.finditer(text):
+        values = parse_values(m.group(3))
+        if len(values) != 9:
+            raise ValueError(f"{path}:{line_of(m.start())}: {m.group(1)} has {len(values)} values")
+        expected.append({"name": m.group(1), "applications": int(m.group(2)), "line": line_of(m.start()),
+                         "hex": [v.hex() for v in values]})
+    d = SO3_DIRECTION.search(text)
+    a = SO3_ANGLE.search(text)
+    t = SO3_TIMES.search(text)
+    if not (expected and d and a and t):
+        raise ValueError(f"{path}: SO(3) test layout not recognised")
+    direction = parse_values(d.group(1))
+    return {
+        "direction": [v.hex() for v in direction], "direction_line": line_of(d.start()),
+        "angle_deg": float(a.group(1)).hex(), "angle_line": line_of(a.start()),
+        "time_delta": (float(t.group(2)) - float(t.group(1))).hex(), "time_line": line_of(t.start()),
+        "expected": expected,
+    }
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", default="/root/reference")
@@ -139,6 +178,18 @@ def main(argv=None) -> int:
             json.dump(doc, f, indent=1, sort_keys=True)
         n_sec = sum(len(c["sections"]) for c in cases)
         print(f"{out}: {len(cases)} cases, {n_sec} sections")
+    so3 = parse_so3(os.path.join(args.reference, SO3_FILE))
+    doc = {
+        "source": SO3_FILE,
+        "generator": "tests/golden/make_golden.py (text extraction, no reference code executed)",
+        "note": "Rotation vector = time_delta * angle_deg * pi / 180 * direction / |direction|, applied "
+                "to the identity director; expected directors q[3k+j] = component j of d_k; float.hex.",
+        **so3,
+    }
+    out = os.path.join(args.out, "so3_add_assign.json")
+    with open(out, "w", encoding="utf-8") as f:
+        json.dump(doc, f, indent=1, sort_keys=True)
+    print(f"{out}: {len(so3['expected'])} expected directors")
     return 0
 
 
