@@ -162,11 +162,34 @@ def cpu_reference_rate(wl, n_steps: int, budget_s: float = None, max_rods: int |
     return rate, cores, sample
 
 
-def run_reference(args, wl_fn):
+def bench_workload(args, W, rank, world):
+    """The rods this rank steps.  One process: the named workload.  Several
+    (weak scaling): one global batch of world x the per-GPU rods, sharded by
+    the Karmarkar-Karp partition of its rods (element-balanced); the
+    cantilever runs as one replica per rank."""
+    if args.workload == "cantilever":
+        return W.cantilever()
+    if world > 1:
+        from elasticapp_b200 import dist as ebdist
+        per = args.rods if args.rods is not None else 16384
+        return ebdist.shard(W.CONFIGS[args.workload](n_rods=per * world, seed=1002), rank, world)
+    kw = {"seed": 1002 + rank}
+    if args.rods is not None:
+        kw["n_rods"] = args.rods
+    return W.CONFIGS[args.workload](**kw)
+
+
+def run_reference(args, W):
+    """The reference arm: the CPU restatement of the reference's scalar path
+    on all host cores, on the rods rank 0 of the GPU arm steps (the whole
+    workload on one process; rank 0's shard under torchrun, where only rank 0
+    runs and the others exit at once).  Element-steps/s of this CPU path does
+    not depend on how many rods it holds beyond a few thousand, so the shard
+    stands for the whole job."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    wl = wl_fn(0)
+    wl = bench_workload(args, W, 0, world)
     cores = os.cpu_count() or 1
     # warm-up steps, then K timed steps over the whole workload
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -187,7 +210,8 @@ def run_reference(args, wl_fn):
         "data": "synthetic (seeded)",
         "config": workload_config(wl, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"whole workload ({len(wl.rods)} rods, {wl.total_elements} elements) "
+                         "sample": f"{'rank 0 shard' if world > 1 else 'whole workload'} "
+                                   f"({len(wl.rods)} rods, {wl.total_elements} elements) "
                                    f"x {args.steps} steps; CPU restatement of the reference's scalar "
                                    "path (reference not buildable here: Blaze/TBB absent)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -481,15 +505,8 @@ def main(argv=None) -> int:
 
     from elasticapp_b200 import workloads as W
 
-    def wl_fn(rank):
-        if args.workload == "cantilever":
-            return W.cantilever()
-        kw = {"seed": 1002 + rank}
-        if args.rods is not None:
-            kw["n_rods"] = args.rods
-        return W.CONFIGS[args.workload](**kw)
     if args.impl == "reference":
-        return run_reference(args, wl_fn)
+        return run_reference(args, W)
 
     import torch
 
@@ -507,14 +524,7 @@ def main(argv=None) -> int:
 
     import elasticapp_b200 as eb
 
-    if world > 1 and args.workload != "cantilever":
-        # one global batch of world x the per-GPU size, sharded by the
-        # Karmarkar-Karp partition of its rods (element-balanced, weak scaling)
-        from elasticapp_b200 import dist as ebdist
-        per = args.rods if args.rods is not None else 16384
-        wl = ebdist.shard(W.CONFIGS[args.workload](n_rods=per * world, seed=1002), rank, world)
-    else:
-        wl = wl_fn(rank)
+    wl = bench_workload(args, W, rank, world)
     sim = wl.build(device=local, reference_rounding=args.reference_rounding, window=args.window,
                    step_mode="streaming")
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=torch.device("cuda", local))
