@@ -13,7 +13,11 @@ the oracle's step uses, checked one element at a time against
   ``correctness`` (lines 26-61: two directors a 120 deg rotation about
   (1, 1, 1) apart, divided by 0.25, epsilon 1.3e-10) and
   ``circle_in_two_dimensions`` (lines 62-135: 512 directors around a planar
-  circle in both senses, margin 1e-16 on top of Catch's default epsilon).
+  circle in both senses, margin 1e-16 on top of Catch's default epsilon);
+
+and, through the oracle's force evaluation, the pattern of
+``tests/Unit/Systems/CosseratRods/Components/Elasticity/Test_WithDiagonalLinearHyperElasticModel.cpp:183-249``
+(uniformly strained rods: loads at the end nodes only, equal interior torques).
 """
 import ctypes
 import math
@@ -141,3 +145,62 @@ def test_inv_rotate_divide_circle_in_two_dimensions(oracle_mod, sense):
         scale = np.linalg.norm(k)
         assert _catch(k / scale, axis, eps=100 * FLT_EPS, margin=1e-16), (i, k)
         assert _catch(scale, dtheta, eps=100 * FLT_EPS, margin=1e-16), (i, scale, dtheta)
+
+
+def _stretched_rod(oracle_mod, stretch: float, tilt: float = 0.0):
+    """One rod of 8 elements along +z, rest length 0.125 per element, every
+    node moved to ``stretch`` times its rest position (exactly representable
+    for the stretches used), every director turned by ``tilt`` about d1, at
+    rest (v = w = 0).  Returns the oracle's rod arrays with diagnostics on."""
+    n = 8
+    init = oracle_mod.straight_rod(n, (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), (1.0, 0.0, 0.0), 1.0, 0.05, 1000.0,
+                                   1e6, 1e6 / 3)
+    assert np.array_equal(init["x"][2], 0.125 * np.arange(n + 1))
+    rods = oracle_mod.RodArrays([n])
+    for key, src in (("mass", "mass"), ("rest_length", "l0"), ("rest_voronoi", "D0"), ("volume", "V"),
+                     ("shear_diag", "S"), ("bend_diag", "B"), ("inertia_diag", "J"), ("inv_inertia", "Jinv")):
+        rods.set_rod(key, 0, init[src])
+    rods.set_rod("x", 0, init["x"] * stretch)
+    c, s = math.cos(tilt), math.sin(tilt)
+    turn = np.array([[1.0, 0.0, 0.0], [0.0, c, s], [0.0, -s, c]])
+    q = init["Q"].transpose(2, 0, 1)  # (element, director, component)
+    q = np.einsum("ab,ebj->eaj", turn, q) if tilt else q
+    rods.set_rod("Q", 0, q.transpose(1, 2, 0).reshape(9, n))
+    rods.enable_diagnostics()
+    rods.force_eval()
+    return rods, init, n
+
+
+def test_uniform_stretch_loads_at_the_ends_only(oracle_mod):
+    """The pattern of the reference's elasticity component test
+    (Components/Elasticity/Test_WithDiagonalLinearHyperElasticModel.cpp:183-209):
+    a uniformly strained rod has internal loads +Q^T n_L / e on the first node,
+    the opposite on the last and exactly zero in between.  Pure stretch along
+    d3 gives n_L = (0, 0, S3 (e - 1)), no couple and no torque."""
+    rods, init, n = _stretched_rod(oracle_mod, 1.125)
+    loads = rods.get_diag("d_loads", 0, n + 1)
+    torques = rods.get_diag("d_torques", 0, n)
+    e = 1.125
+    s3 = init["S"][2, 0]
+    edge = np.array([0.0, 0.0, s3 * (e - 1.0) / e])
+    assert np.all(loads[:, 1:n] == 0.0)
+    assert _catch(loads[:, 0], edge, eps=1e-15, margin=1e-300)
+    assert np.array_equal(loads[:, n], -loads[:, 0])
+    assert np.all(torques == 0.0)
+
+
+def test_uniform_shear_interior_terms_cancel(oracle_mod):
+    """Directors turned uniformly against the tangent: every element carries
+    the same shear strain, so interior node loads cancel exactly and every
+    interior element sees the same torque (shear couple, no curvature
+    gradient), while the end elements differ by the boundary terms."""
+    rods, _, n = _stretched_rod(oracle_mod, 1.0, tilt=0.01)
+    loads = rods.get_diag("d_loads", 0, n + 1)
+    torques = rods.get_diag("d_torques", 0, n)
+    assert np.all(loads[:, 1:n] == 0.0)
+    assert np.array_equal(loads[:, n], -loads[:, 0])
+    assert np.abs(loads[1, 0]) > 0.0  # the shear component of n_L
+    mid = torques[:, 1]
+    for i in range(2, n - 1):
+        assert np.array_equal(torques[:, i], mid), i
+    assert np.abs(mid[0]) > 0.0  # (Q t) x n_L about d1
