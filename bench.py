@@ -231,12 +231,19 @@ def workload_config(wl, world):
 
 
 def mixed_comparison(W, eb, torch, args, rank, local, barrier, pg):
+    """The mixed batch (65,536 rods, n ~ U{64..256}, helical rest curvature,
+    end torque) advanced args.mixed_steps steps three ways from the same
+    initial state: the FP64 streaming drop-in (one launch a step), the FP64
+    default plan (the planner's choice, resident on this batch) and the
+    mixed-precision resident kernel.  Tip positions and total energies after
+    the run are compared with the FP64 default plan's."""
     wl = W.mixed_batch(n_rods=args.mixed_rods, seed=1003 + rank)
     out = {"workload": "mixed_batch", "rods": len(wl.rods), "elements": wl.total_elements, "dt": wl.dt,
-           "steps": args.mixed_steps, "untimed_steps_before": 1,
-           "dt_rule": "0.5 min(l^2 / (r c)); 1e-5 s is unstable for these rods in the FP64 reference path"}
+           "steps": args.mixed_steps,
+           "dt_rule": "0.5 min(l^2/(r c)); 1e-5 s is unstable for these rods in the FP64 reference path"}
     res = {}
-    for label, kw in (("fp64", {"step_mode": "streaming"}), ("mixed", {"precision": "mixed"})):
+    for label, kw in (("fp64_streaming", {"step_mode": "streaming"}), ("fp64_default", {}),
+                      ("mixed", {"precision": "mixed"})):
         sim = wl.build(device=local, **kw)
         # one untimed step: the step planner's one-off probes run here
         t0 = sim.step(eb.PositionVerlet(), 0.0, wl.dt, 1)
@@ -259,20 +266,26 @@ def mixed_comparison(W, eb, torch, args, rank, local, barrier, pg):
         res[label] = {"ms": float(ms.item()), "tips": tips, "e0": e0, "e1": e1, "plan": sim.step_plan()}
         sim.close()
     lengths = np.array([r.length for r in wl.rods])
-    err = np.linalg.norm(res["mixed"]["tips"] - res["fp64"]["tips"], axis=1) / lengths
+    ref = res["fp64_default"]
+    err = np.linalg.norm(res["mixed"]["tips"] - ref["tips"], axis=1) / lengths
+    err64 = np.linalg.norm(res["fp64_streaming"]["tips"] - ref["tips"], axis=1) / lengths
     n_el = float(wl.total_elements)
+    rate = {k: n_el * args.mixed_steps / (v["ms"] / 1e3) for k, v in res.items()}
     out.update({
-        "fp64_value": n_el * args.mixed_steps / (res["fp64"]["ms"] / 1e3),
-        "value": n_el * args.mixed_steps / (res["mixed"]["ms"] / 1e3),
-        "unit": UNIT,
+        "value": rate["mixed"], "unit": UNIT,
+        "fp64_streaming_value": rate["fp64_streaming"],
+        "fp64_default_value": rate["fp64_default"],
+        "fp64_default_plan": ref["plan"]["mode"],
+        "mixed_plan": res["mixed"]["plan"]["mode"],
         "tip_error_max": float(np.max(err)), "tip_error_p99": float(np.percentile(err, 99)),
-        "tip_error_definition": "|tip_mixed - tip_fp64| / rod length after all steps",
-        "energy_fp64": [res["fp64"]["e0"], res["fp64"]["e1"]], "energy_mixed": [res["mixed"]["e0"], res["mixed"]["e1"]],
-        "energy_rel_diff": abs(res["mixed"]["e1"] - res["fp64"]["e1"]) / abs(res["fp64"]["e1"]),
+        "tip_error_definition": "|tip_mixed - tip_fp64_default| / rod length after all steps",
+        "fp64_plans_tip_diff_max": float(np.max(err64)),
+        "energy_fp64": [ref["e0"], ref["e1"]], "energy_mixed": [res["mixed"]["e0"], res["mixed"]["e1"]],
+        "energy_rel_diff": abs(res["mixed"]["e1"] - ref["e1"]) / abs(ref["e1"]),
         "finite": bool(np.all(np.isfinite(err))),
-        "plan": res["mixed"]["plan"],
     })
-    out["speedup_vs_fp64_dropin"] = out["value"] / out["fp64_value"]
+    out["speedup_vs_fp64_streaming"] = rate["mixed"] / rate["fp64_streaming"]
+    out["speedup_vs_fp64_default"] = rate["mixed"] / rate["fp64_default"]
     return out
 
 
@@ -399,11 +412,27 @@ def _serve_request(eb, W, rng):
     return rods, vel, dt, steps, int(n.sum())
 
 
+def censored_percentiles(done: np.ndarray, censored: np.ndarray, qs=(50, 99)) -> dict:
+    """Percentiles of a latency sample in which some requests had not
+    finished when the run ended.  An unfinished request contributes its age
+    at the end, a lower bound on its latency, so each percentile taken over
+    every submitted request is a lower bound of the true one whenever any
+    request is censored (and exact when none is)."""
+    allv = np.concatenate([np.asarray(done, float), np.asarray(censored, float)])
+    if allv.size == 0:
+        return {f"p{q}": None for q in qs}
+    return {f"p{q}": float(np.percentile(allv, q)) for q in qs}
+
+
 def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
     """Poisson arrivals at `rate` requests/s for `seconds`, then up to
-    `drain_s` more seconds; latency = completion seen - scheduled arrival.
-    The requests are generated before the clock starts (building them is the
-    client's work, not the server's)."""
+    `drain_s` more seconds.  Latency = completion seen - scheduled arrival;
+    requests still unfinished at the end count with their age then (censored,
+    so the percentiles over all submitted requests are lower bounds).
+    Queueing delay = submission to first admission (server clock; still
+    queued: age at the end).  Each request is generated at its arrival time
+    (the client's work; the server's ticks run for hundreds of milliseconds
+    each at this load, so it does not delay them)."""
     from elasticapp_b200.server import Server
 
     srv = Server(precision="mixed", hbm_budget_bytes=budget)
@@ -414,16 +443,14 @@ def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
         if t >= seconds:
             break
         arrivals.append(t)
-    requests = [_serve_request(eb, W, np.random.Generator(np.random.PCG64(seed * 1000003 + i)))
-                for i in range(len(arrivals))]
-    arrival_of, lat, work = {}, [], 0.0
+    arrival_of, lat, qdelay, work = {}, [], [], 0.0
     nxt = 0
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         while nxt < len(arrivals) and arrivals[nxt] <= now:
-            rods, vel, dt, steps, elems = requests[nxt]
-            requests[nxt] = None
+            rods, vel, dt, steps, elems = _serve_request(
+                eb, W, np.random.Generator(np.random.PCG64(seed * 1000003 + nxt)))
             rid = srv.submit(rods, dt, steps, gravity=(0.0, 0.0, -9.81), clamp=True, damper=(0.1, 0.1),
                              velocities=vel)
             arrival_of[rid] = arrivals[nxt]
@@ -435,27 +462,40 @@ def serve_stream(eb, W, rate, seconds, drain_s, seed, budget):
             seen = time.perf_counter() - t0
             for c in done:
                 lat.append(seen - arrival_of.pop(c["request_id"]))
+                qdelay.append(c["queued_s"])
                 srv.release(c["request_id"])
         if (nxt == len(arrivals) and left == 0) or now > seconds + drain_s:
             break
-    elapsed = time.perf_counter() - t0
+    end = time.perf_counter() - t0
+    # requests still in flight: latency and queueing delay censored at the end
+    cens_lat, cens_q, never_admitted = [], [], 0
+    for rid, arr in arrival_of.items():
+        info = srv.request_status(rid)
+        cens_lat.append(end - arr)
+        cens_q.append(info["queued_s"])
+        never_admitted += info["state"] == "queued"
     st = srv.stats()
     srv.close()
-    lat = np.array(lat) if lat else np.array([np.nan])
-    return {"rate_req_s": rate, "arrival_window_s": seconds, "submitted": len(arrivals),
-            "completed": int(st["completed"]), "in_flight_at_end": len(arrivals) - int(st["completed"]),
-            "fallbacks": int(st["fallbacks"]), "p50_latency_s": float(np.nanpercentile(lat, 50)),
-            "p99_latency_s": float(np.nanpercentile(lat, 99)), "elapsed_s": elapsed,
-            "value": st["element_steps"] / elapsed, "unit": UNIT,
+    lp = censored_percentiles(lat, cens_lat)
+    qp = censored_percentiles(qdelay, cens_q)
+    label = "censored_lower_bound" if cens_lat else "exact"
+    return {"rate_req_s": rate, "arrival_window_s": seconds, "drain_s": drain_s, "submitted": len(arrivals),
+            "completed": len(lat), "censored": len(cens_lat), "never_admitted": int(never_admitted),
+            "fallbacks": int(st["fallbacks"]),
+            "p50_latency_s": lp["p50"], "p99_latency_s": lp["p99"], "latency_percentiles": label,
+            "p50_latency_completed_s": float(np.percentile(lat, 50)) if lat else None,
+            "p99_latency_completed_s": float(np.percentile(lat, 99)) if lat else None,
+            "p99_queueing_s": qp["p99"], "p50_queueing_s": qp["p50"],
+            "elapsed_s": end, "value": st["element_steps"] / end, "unit": UNIT,
             "offered_element_steps_per_s": work / max(seconds, 1e-9), "ticks": int(st["ticks"]),
             "bins_total": int(st["bins_total"]), "kernel_seconds": st["kernel_seconds"],
-            "gpu_busy_frac": st["kernel_seconds"] / elapsed,
+            "gpu_busy_frac": st["kernel_seconds"] / end,
             "kernel_element_steps_per_s": st["element_steps"] / max(st["kernel_seconds"], 1e-9)}
 
 
 def serving_section(eb, W, args, capacity_hint):
     """The serving stream at the stated load (200 requests/s) for a bounded
-    window, and at a sustainable load (half the measured capacity)."""
+    arrival window, and at a sustainable load (half the measured capacity)."""
     out = {"workload": "serve_stream", "hbm_budget_bytes": args.serve_budget, "precision": "mixed (FP64 fallback)",
            "steps_per_launch": 128,
            "request": "1-256 rods log-uniform, n ~ U{32..1024} (520-slot bins, one CTA each; rods of 520 or more "
@@ -464,8 +504,57 @@ def serving_section(eb, W, args, capacity_hint):
     mean_work = 46.0 * 528.0 * 50500.0  # mean rods x mean n x mean horizon
     out["stated_load"] = serve_stream(eb, W, 200.0, args.serve_seconds, args.serve_drain, 1005, args.serve_budget)
     rate = args.serve_rate if args.serve_rate > 0 else max(1.0, 0.5 * capacity_hint / mean_work)
-    out["sustained_load"] = serve_stream(eb, W, rate, args.serve_seconds, args.serve_drain, 1006, args.serve_budget)
+    out["sustained_load"] = serve_stream(eb, W, rate, args.serve_sustained_seconds, args.serve_drain, 1006,
+                                         args.serve_budget)
     return out
+
+
+def _pick(d, keys):
+    return None if d is None else {k: d[k] for k in keys if k in d}
+
+
+def compact_sections(batched, contact, serving, cantilever, mixed):
+    """The side measurements reduced to their figures, so that the whole
+    bench line stays short (the full sections go to --detail-out)."""
+    out = {}
+    if batched is not None:
+        out["batched"] = {"value": batched["value"], "plan": batched["plan"]["mode"],
+                          "ms_per_step": batched["ms_per_step"],
+                          "pefrl_default": batched["pefrl"]["default_plan"]["value"],
+                          "pefrl_streaming": batched["pefrl"]["streaming"]["value"]}
+    if contact is not None:
+        out["contact"] = _pick(contact, ("value", "ms_per_step", "candidate_pairs", "launches_per_step"))
+        if contact.get("cpu_baseline"):
+            out["contact"]["cpu_value"] = contact["cpu_baseline"]["value"]
+    if cantilever is not None:
+        out["cantilever"] = {"value": cantilever["value"],
+                             "tip_err_max": cantilever["tip_trajectory"]["max_rel_error"],
+                             "cpu_value": cantilever["cpu_baseline"]["value"]}
+    if serving is not None:
+        keys = ("rate_req_s", "arrival_window_s", "submitted", "completed", "censored", "p50_latency_s",
+                "p99_latency_s", "latency_percentiles", "p99_queueing_s", "value", "gpu_busy_frac", "fallbacks")
+        out["serving"] = {"stated": _pick(serving["stated_load"], keys),
+                          "sustained": _pick(serving["sustained_load"], keys)}
+    if mixed is not None:
+        out["mixed"] = _pick(mixed, ("rods", "elements", "steps", "dt", "value", "fp64_default_value",
+                                     "fp64_streaming_value", "fp64_default_plan", "speedup_vs_fp64_default",
+                                     "speedup_vs_fp64_streaming", "tip_error_max", "tip_error_p99",
+                                     "energy_rel_diff", "finite"))
+    return out
+
+
+def relaunch_under_torchrun(n: int, argv) -> int:
+    """bench.py --gpus N started without a launcher: run N ranks on this node
+    with torch.distributed.run (rendezvous on 127.0.0.1) and return its exit
+    status.  Rank 0 prints the line."""
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+    return subprocess.run(cmd, check=False).returncode
 
 
 def main(argv=None) -> int:
@@ -489,8 +578,10 @@ def main(argv=None) -> int:
                     help="timed steps of the contact batch (each from its initial state); 0 skips it")
     ap.add_argument("--cantilever-steps", type=int, default=100000,
                     help="steps of the single-rod cantilever; 0 skips it")
-    ap.add_argument("--serve-seconds", type=float, default=15.0,
-                    help="arrival window of each serving stream; 0 skips serving")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="arrival window of the stated-load serving stream; 0 skips serving")
+    ap.add_argument("--serve-sustained-seconds", type=float, default=30.0,
+                    help="arrival window of the sustained-load serving stream")
     ap.add_argument("--serve-drain", type=float, default=30.0, help="extra seconds to finish in-flight requests")
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="sustained-load arrival rate (0: half the measured mixed capacity)")
@@ -500,8 +591,18 @@ def main(argv=None) -> int:
     ap.add_argument("--reference-rounding", action="store_true",
                     help="FP64 build that rounds every operation as the reference's scalar code")
     ap.add_argument("--window", type=int, default=0, help="slots per CTA of the step kernel (128/256)")
+    ap.add_argument("--detail-out", default=None, help="also write every section in full to this JSON file")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
+
+    # --gpus N is the number of ranks: started without a launcher, relaunch
+    # under torch.distributed.run; under a launcher, the world size must agree
+    launched = "WORLD_SIZE" in os.environ
+    if not launched and args.gpus > 1:
+        return relaunch_under_torchrun(args.gpus, sys.argv[1:] if argv is None else argv)
+    if launched and int(os.environ["WORLD_SIZE"]) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={os.environ['WORLD_SIZE']}", file=sys.stderr)
+        return 2
 
     from elasticapp_b200 import workloads as W
 
@@ -703,8 +804,7 @@ def main(argv=None) -> int:
             "config": workload_config(wl, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                         else "fallback 6.65 TB/s",
+                         "peak_source": f"{peak_kind} hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "kernel": "rod_step_fp64" + ("_reference" if args.reference_rounding else ""),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": cpu,
@@ -714,13 +814,15 @@ def main(argv=None) -> int:
             "gpu_launches": launches,
             "clocks": clock_info,
             "state_finite": bool(finite),
-            "batched": batched,
-            "mixed": mixed,
-            "contact": contact,
-            "serving": serving,
-            "cantilever": cantilever,
         }
-        print(json.dumps(line), flush=True)
+        if args.detail_out:
+            full = dict(line, batched=batched, contact=contact, serving=serving, cantilever=cantilever,
+                        mixed=mixed)
+            with open(args.detail_out, "w", encoding="utf-8") as f:
+                json.dump(full, f, indent=1)
+        # the side measurements in short form, the mixed-precision target last
+        line.update(compact_sections(batched, contact, serving, cantilever, mixed))
+        print(json.dumps(line, separators=(",", ":")), flush=True)
     if sim is not None:
         sim.close()
     return 0

@@ -99,7 +99,8 @@ class EbRequest(ctypes.Structure):
 class EbCompletion(ctypes.Structure):
     _fields_ = [("request_id", ctypes.c_int64), ("precision", ctypes.c_int32), ("fell_back", ctypes.c_int32),
                 ("latency_s", ctypes.c_double), ("energy_initial", ctypes.c_double),
-                ("energy_final", ctypes.c_double), ("elements", ctypes.c_int64), ("steps", ctypes.c_int64)]
+                ("energy_final", ctypes.c_double), ("elements", ctypes.c_int64), ("steps", ctypes.c_int64),
+                ("queued_s", ctypes.c_double)]
 
 
 class EbServerStats(ctypes.Structure):
@@ -177,6 +178,8 @@ SIGNATURES = {
                           ctypes.c_int64], ctypes.c_int),
     "eb_server_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
     "eb_server_get_stats": ([ctypes.c_void_p, _P(EbServerStats)], ctypes.c_int),
+    "eb_server_request_status": ([ctypes.c_void_p, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_double),
+                                  _P(ctypes.c_double)], ctypes.c_int),
     "eb_snapshot_size": ([_sim, _P(ctypes.c_uint64)], ctypes.c_int),
     "eb_snapshot_save": ([_sim, ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
     "eb_snapshot_load": ([_sim, ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),

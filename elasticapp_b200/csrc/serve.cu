@@ -201,6 +201,7 @@ struct Request {
   bool damped = false;
   Clock::time_point t_submit;
   double latency_s = 0.0;
+  double queued_s = -1.0;  // submission to first admission; < 0 until admitted
   ReqState state = kQueued;
   // placement: units of one bin, or of a bin pair holding one long rod
   std::vector<int64_t> bins;        // first bin of each unit
@@ -498,6 +499,7 @@ eb_status admit(eb_server* s) {
     r.steps_done = 0;
     r.damped = false;
     if (eb_status e = place(s, r)) return e;
+    if (r.queued_s < 0.0) r.queued_s = std::chrono::duration<double>(Clock::now() - r.t_submit).count();
     r.state = kActive;
     s->queue.pop_front();
     s->active.push_back(&r);
@@ -619,6 +621,7 @@ void land(eb_server* s, Request& r) {
   c.precision = r.precision;
   c.fell_back = r.fell_back ? 1 : 0;
   c.latency_s = r.latency_s;
+  c.queued_s = r.queued_s;
   c.energy_initial = E0;
   c.energy_final = E1;
   c.elements = r.elements;
@@ -917,6 +920,19 @@ EB_API eb_status eb_server_release(eb_server* s, int64_t request_id) {
   if (it->second->state != kDone) return fail(EB_ERR_INVALID_STATE, "request not completed");
   if (it->second->event) cudaEventDestroy(it->second->event);
   s->requests.erase(it);
+  return EB_OK;
+}
+
+EB_API eb_status eb_server_request_status(const eb_server* s, int64_t request_id, int32_t* state,
+                                          double* age_s, double* queued_s) {
+  if (!s || !state) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
+  auto it = s->requests.find(request_id);
+  if (it == s->requests.end()) return fail(EB_ERR_NOT_FOUND, "unknown request");
+  const Request& r = *it->second;
+  const double age = std::chrono::duration<double>(Clock::now() - r.t_submit).count();
+  *state = static_cast<int32_t>(r.state);
+  if (age_s) *age_s = r.state == kDone ? r.latency_s : age;
+  if (queued_s) *queued_s = r.queued_s >= 0.0 ? r.queued_s : age;
   return EB_OK;
 }
 

@@ -84,7 +84,8 @@ class Server:
         n = ctypes.c_int32()
         L.call("eb_server_poll", self._h, buf, capacity, ctypes.byref(n))
         return [{"request_id": c.request_id, "precision": _NAMES[c.precision], "fell_back": bool(c.fell_back),
-                 "latency_s": c.latency_s, "energy_initial": c.energy_initial, "energy_final": c.energy_final,
+                 "latency_s": c.latency_s, "queued_s": c.queued_s, "energy_initial": c.energy_initial,
+                 "energy_final": c.energy_final,
                  "elements": c.elements, "steps": c.steps} for c in buf[:n.value]]
 
     def result(self, request_id: int, rod: int, name: str) -> np.ndarray:
@@ -99,6 +100,17 @@ class Server:
     def release(self, request_id: int) -> None:
         L.call("eb_server_release", self._h, int(request_id))
         self._rods.pop(request_id, None)
+
+    _STATES = ("queued", "active", "finishing", "done")
+
+    def request_status(self, request_id: int) -> dict:
+        """Where a request is (queued, active, finishing, done), its age (its
+        latency once done) and its queueing delay (a lower bound while it is
+        still queued)."""
+        st, age, q = ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+        L.call("eb_server_request_status", self._h, int(request_id), ctypes.byref(st), ctypes.byref(age),
+               ctypes.byref(q))
+        return {"state": self._STATES[st.value], "age_s": age.value, "queued_s": q.value}
 
     def stats(self) -> dict:
         st = L.EbServerStats()

@@ -467,6 +467,7 @@ typedef struct eb_completion {
   double energy_final;
   int64_t elements;
   int64_t steps;
+  double queued_s;            /* submission to first admission (time spent waiting for bins) */
 } eb_completion;
 
 typedef struct eb_server_stats {
@@ -488,6 +489,17 @@ EB_API eb_status eb_server_result(struct eb_server* server, int64_t request_id, 
                                   double* values, int64_t count);
 EB_API eb_status eb_server_release(struct eb_server* server, int64_t request_id);
 EB_API eb_status eb_server_get_stats(const struct eb_server* server, eb_server_stats* out);
+/* where a request is: *state 0 queued (not yet admitted), 1 active,
+ * 2 finishing, 3 done; *age_s (optional) the time since submission (the
+ * latency once done); *queued_s (optional) the time from submission to its
+ * first admission, or since submission while it is still queued (a lower
+ * bound on its queueing delay) */
+#define EB_REQUEST_QUEUED 0
+#define EB_REQUEST_ACTIVE 1
+#define EB_REQUEST_FINISHING 2
+#define EB_REQUEST_DONE 3
+EB_API eb_status eb_server_request_status(const struct eb_server* server, int64_t request_id, int32_t* state,
+                                          double* age_s, double* queued_s);
 
 /* --- candidate pairs of caller-provided boxes, allocating nothing.  No
  * counterpart in the reference: it is the collision system's broad phase

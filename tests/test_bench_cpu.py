@@ -55,3 +55,62 @@ def test_reference_arm_two_ranks_rank0_shard():
     _check_line(line, 2, line["config"]["rods"])
     assert 64 <= line["config"]["rods"] <= 192
     assert line["cpu_baseline"]["sample"].startswith("rank 0 shard")
+
+
+def test_gpus_flag_without_launcher_runs_that_many_ranks():
+    """--gpus N without torchrun relaunches itself as N ranks on this node
+    (the line reports n_gpus == N)."""
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--rods", "128",
+                        "--steps", "1", "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    _check_line(lines[0], 2, lines[0]["config"]["rods"])
+
+
+def test_gpus_flag_disagreeing_with_launcher_is_refused():
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--rods", "16",
+                        "--steps", "1", "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=300,
+                       env=env)
+    assert r.returncode != 0
+    assert "WORLD_SIZE" in r.stderr
+
+
+def test_censored_percentiles_are_lower_bounds():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    done = [1.0, 2.0, 3.0]
+    # no censoring: ordinary percentiles
+    assert bench.censored_percentiles(done, [])["p50"] == 2.0
+    # two requests still running at ages 10 and 20: they enter with their ages
+    p = bench.censored_percentiles(done, [10.0, 20.0])
+    assert p["p50"] == 3.0 and p["p99"] > 10.0
+    assert bench.censored_percentiles([], [])["p99"] is None
+
+
+def test_compact_line_fits_the_tail():
+    """The printed line with every side section in short form stays short."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    serving = {k: {"rate_req_s": 200.0, "arrival_window_s": 60.0, "submitted": 12000, "completed": 700,
+                   "censored": 11300, "p50_latency_s": 31.123456789, "p99_latency_s": 59.123456789,
+                   "latency_percentiles": "censored_lower_bound", "p99_queueing_s": 58.1234567, "value": 1.7e10,
+                   "gpu_busy_frac": 0.91234567, "fallbacks": 1, "ticks": 5}
+               for k in ("stated_load", "sustained_load")}
+    mixed = {"rods": 65536, "elements": 10473311, "steps": 10000, "dt": 4.6e-7, "value": 2.7e10,
+             "fp64_default_value": 1.3e10, "fp64_streaming_value": 9.6e9, "fp64_default_plan": "resident",
+             "speedup_vs_fp64_default": 2.0123456, "speedup_vs_fp64_streaming": 2.88123456,
+             "tip_error_max": 1.1e-7, "tip_error_p99": 4.7e-8, "energy_rel_diff": 2.3e-8, "finite": True,
+             "energy_fp64": [1.0, 2.0]}
+    batched = {"value": 1.5e10, "plan": {"mode": "resident", "probe_ms": [0.0] * 20}, "ms_per_step": 0.29,
+               "pefrl": {"default_plan": {"value": 4e9}, "streaming": {"value": 2.4e9}}}
+    contact = {"value": 6.3e8, "ms_per_step": 0.83, "candidate_pairs": 1211410, "launches_per_step": 13,
+               "cpu_baseline": {"value": 1.1e6}}
+    cant = {"value": 3.6e7, "tip_trajectory": {"max_rel_error": 3e-14}, "cpu_baseline": {"value": 5.6e6}}
+    sec = bench.compact_sections(batched, contact, {"stated_load": serving["stated_load"],
+                                                    "sustained_load": serving["sustained_load"]}, cant, mixed)
+    assert list(sec)[-1] == "mixed"
+    assert len(json.dumps(sec, separators=(",", ":"))) < 1500

@@ -4,8 +4,9 @@ The mixed path keeps the state (x, v, Q, w) and the cancellation-prone
 quantities in FP64 and the element-local arithmetic in FP32.  Its accuracy
 requirement: tip positions within 1e-5 of the FP64 path after 10^4 steps,
 relative to the rod length, on rods shaped like the 65,536-rod mixed batch
-(n ~ U{64..256}, helical rest curvature up to 10 1/m, end torque 1e-3 N m,
-dt = 1e-5 s)."""
+(n ~ U{64..256}, helical rest curvature up to 10 1/m, end torque 1e-3 N m),
+at the batch's step dt = 0.5 min(l^2 / (r c)), about 4.6e-7 s: at 1e-5 s
+these rods are unstable in FP64 as well."""
 import numpy as np
 import pytest
 

@@ -140,3 +140,39 @@ def test_serve_error_paths(eb):
     with pytest.raises(EbError):
         srv.submit([long_rod], dt, 10)
     srv.close()
+
+
+def test_request_status_and_queueing_delay(eb):
+    """A request waiting for bins reports 'queued' with its age as a lower
+    bound on its queueing delay; once done its completion carries the
+    delay from submission to admission, no longer than its latency."""
+    from elasticapp_b200.server import Server
+    srv = Server(hbm_budget_bytes=2.0e6)  # a few bins: the second request waits
+    n_bins = srv.stats()["bins_total"]
+    # one rod of 300-500 elements a bin (two do not fit in 512 slots): the
+    # first request takes every bin
+    r1 = _request(500, n_bins, (300, 500))
+    r2 = _request(501, 1, (100, 300))
+    a = srv.submit(r1[0], r1[2], 300, velocities=r1[1])
+    b = srv.submit(r2[0], r2[2], 300, velocities=r2[1])
+    srv.tick()
+    sa, sb = srv.request_status(a), srv.request_status(b)
+    assert sa["state"] in ("active", "finishing", "done")
+    assert sb["state"] == "queued" and sb["queued_s"] >= 0.0
+    done = {}
+    for _ in range(10000):
+        left = srv.tick()
+        for c in srv.poll():
+            done[c["request_id"]] = c
+        if left == 0:
+            break
+    done.update({c["request_id"]: c for c in srv.poll()})
+    assert set(done) == {a, b}
+    for rid in (a, b):
+        c = done[rid]
+        assert 0.0 <= c["queued_s"] <= c["latency_s"]
+        assert srv.request_status(rid)["state"] == "done"
+    assert done[b]["queued_s"] >= sb["queued_s"]
+    with pytest.raises(Exception):
+        srv.request_status(123456)
+    srv.close()
