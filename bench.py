@@ -58,17 +58,37 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+def source_digest(*names: str) -> str:
+    """First 16 hex digits of the SHA-256 of the named kernel sources."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for n in names:
+        with open(os.path.join(ROOT, "elasticapp_b200", "csrc", n), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def profile_traffic(kernel: str, workload: str, sources: tuple):
+    """DRAM bytes per launch from the committed ncu summary of this kernel
+    and workload, if its recorded source digest matches the kernel sources
+    as they are now (a summary of an older kernel is not reported).
+    Returns (bytes or None, note)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    traffic, digest = None, None
     try:
         with open(path, encoding="utf-8") as f:
             for line in f:
                 if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].strip())
+                    traffic = float(line.split(":", 1)[1].strip())
+                elif line.startswith("source_digest:"):
+                    digest = line.split(":", 1)[1].strip()
     except OSError:
-        pass
-    return None
+        return None, "no ncu summary"
+    now = source_digest(*sources)
+    if digest != now:
+        return None, f"ncu summary is of other kernel sources ({digest} != {now})"
+    return traffic, f"ncu capture of these sources ({now}), profiles/{kernel}_{workload}.txt"
 
 
 class ClockSampler:
@@ -669,7 +689,8 @@ def main(argv=None) -> int:
     alg = algorithmic_bytes(wl.n_elements, damped=False)
     per_launch_s = (ms / 1e3) / args.steps
     achieved = alg / per_launch_s / 1e9
-    traffic = profile_traffic("rod_step_fp64", wl.name)
+    traffic, traffic_note = profile_traffic("rod_step_fp64", wl.name,
+                                            ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh", "eb_internal.h"))
 
     # ---- end to end through the public API with host buffers: each cycle
     # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE
@@ -805,6 +826,7 @@ def main(argv=None) -> int:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "traffic_source": traffic_note,
                          "kernel": "rod_step_fp64" + ("_reference" if args.reference_rounding else ""),
                          "algorithmic_bytes_per_launch": alg},
             "cpu_baseline": cpu,

@@ -7,8 +7,9 @@ fallback.
 """
 from .simulator import (AnalyticalLinearDamper, Clamp, CollisionSystem, ContactMaterial, CosseratRod,
                         CosseratRodWithoutDamping, EndTorque, FreeJoint, GravityField, HingeJoint, Material, PEFRL,
+                        VelocityVerlet,
                         PositionVerlet, RodRef, Simulator, StraightRod)
 from . import _lib
 
 __all__ = ["AnalyticalLinearDamper", "Clamp", "CollisionSystem", "ContactMaterial", "CosseratRod", "CosseratRodWithoutDamping", "EndTorque",
-           "FreeJoint", "GravityField", "HingeJoint", "Material", "PEFRL", "PositionVerlet", "RodRef", "Simulator", "StraightRod", "_lib"]
+           "FreeJoint", "GravityField", "HingeJoint", "Material", "PEFRL", "PositionVerlet", "RodRef", "VelocityVerlet", "Simulator", "StraightRod", "_lib"]

@@ -16,6 +16,8 @@ EB_OK = 0
 STATUS_NAMES = {0: "EB_OK", 1: "EB_ERR_INVALID_ARGUMENT", 2: "EB_ERR_INVALID_STATE",
                 3: "EB_ERR_UNSUPPORTED", 4: "EB_ERR_OUT_OF_MEMORY", 5: "EB_ERR_CUDA",
                 6: "EB_ERR_NOT_FOUND", 7: "EB_ERR_NUMERICAL"}
+EB_ERR_INVALID_ARGUMENT = 1
+EB_ERR_CUDA = 5
 
 EB_PRECISION_FP64 = 0
 EB_PRECISION_MIXED = 1
@@ -27,6 +29,7 @@ EB_FLAG_CUDA_GRAPH = 0x10
 EB_FLAG_STEP_BUCKETED = 0x20
 EB_STEPPER_POSITION_VERLET = 0
 EB_STEPPER_PEFRL = 1
+EB_STEPPER_VELOCITY_VERLET = 2
 EB_ROD_DAMPED = 0
 EB_ROD_UNDAMPED = 1
 EB_LAYOUT_PER_ROD = 0
@@ -153,6 +156,7 @@ SIGNATURES = {
     "eb_constrain_clamp": ([_sim, ctypes.c_int64, ctypes.c_int64], ctypes.c_int),
     "eb_add_gravity": ([_sim, _P(ctypes.c_double)], ctypes.c_int),
     "eb_add_end_torque": ([_sim, ctypes.c_int64, _P(ctypes.c_double)], ctypes.c_int),
+    "eb_add_element_torque": ([_sim, ctypes.c_int64, ctypes.c_int64, _P(ctypes.c_double)], ctypes.c_int),
     "eb_add_analytical_damper": ([_sim, ctypes.c_int64, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "eb_add_contact_material": ([_sim, _P(EbContactMaterial), _P(ctypes.c_int32)], ctypes.c_int),
     "eb_add_rod_contact": ([_sim, ctypes.c_int64, ctypes.c_int32], ctypes.c_int),
@@ -169,6 +173,7 @@ SIGNATURES = {
     "eb_get_stream": ([_sim, _P(ctypes.c_void_p)], ctypes.c_int),
     "eb_step_plan": ([_sim, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_float), ctypes.c_int32], ctypes.c_int),
     "eb_launch_count": ([_sim, _P(ctypes.c_int64)], ctypes.c_int),
+    "eb_debug_set_wait_bound": ([_sim, ctypes.c_uint32], ctypes.c_int),
     "eb_server_create": ([_P(EbServerConfig), _P(ctypes.c_void_p)], ctypes.c_int),
     "eb_server_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "eb_server_submit": ([ctypes.c_void_p, _P(EbRequest), _P(ctypes.c_int64)], ctypes.c_int),

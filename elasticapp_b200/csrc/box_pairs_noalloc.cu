@@ -201,8 +201,36 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const double* boxes, 
   for (int d = 0; d < 6; ++d) s.sorted_box[6 * pos + d] = boxes[6 * i + d];
 }
 
+// Sort the partners (second entries) of one box's pair segment in place,
+// ascending: heapsort, O(c log c) for c partners and no extra memory (the
+// first entries are all the box's own index).
+__device__ void sort_partners(int64_t* seg, int32_t c) {
+  auto sift = [seg](int32_t root, int32_t end) {
+    while (true) {
+      int32_t child = 2 * root + 1;
+      if (child >= end) return;
+      if (child + 1 < end && seg[2 * child + 1] < seg[2 * child + 3]) ++child;
+      if (seg[2 * root + 1] >= seg[2 * child + 1]) return;
+      const int64_t t = seg[2 * root + 1];
+      seg[2 * root + 1] = seg[2 * child + 1];
+      seg[2 * child + 1] = t;
+      root = child;
+    }
+  };
+  for (int32_t k = c / 2 - 1; k >= 0; --k) sift(k, c);
+  for (int32_t end = c - 1; end > 0; --end) {
+    const int64_t t = seg[1];
+    seg[1] = seg[2 * end + 1];
+    seg[2 * end + 1] = t;
+    sift(0, end);
+  }
+}
+
 // every box counts (pass 1) or writes (pass 2) its partners with a larger
-// index; the written segment of box i is sorted by partner
+// index; the written segment of box i is sorted by partner.  The cell edge
+// is the largest box extent, so one very large box puts many boxes in one
+// cell: the search then costs up to O(n) per box (O(n^2) in all), which the
+// box limit bounds.
 template <bool kWrite>
 __global__ void __launch_bounds__(kThreads) pairs_kernel(int64_t n, Scratch s, int64_t* pairs, int64_t capacity) {
   const int64_t e = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
@@ -239,15 +267,7 @@ __global__ void __launch_bounds__(kThreads) pairs_kernel(int64_t n, Scratch s, i
   if constexpr (!kWrite) {
     s.pair_count[id] = cnt;
   } else {
-    for (int32_t a = 1; a < cnt; ++a) {
-      const int64_t v = out[2 * a + 1];
-      int32_t b = a - 1;
-      while (b >= 0 && out[2 * b + 1] > v) {
-        out[2 * (b + 1) + 1] = out[2 * b + 1];
-        --b;
-      }
-      out[2 * (b + 1) + 1] = v;
-    }
+    sort_partners(out, cnt);
   }
 }
 

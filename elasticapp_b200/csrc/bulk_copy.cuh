@@ -24,6 +24,13 @@ __device__ __forceinline__ void mbar_fence_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// order this thread's earlier generic-proxy accesses to shared memory before
+// later async-proxy (bulk copy) writes to it: needed before a buffer that
+// threads have read or written is refilled by a bulk copy
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                : "memory");
@@ -39,6 +46,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "r"(smem_addr(bar)), "r"(parity)
       : "memory");
   return done != 0;
+}
+
+// Non-blocking test of the barrier phase.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Test the barrier phase at most `tests` times without blocking (a small
+// count gives up before copies issued just before can land).
+__device__ __forceinline__ bool mbar_test_bounded(uint64_t* bar, uint32_t parity, uint32_t tests) {
+  for (uint32_t i = 0; i < tests; ++i)
+    if (mbar_test_wait(bar, parity)) return true;
+  return false;
 }
 
 // Wait for the barrier phase with an iteration cap.  Returns false when the

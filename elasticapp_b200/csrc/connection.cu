@@ -36,10 +36,8 @@ struct P3 {
 
 __device__ __forceinline__ P3 node_position(const JointArgs& a, int64_t g) {
   const uint32_t m = a.meta[g];
-  if (m & kFirst) {
-    const RodInfo& ri = a.rods[m >> kRodShift];
-    if (ri.flags & kRodClamp) return {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
-  }
+  double t[3];
+  if (clamp_position(a.rods[m >> kRodShift], g, t)) return {t[0], t[1], t[2]};
   const int64_t S = a.stride;
   const double* in = a.state;
   return {in[kStX * S + g] + a.pre * in[kStV * S + g], in[(kStX + 1) * S + g] + a.pre * in[(kStV + 1) * S + g],

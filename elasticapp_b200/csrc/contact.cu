@@ -129,11 +129,14 @@ __global__ void __launch_bounds__(kThreads) capsule_kernel(const ContactArgs a) 
     // positions after the first half drift (PositionVerlet.hpp:60-69) and
     // the clamp's value constraint
     D3 x0 = {x[s] + c * v[s], x[S + s] + c * v[S + s], x[2 * S + s] + c * v[2 * S + s]};
-    const D3 x1 = {x[s + 1] + c * v[s + 1], x[S + s + 1] + c * v[S + s + 1], x[2 * S + s + 1] + c * v[2 * S + s + 1]};
+    D3 x1 = {x[s + 1] + c * v[s + 1], x[S + s + 1] + c * v[S + s + 1], x[2 * S + s + 1] + c * v[2 * S + s + 1]};
     const uint32_t meta = a.meta[s];
-    if ((meta & kFirst) && (a.sim_flags & kSimClamp)) {
+    if (a.sim_flags & kSimClamp) {
+      // either node of the element may be held by a clamp
       const RodInfo& ri = a.rods[meta >> kRodShift];
-      if (ri.flags & kRodClamp) x0 = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+      double t[3];
+      if (clamp_position(ri, s, t)) x0 = {t[0], t[1], t[2]};
+      if (clamp_position(ri, s + 1, t)) x1 = {t[0], t[1], t[2]};
     }
     const D3 dx = x1 - x0;
     const double l = norm3(dx);

@@ -25,6 +25,8 @@
 
 namespace eb {
 cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream);
+cudaError_t launch_check_inverse_inertia(int64_t stride, int64_t n_slots, const double* par, const uint32_t* meta,
+                                         uint32_t* mismatch, cudaStream_t stream);
 cudaError_t launch_rod_step_fp64_reference(const StepArgs& args, bool diag, bool damped, int window,
                                            cudaStream_t stream);
 int block_config_count();
@@ -111,6 +113,11 @@ struct RodHost {
   // local slot-layout arrays: field f component c at (f + c) * (n + 1) + j
   std::vector<double> state, param, diag;
   eb::RodInfo info{};
+  // rod-local index of each clamp (node k, and element k when k < n; -1:
+  // none) and the element the torque acts on; the global slots are filled
+  // in when the rod table is uploaded
+  int64_t clamp_index[2] = {-1, -1};
+  int64_t torque_index = -1;
   double damper_nu_t = 0.0;
   int32_t contact_material = -1;  // collision-system material, -1: no contact
 };
@@ -183,6 +190,13 @@ struct eb_sim {
   int64_t* d_offsets = nullptr;
   double* d_energy = nullptr;
   uint32_t* d_status = nullptr;
+  // the streaming kernel forms 1 / J unless a stored J^-1 differs from it
+  // (a caller set J or J^-1 after the initializer): then it reads the stored
+  // rows.  jinv_dirty: J or J^-1 changed on the device since the last check
+  bool stored_jinv = false;
+  bool jinv_dirty = false;
+  uint32_t* d_jinv_flag = nullptr;
+  uint32_t max_polls = 0;  // bounded-wait polls of the streaming kernel (0: built in)
   int cur = 0;
   double damper_dt = -1.0;
   int64_t launches = 0;
@@ -397,6 +411,8 @@ void host_free(eb_sim* s) {
   if (s->d_energy) cudaFree(s->d_energy);
   if (s->d_status) cudaFree(s->d_status);
   s->d_status = nullptr;
+  if (s->d_jinv_flag) cudaFree(s->d_jinv_flag);
+  s->d_jinv_flag = nullptr;
   {
     std::vector<void*> owned;
     for (auto* p : s->d_cta_start) owned.push_back(p);
@@ -466,7 +482,13 @@ eb_status check_device_status(eb_sim* s) {
 
 eb_status upload_rod_table(eb_sim* s) {
   std::vector<eb::RodInfo> info(s->rods.size());
-  for (size_t r = 0; r < s->rods.size(); ++r) info[r] = s->rods[r].info;
+  for (size_t r = 0; r < s->rods.size(); ++r) {
+    const RodHost& R = s->rods[r];
+    info[r] = R.info;
+    for (int c = 0; c < 2; ++c)
+      info[r].clamp_slot[c] = R.clamp_index[c] >= 0 ? s->offsets[r] + R.clamp_index[c] : -1;
+    info[r].torque_slot = R.torque_index >= 0 ? s->offsets[r] + R.torque_index : -1;
+  }
   EB_CUDA(cudaMemcpyAsync(s->d_rods, info.data(), info.size() * sizeof(eb::RodInfo),
                           cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
@@ -623,10 +645,11 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
     return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
   if (cfg.precision == EB_PRECISION_MIXED && (cfg.flags & (EB_FLAG_REFERENCE_ROUNDING | EB_FLAG_STEP_STREAMING)))
     return fail(EB_ERR_INVALID_ARGUMENT, "mixed precision runs on the resident kernels only");
-  if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.stepper != EB_STEPPER_PEFRL)
+  if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.stepper != EB_STEPPER_PEFRL &&
+      cfg.stepper != EB_STEPPER_VELOCITY_VERLET)
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown time stepper");
-  if (cfg.stepper == EB_STEPPER_PEFRL && cfg.precision == EB_PRECISION_MIXED)
-    return fail(EB_ERR_UNSUPPORTED, "PEFRL runs in FP64 only");
+  if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.precision == EB_PRECISION_MIXED)
+    return fail(EB_ERR_UNSUPPORTED, "PEFRL and VelocityVerlet run in FP64 only");
   if (cfg.flags & ~static_cast<uint32_t>(EB_FLAG_RECORD_DIAGNOSTICS | EB_FLAG_REFERENCE_ROUNDING |
                                           EB_FLAG_STEP_STREAMING | EB_FLAG_STEP_RESIDENT | EB_FLAG_CUDA_GRAPH |
                                           EB_FLAG_STEP_BUCKETED))
@@ -743,6 +766,7 @@ EB_API eb_status eb_set_field(eb_sim* s, int64_t rod, int32_t field, const doubl
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, *fi);
   if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  if (fi->kind == kParam && (fi->offset == eb::kJ || fi->offset == eb::kJinv)) s->jinv_dirty = true;
   EB_CUDA(cudaMemcpy2DAsync(base + s->offsets[rod], s->stride * sizeof(double), values,
                             per * sizeof(double), per * sizeof(double), fi->ncomp,
                             cudaMemcpyHostToDevice, s->stream));
@@ -795,6 +819,7 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, fi);
   if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
+  if (to_device && fi.kind == kParam && (fi.offset == eb::kJ || fi.offset == eb::kJinv)) s->jinv_dirty = true;
   const size_t pitch = static_cast<size_t>(s->stride) * sizeof(double);
   if (layout == EB_LAYOUT_SLOTS) {
     if (count != fi.ncomp * s->n_slots)
@@ -860,11 +885,21 @@ EB_API eb_status eb_constrain_clamp(eb_sim* s, int64_t rod, int64_t index) {
   if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
   if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add constraints after finalize");
   if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
-  if (index != 0) return fail(EB_ERR_UNSUPPORTED, "only the clamp at index 0 is supported");
   RodHost& r = s->rods[rod];
+  if (index < 0 || index > r.n) return fail(EB_ERR_INVALID_ARGUMENT, "clamp index must name a node of the rod");
+  if (index == r.clamp_index[0] || index == r.clamp_index[1])
+    return fail(EB_ERR_INVALID_STATE, "this index of the rod is clamped already");
+  const int c = r.clamp_index[0] < 0 ? 0 : (r.clamp_index[1] < 0 ? 1 : -1);
+  if (c < 0) return fail(EB_ERR_UNSUPPORTED, "at most two clamps per rod");
+  // targets: the node's position and the element's directors now (the
+  // reference's generator captures them when it is built)
   const int64_t W = r.n + 1;
-  for (int d = 0; d < 3; ++d) r.info.clamp_x[d] = r.state[static_cast<size_t>((eb::kStX + d) * W)];
-  for (int k = 0; k < 9; ++k) r.info.clamp_Q[k] = r.state[static_cast<size_t>((eb::kStQ + k) * W)];
+  double* tx = c == 0 ? r.info.clamp_x : r.info.clamp2_x;
+  double* tq = c == 0 ? r.info.clamp_Q : r.info.clamp2_Q;
+  const int64_t e = index < r.n ? index : r.n - 1;  // a clamp at node n fixes no element
+  for (int d = 0; d < 3; ++d) tx[d] = r.state[static_cast<size_t>((eb::kStX + d) * W + index)];
+  for (int k = 0; k < 9; ++k) tq[k] = r.state[static_cast<size_t>((eb::kStQ + k) * W + e)];
+  r.clamp_index[c] = index;
   r.info.flags |= eb::kRodClamp;
   s->sim_flags |= eb::kSimClamp;
   return EB_OK;
@@ -880,15 +915,25 @@ EB_API eb_status eb_add_gravity(eb_sim* s, const double gravity[3]) {
   return EB_OK;
 }
 
-EB_API eb_status eb_add_end_torque(eb_sim* s, int64_t rod, const double torque_lab[3]) {
+EB_API eb_status eb_add_element_torque(eb_sim* s, int64_t rod, int64_t element, const double torque_lab[3]) {
   if (check_sim(s) || !torque_lab) return fail(EB_ERR_INVALID_ARGUMENT, "null argument");
   if (s->finalized) return fail(EB_ERR_INVALID_STATE, "cannot add forcing after finalize");
   if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
   RodHost& r = s->rods[rod];
+  if (element < 0 || element >= r.n) return fail(EB_ERR_INVALID_ARGUMENT, "element index out of range");
+  if (r.torque_index >= 0 && r.torque_index != element)
+    return fail(EB_ERR_UNSUPPORTED, "the torques of a rod act on one element");
   for (int d = 0; d < 3; ++d) r.info.end_torque[d] += torque_lab[d];
+  r.torque_index = element;
   r.info.flags |= eb::kRodEndTorque;
   s->sim_flags |= eb::kSimEndTorque;
   return EB_OK;
+}
+
+EB_API eb_status eb_add_end_torque(eb_sim* s, int64_t rod, const double torque_lab[3]) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  if (rod < 0 || rod >= static_cast<int64_t>(s->rods.size())) return fail(EB_ERR_NOT_FOUND, "unknown rod id");
+  return eb_add_element_torque(s, rod, s->rods[rod].n - 1, torque_lab);
 }
 
 EB_API eb_status eb_add_analytical_damper(eb_sim* s, int64_t rod, double translational_rate,
@@ -1080,9 +1125,17 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   std::vector<double> hd;
   if (want_diag) hd.assign(static_cast<size_t>(eb::kDiagFields * S), 0.0);
   std::vector<uint32_t> meta(static_cast<size_t>(S), 0u);
+  s->stored_jinv = false;
+  s->jinv_dirty = false;
   for (int64_t r = 0; r < nr; ++r) {
     const RodHost& R = s->rods[r];
     const int64_t W = R.n + 1, o = s->offsets[r];
+    for (int d = 0; d < 3 && !s->stored_jinv; ++d)
+      for (int64_t i = 0; i < R.n; ++i)
+        if (R.param[static_cast<size_t>((eb::kJinv + d) * W + i)] != 1.0 / R.param[static_cast<size_t>((eb::kJ + d) * W + i)]) {
+          s->stored_jinv = true;
+          break;
+        }
     for (int f = 0; f < eb::kStateFields; ++f)
       std::memcpy(&hs[static_cast<size_t>(f * S + o)], &R.state[static_cast<size_t>(f * W)], W * sizeof(double));
     for (int f = 0; f < eb::kParamFields; ++f)
@@ -1113,6 +1166,7 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   alloc(reinterpret_cast<void**>(&s->d_offsets), static_cast<size_t>(nr + 1) * sizeof(int64_t));
   alloc(reinterpret_cast<void**>(&s->d_energy), static_cast<size_t>(4 * nr) * sizeof(double));
   alloc(reinterpret_cast<void**>(&s->d_status), sizeof(uint32_t));
+  alloc(reinterpret_cast<void**>(&s->d_jinv_flag), sizeof(uint32_t));
   if (e != cudaSuccess) {
     host_free(s);
     return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA,
@@ -1159,15 +1213,58 @@ eb::StepArgs step_args(eb_sim* s, double dt) {
   a.drift_pre = 0.5 * dt;
   a.kick = dt;
   a.drift_post = 0.5 * dt;
+  a.damper_time = dt;
   for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
   a.sim_flags = s->sim_flags;
   a.status = s->d_status;
+  a.stored_jinv = s->stored_jinv ? 1u : 0u;
+  a.max_polls = s->max_polls;
   return a;
+}
+
+// the clock after n steps: PositionVerlet takes two TimeUpdate substeps of
+// dt/2 a step (PositionVerlet.hpp:52-58), VelocityVerlet one of dt
+// (VelocityVerlet.hpp:61-67)
+void advance_time(const eb_sim* s, double* time, double dt, int64_t n_steps) {
+  if (!time) return;
+  for (int64_t k = 0; k < n_steps; ++k) {
+    if (s->cfg.stepper == EB_STEPPER_VELOCITY_VERLET) {
+      *time += dt;
+    } else {
+      *time += 0.5 * dt;
+      *time += 0.5 * dt;
+    }
+  }
+}
+
+void drop_graphs(eb_sim* s) {
+  for (int p = 0; p < 2; ++p)
+    if (s->graph[p]) {
+      cudaGraphExecDestroy(s->graph[p]);
+      s->graph[p] = nullptr;
+    }
+}
+
+// After J or J^-1 changed on the device: does every stored J^-1 still equal
+// 1.0 / J?  Captured graphs hold the kernel variant, so they are dropped
+// when the answer changes.
+eb_status check_inverse_inertia(eb_sim* s) {
+  if (!s->jinv_dirty) return EB_OK;
+  uint32_t mismatch = 0;
+  EB_CUDA(eb::launch_check_inverse_inertia(s->stride, s->n_slots, s->d_param, s->d_meta, s->d_jinv_flag,
+                                           s->stream));
+  EB_CUDA(cudaMemcpyAsync(&mismatch, s->d_jinv_flag, sizeof(mismatch), cudaMemcpyDeviceToHost, s->stream));
+  EB_CUDA(cudaStreamSynchronize(s->stream));
+  const bool stored = mismatch != 0;
+  if (stored != s->stored_jinv) drop_graphs(s);
+  s->stored_jinv = stored;
+  s->jinv_dirty = false;
+  return EB_OK;
 }
 
 cudaError_t launch_streaming(eb_sim* s, eb::StepArgs& a, bool rec) {
   a.diag = rec ? s->d_diag : nullptr;
-  const int window = s->cfg.step_window ? s->cfg.step_window : 128;
+  const int window = s->cfg.step_window;  // 0: the persistent kernel
   if (s->cfg.flags & EB_FLAG_REFERENCE_ROUNDING)
     return eb::launch_rod_step_fp64_reference(a, rec, s->any_damped, window, s->stream);
   return eb::launch_rod_step_fp64(a, rec, s->any_damped, window, s->stream);
@@ -1268,21 +1365,25 @@ eb_status build_block_worklists(eb_sim* s) {
   return EB_OK;
 }
 
-// Substeps of one step as (drift before, kick, drift after) in units of dt:
-// PositionVerlet (PositionVerlet.hpp:49-88) fuses its two half drifts around
-// one kick; PEFRL (Omelyan, Mryglod and Folk 2002) is four kicks with the
-// drifts xi, chi, 1 - 2 (chi + xi), chi, xi between them.
+// Substeps of one step as (drift before, kick, drift after, damper time) in
+// units of dt: PositionVerlet (PositionVerlet.hpp:49-88) fuses its two half
+// drifts around one kick; VelocityVerlet (VelocityVerlet.hpp:49-87) kicks by
+// 1/2, drifts by 1, kicks by 1/2, with the damper's full-dt factors after
+// each kick; PEFRL (Omelyan, Mryglod and Folk 2002) is four kicks with the
+// drifts xi, chi, 1 - 2 (chi + xi), chi, xi between them and the damper's
+// factors for each kick's share of dt.
 struct Substep {
-  double pre, kick, post;
+  double pre, kick, post, damper;
 };
 using eb::kPefrlChi;
 using eb::kPefrlLambda;
 using eb::kPefrlXi;
-const Substep kVerlet[1] = {{0.5, 1.0, 0.5}};
-const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0},
-                           {kPefrlChi, kPefrlLambda, 0.0},
-                           {1.0 - 2.0 * (kPefrlChi + kPefrlXi), kPefrlLambda, 0.0},
-                           {kPefrlChi, 0.5 * (1.0 - 2.0 * kPefrlLambda), kPefrlXi}};
+const Substep kVerlet[1] = {{0.5, 1.0, 0.5, 1.0}};
+const Substep kVelocityVerlet[2] = {{0.0, 0.5, 1.0, 1.0}, {0.0, 0.5, 0.0, 1.0}};
+const Substep kPefrl[4] = {{kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda), 0.0, 0.5 * (1.0 - 2.0 * kPefrlLambda)},
+                           {kPefrlChi, kPefrlLambda, 0.0, kPefrlLambda},
+                           {1.0 - 2.0 * (kPefrlChi + kPefrlXi), kPefrlLambda, 0.0, kPefrlLambda},
+                           {kPefrlChi, 0.5 * (1.0 - 2.0 * kPefrlLambda), kPefrlXi, 0.5 * (1.0 - 2.0 * kPefrlLambda)}};
 
 int substeps(const eb_sim* s, const Substep** table);
 
@@ -1297,6 +1398,10 @@ int substeps(const eb_sim* s, const Substep** table) {
     *table = kPefrl;
     return 4;
   }
+  if (s->cfg.stepper == EB_STEPPER_VELOCITY_VERLET) {
+    *table = kVelocityVerlet;
+    return 2;
+  }
   *table = kVerlet;
   return 1;
 }
@@ -1310,10 +1415,12 @@ cudaError_t stream_one_step(eb_sim* s, eb::StepArgs& a, double dt, bool rec) {
       a.drift_pre = 0.5 * dt;  // PositionVerlet: bit-identical to half_dt
       a.kick = dt;
       a.drift_post = 0.5 * dt;
+      a.damper_time = dt;
     } else {
       a.drift_pre = sub[k].pre * dt;
       a.kick = sub[k].kick * dt;
       a.drift_post = sub[k].post * dt;
+      a.damper_time = sub[k].damper * dt;
     }
     a.in = s->d_state[s->cur];
     a.out = s->d_state[s->cur ^ 1];
@@ -1535,7 +1642,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   // contact needs a global exchange every step, PEFRL four force evaluations
   // a step: the streaming kernel
   const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
-                            s->contact.on || s->jd.on;
+                            s->contact.on || s->jd.on || s->cfg.stepper == EB_STEPPER_VELOCITY_VERLET;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -1905,16 +2012,13 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (n_steps == 0) return EB_OK;
   if (eb_status st = set_device(s)) return st;
   if (eb_status st = damper_for_dt(s, dt)) return st;
+  if (eb_status st = check_inverse_inertia(s)) return st;
   if (s->plan_mode == 0)
     if (eb_status st = plan_steps(s, dt, static_cast<int>(std::min<int64_t>(n_steps, kResidentChunk)))) return st;
   const bool diag = s->d_diag != nullptr;
   if (s->contact.on || s->jd.on) {
     if (eb_status st = step_with_contact(s, dt, n_steps, diag)) return st;
-    if (time)
-      for (int64_t k = 0; k < n_steps; ++k) {
-        *time += 0.5 * dt;
-        *time += 0.5 * dt;
-      }
+    advance_time(s, time, dt, n_steps);
     return EB_OK;
   }
   eb::StepArgs a = step_args(s, dt);
@@ -1953,13 +2057,7 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
     }
   }
   for (; done < n_steps; ++done) EB_CUDA(stream_one_step(s, a, dt, diag && done == n_steps - 1));
-  if (time) {
-    for (int64_t k = 0; k < n_steps; ++k) {
-      // two TimeUpdate substeps of dt/2 (PositionVerlet.hpp:52-58)
-      *time += 0.5 * dt;
-      *time += 0.5 * dt;
-    }
-  }
+  advance_time(s, time, dt, n_steps);
   return EB_OK;
 }
 
@@ -2053,11 +2151,7 @@ EB_API eb_status eb_step_host_state(eb_sim* s, double* time, double dt, int64_t 
     EB_CUDA(cudaStreamWaitEvent(s->stream, ev[1 + 2 * G + k], 0));
   }
   s->cur = c1;
-  if (time)
-    for (int64_t k = 0; k < n_steps; ++k) {
-      *time += 0.5 * dt;
-      *time += 0.5 * dt;
-    }
+  advance_time(s, time, dt, n_steps);
   if (!any_out) return EB_OK;
   EB_CUDA(cudaStreamSynchronize(s->stream));
   return check_device_status(s);
@@ -2257,7 +2351,15 @@ EB_API eb_status eb_snapshot_load(eb_sim* s, const void* buffer, uint64_t bytes)
   EB_CUDA(cudaMemcpyAsync(s->d_rods, p, s->rods.size() * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
   s->damper_dt = -1.0;  // the damper factors are refreshed for the next step's dt
+  s->jinv_dirty = true;  // restored parameters: check J^-1 against 1 / J again
   return check_device_status(s);
+}
+
+EB_API eb_status eb_debug_set_wait_bound(eb_sim* s, uint32_t polls) {
+  if (check_sim(s)) return EB_ERR_INVALID_ARGUMENT;
+  s->max_polls = polls;
+  drop_graphs(s);  // captured launches hold the bound
+  return EB_OK;
 }
 
 EB_API eb_status eb_get_stream(const eb_sim* s, void** stream) {

@@ -83,7 +83,43 @@ struct RodInfo {
   double damper_r;       // nu_r
   uint32_t flags;
   uint32_t pad;
+  // global slots the constraints and the forcing act on (-1: none): clamp
+  // 0 (targets clamp_x, clamp_Q) and clamp 1 (targets clamp2_x, clamp2_Q)
+  // fix the node at their slot and, where the slot holds one, its element;
+  // end_torque acts on the element at torque_slot
+  int64_t clamp_slot[2];
+  int64_t torque_slot;
+  double clamp2_x[3];
+  double clamp2_Q[9];
 };
+
+// per-slot bits derived from a slot's rod data (kernels keep them with the
+// slot): which clamp holds the slot, whether the rod's torque acts on it,
+// whether its rod has the damper
+enum SlotHits : uint32_t { kHitClamp0 = 1u, kHitClamp1 = 2u, kHitTorque = 4u, kHitDamper = 8u };
+
+// the clamp target of global slot g if one of the rod's clamps holds it
+// (returns true and sets x), as the value constraint leaves it
+__host__ __device__ __forceinline__ bool clamp_position(const RodInfo& ri, int64_t g, double x[3]) {
+  if (!(ri.flags & kRodClamp)) return false;
+  const double* t = g == ri.clamp_slot[0] ? ri.clamp_x : (g == ri.clamp_slot[1] ? ri.clamp2_x : nullptr);
+  if (!t) return false;
+  x[0] = t[0];
+  x[1] = t[1];
+  x[2] = t[2];
+  return true;
+}
+
+__host__ __device__ __forceinline__ uint32_t slot_hits(const RodInfo& ri, int64_t g) {
+  uint32_t h = 0;
+  if (ri.flags & kRodClamp) {
+    if (g == ri.clamp_slot[0]) h |= kHitClamp0;
+    if (g == ri.clamp_slot[1]) h |= kHitClamp1;
+  }
+  if ((ri.flags & kRodEndTorque) && g == ri.torque_slot) h |= kHitTorque;
+  if (ri.flags & kRodDamper) h |= kHitDamper;
+  return h;
+}
 
 struct StepArgs {
   int64_t stride;   // array stride (>= n_slots, multiple of 32)
@@ -102,6 +138,11 @@ struct StepArgs {
   double drift_pre;
   double kick;
   double drift_post;
+  // time the analytical damper's factors of this launch's rate constraint
+  // stand for: dt (PositionVerlet; VelocityVerlet, whose damper constants
+  // hold the full dt and act after each of its two kicks) or the kick's
+  // share of dt (PEFRL)
+  double damper_time;
   // force evaluations per step for the resident kernels: 0 or 1 is
   // PositionVerlet, 4 is PEFRL (coefficients below)
   int32_t n_sub;
@@ -115,6 +156,12 @@ struct StepArgs {
   // node slot, torques per element slot; or nullptr without connections
   const double* joint_force;
   const double* joint_torque;
+  // streaming kernel: read the stored J^-1 rows (1) or form 1 / J (0; bit
+  // identical while every stored J^-1 equals 1.0 / J, which the host checks)
+  uint32_t stored_jinv;
+  // bound on the polls of a bounded wait for bulk copies (0: the built-in
+  // bound); a small value exercises the timeout path
+  uint32_t max_polls;
 };
 
 // Rods longer than one CTA's capacity run on a pair of CTAs (a thread-block

@@ -124,6 +124,8 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
   extern __shared__ __align__(128) double smem[];
   const BRows<kCap> R{smem};
   uint32_t* meta_s = reinterpret_cast<uint32_t*>(smem + block_rows<kDamped>() * kCap);
+  // per slot: which clamp holds it, the torque, the damper (SlotHits)
+  uint8_t* hit_s = reinterpret_cast<uint8_t*>(meta_s + kCap);
 
   const int tid = threadIdx.x;
   int64_t g0;
@@ -186,10 +188,14 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
     return R.at(r, s);
   };
 
+  const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
+
   // ---- stage state, parameters and slot metadata (coalesced loads)
   for (int s = tid; s < count; s += kThreads) {
     const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
-    meta_s[s] = a.meta[g];
+    const uint32_t m = a.meta[g];
+    meta_s[s] = m;
+    hit_s[s] = static_cast<uint8_t>(any_rod ? slot_hits(a.rods[m >> kRodShift], g) : 0u);
 #pragma unroll 1
     for (int f = 0; f < kStateFields; ++f) R.at(f, s) = a.in[f * S + g];
 #pragma unroll 1
@@ -200,8 +206,6 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
     }
   }
   __syncthreads();
-
-  const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
 
   // drift of slot s by c (x += c v, Q <- exp(-c [w]x) Q), then, with
   // `clamp`, the clamp's value constraint on a clamped rod's first slot
@@ -216,12 +220,16 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
       const D3 w = R.get3(bW, s);
       so3_update_fast(q, c * w.x, c * w.y, c * w.z);
     }
-    if (clamp && any_rod && (meta & kFirst)) {
+    const uint32_t hit = hit_s[s];
+    if (clamp && (hit & (kHitClamp0 | kHitClamp1))) {
+      // the clamp's value constraint: the node, and its element if it has one
       const RodInfo& ri = a.rods[meta >> kRodShift];
-      if (ri.flags & kRodClamp) {
-        x = {ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]};
+      const double* tx = (hit & kHitClamp0) ? ri.clamp_x : ri.clamp2_x;
+      const double* tq = (hit & kHitClamp0) ? ri.clamp_Q : ri.clamp2_Q;
+      x = {tx[0], tx[1], tx[2]};
+      if (meta & kElem) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) q[k] = ri.clamp_Q[k];
+        for (int k = 0; k < 9; ++k) q[k] = tq[k];
       }
     }
     R.put3(bX, s, x);
@@ -329,6 +337,7 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
       const double im = 1.0 / m;
       v = {v.x + kdt * (F.x * im), v.y + kdt * (F.y * im), v.z + kdt * (F.z * im)};
       D3 w{0.0, 0.0, 0.0};
+      const uint32_t hit = hit_s[s];
       const RodInfo* ri = any_rod ? a.rods + (meta >> kRodShift) : nullptr;
       if (meta & kElem) {
         const double e = R.at(bE, s);
@@ -344,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
           const double ct = 0.5 * (m + nb(bMass, s + 1)) * R.at(bNuT, s);
           T = {T.x - ct * w.x, T.y - ct * w.y, T.z - ct * w.z};
         }
-        if (any_rod && (meta & kLastElem) && (ri->flags & kRodEndTorque)) {
+        if (hit & kHitTorque) {
           double q[9];
 #pragma unroll
           for (int k = 0; k < 9; ++k) q[k] = R.at(bQ + k, s);
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
         }
         const D3 ji = R.get3(bJinv, s);
         w = {w.x + kdt * (ji.x * T.x * e), w.y + kdt * (ji.y * T.y * e), w.z + kdt * (ji.z * T.z * e)};
-        if (any_rod && (ri->flags & kRodDamper)) {
+        if (hit & kHitDamper) {
           const double mn = nb(bMass, s + 1);
           double em = 0.5 * (m + mn);
           if (first) em += 0.5 * m;
@@ -361,14 +370,12 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
           w = {w.x * exp(y * ji.x), w.y * exp(y * ji.y), w.z * exp(y * ji.z)};
         }
       }
-      if (any_rod) {
-        if (first && (ri->flags & kRodClamp)) {
-          v = D3{0.0, 0.0, 0.0};
-          w = D3{0.0, 0.0, 0.0};
-        }
-        // exp(-nu_t dt) for a kick of dt; a fractional kick scales the exponent
-        if (ri->flags & kRodDamper) v = scale(v, kc == 1.0 ? ri->damper_t : exp(log(ri->damper_t) * kc));
+      if (hit & (kHitClamp0 | kHitClamp1)) {
+        v = D3{0.0, 0.0, 0.0};
+        w = D3{0.0, 0.0, 0.0};
       }
+      // exp(-nu_t dt) for a kick of dt; a fractional kick scales the exponent
+      if (hit & kHitDamper) v = scale(v, kc == 1.0 ? ri->damper_t : exp(log(ri->damper_t) * kc));
       R.put3(bV, s, v);
       if (meta & kElem) R.put3(bW, s, w);
       if (sub + 1 < nsub) {
@@ -424,7 +431,8 @@ template <int kCap, int kThreads, bool kSplit, bool kServe = false, bool kGather
 cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
   const size_t bytes =
-      size_t(damped ? block_rows<true>() : block_rows<false>()) * kCap * sizeof(double) + size_t(kCap) * sizeof(uint32_t);
+      size_t(damped ? block_rows<true>() : block_rows<false>()) * kCap * sizeof(double) +
+      size_t(kCap) * (sizeof(uint32_t) + sizeof(uint8_t));
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;

@@ -154,14 +154,19 @@ __device__ __forceinline__ void drift(const MRows<kCap>& R, int s, uint32_t meta
   }
 }
 
-// the clamp's value constraint on the first slot of a clamped rod
+// the clamp's value constraint on a slot a clamp holds (hits: SlotHits):
+// the node's position and, where the slot holds an element, its directors
 template <int kCap>
-__device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, const RodInfo& ri) {
-  R.pd3(dX, s, D3{ri.clamp_x[0], ri.clamp_x[1], ri.clamp_x[2]});
+__device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, uint32_t meta, uint32_t hits,
+                                            const RodInfo& ri) {
+  const double* tx = (hits & kHitClamp0) ? ri.clamp_x : ri.clamp2_x;
+  const double* tq = (hits & kHitClamp0) ? ri.clamp_Q : ri.clamp2_Q;
+  R.pd3(dX, s, D3{tx[0], tx[1], tx[2]});
+  if (!(meta & kElem)) return;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    R.ad(dQ + k, s) = ri.clamp_Q[k];
-    R.af(fQ + k, s) = static_cast<float>(ri.clamp_Q[k]);
+    R.ad(dQ + k, s) = tq[k];
+    R.af(fQ + k, s) = static_cast<float>(tq[k]);
   }
 }
 
@@ -307,11 +312,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     float dr = 0.f;
     if (any_rod) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
-      rf = ri.flags;
+      rf = slot_hits(ri, g);
       dtc = ri.damper_t;
       dr = static_cast<float>(ri.damper_r);
     }
-    rflag_s[s] = rf;
+    rflag_s[s] = rf;  // the slot's SlotHits
     R.af(fDampC, s) = static_cast<float>(1.0 - dtc);
     R.af(fDampR, s) = dr;
 #pragma unroll 1
@@ -342,7 +347,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   for (int s = tid; s < count; s += kThreads) {
     const uint32_t meta = meta_s[s];
     drift(R, s, meta, hdt, R.d3(dV, s), R.d3(dW, s));
-    if ((meta & kFirst) && (rflag_s[s] & kRodClamp)) clamp_value(R, s, a.rods[meta >> kRodShift]);
+    const uint32_t hits = rflag_s[s];
+    if (hits & (kHitClamp0 | kHitClamp1)) clamp_value(R, s, meta, hits, a.rods[meta >> kRodShift]);
   }
   sync_neighbours();
 
@@ -469,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           const F3 wf = R.f3(fW, s);
           T = {T.x - ct * wf.x, T.y - ct * wf.y, T.z - ct * wf.z};
         }
-        if ((meta & kLastElem) && (rf & kRodEndTorque)) {
+        if (rf & kHitTorque) {
           const RodInfo& ri = a.rods[meta >> kRodShift];
           float qf[9];
 #pragma unroll
@@ -480,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const F3 ji = R.f3(fJinv, s);
         w = {w.x + dt * static_cast<double>(ji.x * T.x * e), w.y + dt * static_cast<double>(ji.y * T.y * e),
              w.z + dt * static_cast<double>(ji.z * T.z * e)};
-        if (rf & kRodDamper) {
+        if (rf & kHitDamper) {
           const float mn = kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1);
           float em = 0.5f * (m + mn);
           if (first) em += 0.5f * m;
@@ -490,19 +496,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                w.z * static_cast<double>(exp_small(y * ji.z))};
         }
       }
-      const bool clamped = first && (rf & kRodClamp);
+      const bool clamped = (rf & (kHitClamp0 | kHitClamp1)) != 0;
       if (clamped) {
         v = D3{0.0, 0.0, 0.0};
         w = D3{0.0, 0.0, 0.0};
       }
-      if (rf & kRodDamper) v = scale(v, 1.0 - static_cast<double>(R.af(fDampC, s)));
+      if (rf & kHitDamper) v = scale(v, 1.0 - static_cast<double>(R.af(fDampC, s)));
       R.pd3(dV, s, v);
       if (meta & kElem) {
         R.pd3(dW, s, w);
         R.pf3(fW, s, tof(w));
       }
       drift(R, s, meta, last ? hdt : dt, v, w);
-      if (clamped) clamp_value(R, s, a.rods[meta >> kRodShift]);
+      if (clamped) clamp_value(R, s, meta, rf, a.rods[meta >> kRodShift]);
       if (last) {
         const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
 #pragma unroll

@@ -450,7 +450,13 @@ eb_status place(eb_server* s, Request& r) {
     for (int d = 0; d < 3; ++d) ri.clamp_x[d] = h.state[(eb::kStX + d) * W];
     for (int q = 0; q < 9; ++q) ri.clamp_Q[q] = h.state[(eb::kStQ + q) * W];
     ri.damper_t = 1.0;
-    if (r.options & EB_REQUEST_CLAMP) ri.flags |= eb::kRodClamp;
+    ri.clamp_slot[1] = -1;
+    ri.torque_slot = -1;
+    ri.clamp_slot[0] = -1;
+    if (r.options & EB_REQUEST_CLAMP) {
+      ri.flags |= eb::kRodClamp;
+      ri.clamp_slot[0] = r.bins[b] * kBin + o;  // node 0 / element 0 of the rod
+    }
     if (r.options & EB_REQUEST_DAMPER) {
       ri.flags |= eb::kRodDamper;
       ri.damper_t = std::exp(-r.nu_t * r.dt);

@@ -91,9 +91,10 @@ class StraightRod:
 # -- constraints, forcing, environments, stepper -----------------------------
 @dataclass
 class Clamp:
-    """Value constraint x_0 = origin, Q_0 = Q_0(init) plus rate constraint
-    v_0 = w_0 = 0 (pattern of examples/dynamic_cantilever/
-    DynamicCantileverCaseStudy.cpp:73-89)."""
+    """Value constraint x_k = x_k(now), Q_k = Q_k(now) plus rate constraint
+    v_k = w_k = 0 at the node / element index given with .at(k) (0 if none;
+    pattern of examples/dynamic_cantilever/DynamicCantileverCaseStudy.cpp:
+    73-89).  At most two clamps per rod, e.g. .at(0) and .at(n)."""
 
 
 @dataclass
@@ -107,7 +108,8 @@ class AnalyticalLinearDamper:
 
 @dataclass
 class EndTorque:
-    """Constant lab-frame torque at the last element (Forcing/MakeForcing.hpp)."""
+    """Constant lab-frame torque on one element, the last one unless placed
+    with .at(element) (Forcing/MakeForcing.hpp)."""
 
     torque: Sequence[float]
 
@@ -205,6 +207,16 @@ class PEFRL:
     simulator steps with the stepper it was created with."""
 
 
+@dataclass
+class VelocityVerlet:
+    """Time/SymplecticSteppers/Algorithms/VelocityVerlet.hpp:49-87: kick
+    dt/2, drift dt, kick dt/2 (two force evaluations a step)."""
+
+
+_STEPPERS = {PositionVerlet: L.EB_STEPPER_POSITION_VERLET, PEFRL: L.EB_STEPPER_PEFRL,
+             VelocityVerlet: L.EB_STEPPER_VELOCITY_VERLET}
+
+
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -282,8 +294,9 @@ class Simulator:
         cfg.resident_config = int(resident_config)
         if cuda_graph:
             cfg.flags |= L.EB_FLAG_CUDA_GRAPH
-        self.stepper = PEFRL if isinstance(stepper, PEFRL) or stepper is PEFRL else PositionVerlet
-        cfg.stepper = L.EB_STEPPER_PEFRL if self.stepper is PEFRL else L.EB_STEPPER_POSITION_VERLET
+        kind = stepper if isinstance(stepper, type) else type(stepper)
+        self.stepper = kind if stepper is not None and kind in _STEPPERS else PositionVerlet
+        cfg.stepper = _STEPPERS[self.stepper]
         h = ctypes.c_void_p()
         L.call("eb_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h
@@ -376,10 +389,9 @@ class Simulator:
             L.call("eb_add_analytical_damper", self._h, rod.id, float(item.translational_rate),
                    float(item.rotational_rate))
         elif kind == "force" and isinstance(item, EndTorque):
-            if index not in (None, rod.n_elements - 1):
-                raise ValueError("the end torque acts on the last element")
             t = np.asarray(item.torque, dtype=np.float64)
-            L.call("eb_add_end_torque", self._h, rod.id, _dptr(t))
+            element = rod.n_elements - 1 if index is None else index
+            L.call("eb_add_element_torque", self._h, rod.id, int(element), _dptr(t))
         else:
             raise TypeError(f"unsupported {kind} item {item!r}")
 

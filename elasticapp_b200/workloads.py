@@ -56,6 +56,8 @@ class Workload:
     contact_rod_material: list | None = None  # per rod material id (-1: none)
     planes: list | None = None                # (point, normal, material id)
     connections: list | None = None           # (rod_a, index_a, rod_b, index_b, FreeJoint or HingeJoint)
+    clamp_at: list | None = None              # per rod, the clamped node indices (in place of node 0)
+    torque_element: list | None = None        # per rod, the element the end torque acts on
 
     @property
     def n_elements(self) -> np.ndarray:
@@ -81,11 +83,13 @@ class Workload:
             if self.rest_curvature is not None:
                 ref.set("ReferenceCurvature", self.rest_curvature[k])
             if self.clamp if isinstance(self.clamp, bool) else self.clamp[k]:
-                sim.constrain(ref).at(0).using(Clamp())
+                for idx in (self.clamp_at[k] if self.clamp_at is not None else (0,)):
+                    sim.constrain(ref).at(int(idx)).using(Clamp())
             if self.damper is not None:
                 sim.constrain(ref).using(AnalyticalLinearDamper(*self.damper))
             if self.end_torque is not None:
-                sim.force(ref).at(ref.n_elements - 1).using(EndTorque(self.end_torque[k]))
+                el = ref.n_elements - 1 if self.torque_element is None else int(self.torque_element[k])
+                sim.force(ref).at(el).using(EndTorque(self.end_torque[k]))
         if self.contact_materials:
             sim.add_environment(CollisionSystem())
             ids = [sim.create_material(m) for m in self.contact_materials]

@@ -95,7 +95,8 @@ typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
   int32_t precision;       /* eb_precision */
   uint32_t flags;          /* EB_FLAG_* */
-  int32_t step_window;     /* slots per CTA of the streaming kernel: 0 (default, 128), 128 or 256 */
+  int32_t step_window;     /* streaming kernel: 0 (default) persistent CTAs over 128-slot windows with
+                              double-buffered inputs; 128 or 256: one CTA per window of that many slots */
   int32_t resident_config; /* 0: chosen by timing; c > 0: resident configuration c - 1 */
   int32_t stepper;         /* eb_stepper (0: PositionVerlet) */
 } eb_config;
@@ -111,7 +112,16 @@ typedef struct eb_config {
  * dt).  PEFRL runs in FP64, on the streaming kernel (four launches a step)
  * or on the resident kernels (four force evaluations a step on chip), as the
  * step plan chooses. */
-typedef enum eb_stepper { EB_STEPPER_POSITION_VERLET = 0, EB_STEPPER_PEFRL = 1 } eb_stepper;
+typedef enum eb_stepper {
+  EB_STEPPER_POSITION_VERLET = 0,
+  EB_STEPPER_PEFRL = 1,
+  /* VelocityVerlet.hpp:49-87: kick dt/2, drift dt, kick dt/2 (two force
+   * evaluations a step), value constraints before and rate constraints
+   * after each kick; the analytical damper multiplies by its full-dt factors
+   * after each kick, as the reference's rate constraint does.  FP64, on the
+   * streaming kernel (two launches a step). */
+  EB_STEPPER_VELOCITY_VERLET = 2
+} eb_stepper;
 
 /* Rod models (elastica/Systems/CosseratRods/Aliases/CosseratRod.hpp:33-40 and
  * Aliases/CosseratRodWithoutDamping.hpp). */
@@ -228,22 +238,32 @@ EB_API eb_status eb_set_field_batch(struct eb_sim* sim, int32_t field, int32_t l
 EB_API eb_status eb_get_field_batch(struct eb_sim* sim, int32_t field, int32_t layout,
                                     double* values, int64_t count);
 
-/* --- constraints: simulator->constrain(rod).at(0).with(clamp), the value
- * constraint fixing x_0, Q_0 and the rate constraint zeroing v_0, w_0
- * (elastica/Simulator/Constraints/MakeConstraint.hpp:458-494; pattern of
- * examples/dynamic_cantilever/DynamicCantileverCaseStudy.cpp:73-89).  The
- * clamp target is the rod's node-0 position and element-0 director at the
- * time of eb_finalize.  Only index 0 is supported. */
+/* --- constraints: simulator->constrain(rod).at(index).with(clamp), the
+ * value constraint fixing node index's position x_k and, for index < n,
+ * element index's directors Q_k, and the rate constraint zeroing v_k and
+ * w_k (elastica/Simulator/Constraints/MakeConstraint.hpp:130-151, 458-494;
+ * the generator of examples/dynamic_cantilever/
+ * DynamicCantileverCaseStudy.cpp:73-89 applied at .at(index)).  index is a
+ * node index, 0..n.  The targets are the node's position and the element's
+ * directors at the time of this call (the reference's generator captures
+ * them when it is built).  A rod takes at most two clamps (a beam clamped
+ * at both ends: indices 0 and n); a third is EB_ERR_UNSUPPORTED, the same
+ * index twice EB_ERR_INVALID_STATE. */
 EB_API eb_status eb_constrain_clamp(struct eb_sim* sim, int64_t rod, int64_t index);
 
 /* --- environments: GravityField, F_ext += g m
  * (elastica/Simulator/Environments/GravityField/GravityField.hpp:239-246). */
 EB_API eb_status eb_add_gravity(struct eb_sim* sim, const double gravity[3]);
 
-/* --- forcing: simulator->force(rod).at(n-1).with(make_forcing(...)) with a
- * constant lab-frame torque applied at the last element in the material
- * frame as Q T (elastica/Simulator/Forcing/MakeForcing.hpp:74-165;
- * examples/axial_stretching/AxialStretchingCaseStudy.cpp:125-134). */
+/* --- forcing: simulator->force(rod).at(element).with(make_forcing(...))
+ * with a constant lab-frame torque applied at one element in the material
+ * frame as Q T (elastica/Simulator/Forcing/MakeForcing.hpp:74-165,
+ * Forcing.hpp:737-749; examples/axial_stretching/
+ * AxialStretchingCaseStudy.cpp:125-134).  Torques added to one rod sum;
+ * they act on one element per rod (another element is EB_ERR_UNSUPPORTED).
+ * eb_add_end_torque is the same at the last element (n - 1). */
+EB_API eb_status eb_add_element_torque(struct eb_sim* sim, int64_t rod, int64_t element,
+                                       const double torque_lab[3]);
 EB_API eb_status eb_add_end_torque(struct eb_sim* sim, int64_t rod, const double torque_lab[3]);
 
 /* --- rate constraint: the analytical linear damper
@@ -404,6 +424,16 @@ EB_API eb_status eb_snapshot_load(struct eb_sim* sim, const void* buffer, uint64
 EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* config, float* probe_ms,
                               int32_t count);
 
+/* Debug only: the number of polls after which the streaming step kernel's
+ * waits for its bulk copies give up (0 restores the built-in bound, millions
+ * of polls).  A kernel that gives up records it in the simulator's status,
+ * waits for the copies it issued and returns; the next call that reads the
+ * status (eb_get_field, eb_synchronize, ...) returns EB_ERR_CUDA and the
+ * simulator's state is no longer valid.  A bound of 1 makes the first wait
+ * run out: it exists to exercise that path without a fault.  No counterpart
+ * in the reference. */
+EB_API eb_status eb_debug_set_wait_bound(struct eb_sim* sim, uint32_t polls);
+
 /* Number of kernel launches this simulator has issued (diagnostic). */
 EB_API eb_status eb_launch_count(const struct eb_sim* sim, int64_t* count);
 
@@ -512,7 +542,10 @@ EB_API eb_status eb_server_request_status(const struct eb_server* server, int64_
  *
  * boxes: device pointer, n_boxes boxes of 6 doubles (lo x, lo y, lo z,
  * hi x, hi y, hi z), closed intervals, finite, hi >= lo.  n_boxes <= 131072
- * (larger counts are rejected with EB_ERR_INVALID_ARGUMENT).  pairs: device
+ * (larger counts are rejected with EB_ERR_INVALID_ARGUMENT).  The grid's cell
+ * edge is the largest box extent: with very uneven extents (one box spanning
+ * the others) most boxes share a cell and the search costs up to O(n^2)
+ * overlap tests.  pairs: device
  * pointer to capacity pairs of int64 (i, j), i < j; the overlapping pairs are
  * written sorted by i then j.  *count (host) receives their number; when it
  * exceeds capacity nothing is written and EB_ERR_INVALID_ARGUMENT is

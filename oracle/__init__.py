@@ -39,6 +39,8 @@ class _OrcRods(ctypes.Structure):
         ("d_sigma", _P), ("d_kappa", _P), ("d_stress", _P), ("d_couple", _P),
         ("d_loads", _P), ("d_torques", _P), ("d_accel", _P), ("d_alpha", _P),
         ("d_dimension", _P),
+        ("clamp_index", ctypes.POINTER(ctypes.c_int64)), ("clamp2_x", _P), ("clamp2_Q", _P),
+        ("torque_index", ctypes.POINTER(ctypes.c_int64)),
     ]
 
 
@@ -81,6 +83,8 @@ def lib():
         _lib.orc_step.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64, ctypes.c_int]
         _lib.orc_force_eval.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_int]
         _lib.orc_step_pefrl.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64, ctypes.c_int]
+        _lib.orc_step_velocity_verlet.argtypes = [ctypes.POINTER(_OrcRods), ctypes.c_double, ctypes.c_int64,
+                                                  ctypes.c_int]
         _lib.orc_energy.argtypes = [ctypes.POINTER(_OrcRods), _P, ctypes.c_int]
         _lib.orc_straight_rod.argtypes = [ctypes.c_int64, _P, _P, _P, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double] + [_P] * 11
@@ -157,6 +161,14 @@ class RodArrays:
         self.clamp = np.zeros(self.n_rods, dtype=np.uint8)
         self.clamp_x = np.zeros(3 * self.n_rods)
         self.clamp_Q = np.zeros(9 * self.n_rods)
+        # clamp c of rod r at index clamp_index[2r + c] (-1: none; clamp 0 at
+        # index 0 by default), targets clamp_x / clamp_Q (c = 0) or
+        # clamp2_x / clamp2_Q (c = 1); end_torque at element torque_index[r]
+        # (-1: the last element)
+        self.clamp_index = np.tile(np.array([0, -1], dtype=np.int64), self.n_rods)
+        self.clamp2_x = np.zeros(3 * self.n_rods)
+        self.clamp2_Q = np.zeros(9 * self.n_rods)
+        self.torque_index = np.full(self.n_rods, -1, dtype=np.int64)
         self.end_torque = np.zeros(3 * self.n_rods)
         self.damper_nu = np.zeros(2 * self.n_rods)
         self.gravity = np.zeros(3)
@@ -201,6 +213,10 @@ class RodArrays:
         s.clamp_Q = self.clamp_Q.ctypes.data_as(_P)
         s.end_torque = self.end_torque.ctypes.data_as(_P)
         s.damper_nu = self.damper_nu.ctypes.data_as(_P)
+        s.clamp_index = self.clamp_index.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        s.clamp2_x = self.clamp2_x.ctypes.data_as(_P)
+        s.clamp2_Q = self.clamp2_Q.ctypes.data_as(_P)
+        s.torque_index = self.torque_index.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
         for i in range(3):
             s.gravity[i] = float(self.gravity[i])
         if self.diag is not None:
@@ -210,7 +226,8 @@ class RodArrays:
 
     def step(self, dt, n_steps=1, n_threads=0, stepper="position_verlet"):
         s = self._struct()
-        fn = lib().orc_step_pefrl if stepper == "pefrl" else lib().orc_step
+        fn = {"pefrl": lib().orc_step_pefrl, "velocity_verlet": lib().orc_step_velocity_verlet,
+              "position_verlet": lib().orc_step}[stepper]
         rc = fn(ctypes.byref(s), float(dt), int(n_steps), int(n_threads))
         if rc != 0:
             raise RuntimeError("orc_step failed")
@@ -231,7 +248,8 @@ class RodArrays:
         c = RodArrays.__new__(RodArrays)
         c.__dict__.update(self.__dict__)
         c.arrays = {k: a.copy() for k, a in self.arrays.items()}
-        for k in ("clamp", "clamp_x", "clamp_Q", "end_torque", "damper_nu", "gravity"):
+        for k in ("clamp", "clamp_x", "clamp_Q", "end_torque", "damper_nu", "gravity", "clamp_index", "clamp2_x",
+                  "clamp2_Q", "torque_index"):
             setattr(c, k, getattr(self, k).copy())
         c.diag = None if self.diag is None else {k: a.copy() for k, a in self.diag.items()}
         return c

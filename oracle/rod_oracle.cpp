@@ -185,14 +185,28 @@ void kinematic(const OrcRods& R, int64_t r, double c) {
   }
 }
 
-// Value constraint of the clamp (examples/dynamic_cantilever/
-// DynamicCantileverCaseStudy.cpp:73-89, applied post-kinematic,
-// Simulator/Interface/TimeSteppers/SymplecticSteppers.hpp:174).
+// index (within the rod) of clamp c of rod r, or -1
+int64_t clamp_at(const OrcRods& R, int64_t r, int c) {
+  if (!R.clamp || !R.clamp[r]) return -1;
+  if (!R.clamp_index) return c == 0 ? 0 : -1;
+  return R.clamp_index[2 * r + c];
+}
+
+// Value constraint of the clamps (examples/dynamic_cantilever/
+// DynamicCantileverCaseStudy.cpp:73-89 at .at(k), applied post-kinematic,
+// Simulator/Interface/TimeSteppers/SymplecticSteppers.hpp:174): node k's
+// position and, for k < n, element k's directors.
 void clamp_values(const OrcRods& R, int64_t r) {
-  if (!R.clamp || !R.clamp[r]) return;
-  const int64_t S = R.n_slots, s = R.offset[r];
-  for (int d = 0; d < 3; ++d) R.x[d * S + s] = R.clamp_x[3 * r + d];
-  for (int c = 0; c < 9; ++c) R.Q[c * S + s] = R.clamp_Q[9 * r + c];
+  const int64_t S = R.n_slots, o = R.offset[r], n = R.offset[r + 1] - o - 1;
+  for (int c = 0; c < 2; ++c) {
+    const int64_t k = clamp_at(R, r, c);
+    if (k < 0) continue;
+    const double* tx = c == 0 ? R.clamp_x : R.clamp2_x;
+    const double* tq = c == 0 ? R.clamp_Q : R.clamp2_Q;
+    for (int d = 0; d < 3; ++d) R.x[d * S + o + k] = tx[3 * r + d];
+    if (k < n)
+      for (int q = 0; q < 9; ++q) R.Q[q * S + o + k] = tq[9 * r + q];
+  }
 }
 
 // Internal forces and torques of one rod (ElasticityInterface.hpp:360-365),
@@ -341,9 +355,10 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
   // Simulator/Forcing/MakeForcing.hpp), then update_acceleration
   // (Components/Kinematics/WithRodKinematics.hpp:684-714).
   V3 tend = {0.0, 0.0, 0.0};
+  const int64_t tk = (R.torque_index && R.torque_index[r] >= 0) ? R.torque_index[r] : n - 1;
   if (R.end_torque) {
     double q[9];
-    load_q(R.Q, S, o + n - 1, q);
+    load_q(R.Q, S, o + tk, q);
     tend = matvec(q, {R.end_torque[3 * r], R.end_torque[3 * r + 1], R.end_torque[3 * r + 2]});
   }
   for (int64_t j = 0; j <= n; ++j) {
@@ -380,7 +395,7 @@ void compute_dynamics(const OrcRods& R, int64_t r, Scratch& sc, double* acc, dou
       const V3 tc = matvec(q, {nt[s], nt[S + s], nt[2 * S + s]});
       te = {te.x + tc.x, te.y + tc.y, te.z + tc.z};
     }
-    if (i == n - 1) te = {te.x + tend.x, te.y + tend.y, te.z + tend.z};
+    if (i == tk) te = {te.x + tend.x, te.y + tend.y, te.z + tend.z};
     const V3 T = getv(sc.tq, i);
     const double e = sc.dil[i];
     alpha[3 * i] = (R.inv_inertia[s] * (T.x + te.x)) * e;
@@ -423,25 +438,31 @@ void write_diagnostics(const OrcRods& R, int64_t r, const Scratch& sc, const dou
 }
 
 // PositionVerlet.hpp:71-77 dynamic substep v += dt a, w += dt alpha, followed
-// by the post-dynamic rate constraints: clamp (v0 = w0 = 0) and the
-// analytical damper (examples/fish_swimming/FishModel/Dissipations/
-// AnalyticalLinearDamper.hpp:15-76, "physical version").
+// by the post-dynamic rate constraints: the clamps (v_k = w_k = 0 at each
+// clamp index k) and the analytical damper (examples/fish_swimming/
+// FishModel/Dissipations/AnalyticalLinearDamper.hpp:15-76, "physical
+// version").  damper_dt: the time step the damper's constants were formed
+// with (its rate constraint multiplies by exp(-nu damper_dt) after every
+// dynamic substep); negative: dt
 void dynamic_update(const OrcRods& R, int64_t r, double dt, const Scratch& sc, const double* acc,
-                    const double* alpha) {
+                    const double* alpha, double damper_dt = -1.0) {
+  const double ddt = damper_dt < 0.0 ? dt : damper_dt;
   const int64_t S = R.n_slots, o = R.offset[r], n = R.offset[r + 1] - o - 1;
   for (int64_t j = 0; j <= n; ++j)
     for (int d = 0; d < 3; ++d) R.v[d * S + o + j] = R.v[d * S + o + j] + dt * acc[3 * j + d];
   for (int64_t i = 0; i < n; ++i)
     for (int d = 0; d < 3; ++d) R.w[d * S + o + i] = R.w[d * S + o + i] + dt * alpha[3 * i + d];
-  if (R.clamp && R.clamp[r]) {
+  for (int c = 0; c < 2; ++c) {
+    const int64_t k = clamp_at(R, r, c);
+    if (k < 0) continue;
     for (int d = 0; d < 3; ++d) {
-      R.v[d * S + o] = 0.0;
-      R.w[d * S + o] = 0.0;
+      R.v[d * S + o + k] = 0.0;
+      if (k < n) R.w[d * S + o + k] = 0.0;
     }
   }
   if (R.damper_nu && (R.damper_nu[2 * r] != 0.0 || R.damper_nu[2 * r + 1] != 0.0)) {
     const double nut = R.damper_nu[2 * r], nur = R.damper_nu[2 * r + 1];
-    const double tcoef = std::exp(-nut * dt);
+    const double tcoef = std::exp(-nut * ddt);
     for (int64_t j = 0; j <= n; ++j)
       for (int d = 0; d < 3; ++d) R.v[d * S + o + j] *= tcoef;
     for (int64_t i = 0; i < n; ++i) {
@@ -450,7 +471,7 @@ void dynamic_update(const OrcRods& R, int64_t r, double dt, const Scratch& sc, c
       if (i == 0) em += 0.5 * R.mass[s];
       if (i == n - 1) em += 0.5 * R.mass[s + 1];
       for (int d = 0; d < 3; ++d) {
-        const double rc = std::exp(-nur * em * R.inv_inertia[d * S + s] * dt);
+        const double rc = std::exp(-nur * em * R.inv_inertia[d * S + s] * ddt);
         R.w[d * S + s] *= std::pow(rc, sc.dil[i]);
       }
     }
@@ -1042,10 +1063,13 @@ std::vector<double> drifted_positions(const OrcRods& R, double c) {
   const int64_t S = R.n_slots;
   std::vector<double> x(R.x, R.x + 3 * S);
   for (int64_t i = 0; i < 3 * S; ++i) x[i] = x[i] + c * R.v[i];
-  if (R.clamp)
-    for (int64_t r = 0; r < R.n_rods; ++r)
-      if (R.clamp[r])
-        for (int d = 0; d < 3; ++d) x[d * S + R.offset[r]] = R.clamp_x[3 * r + d];
+  for (int64_t r = 0; r < R.n_rods; ++r)
+    for (int c = 0; c < 2; ++c) {
+      const int64_t k = clamp_at(R, r, c);
+      if (k < 0) continue;
+      const double* tx = c == 0 ? R.clamp_x : R.clamp2_x;
+      for (int d = 0; d < 3; ++d) x[d * S + R.offset[r] + k] = tx[3 * r + d];
+    }
   return x;
 }
 
@@ -1311,6 +1335,47 @@ extern "C" int orc_step_pefrl(const OrcRods* rods, double dt, int64_t n_steps, i
             clamp_values(R, r);
           }
         }
+    }
+  }
+  (void)n_threads;
+  return 0;
+}
+
+// VelocityVerlet (elastica/Time/SymplecticSteppers/Algorithms/
+// VelocityVerlet.hpp:49-87): substeps [Dynamic(dt/2), Kinematic(dt),
+// TimeUpdate(dt), Dynamic(dt/2)] walked as in Simulator::step
+// (SymplecticSteppers.hpp:152-216): every dynamic substep first applies the
+// value constraints, evaluates the loads at the current state, kicks by
+// dt/2 and applies the rate constraints.  The analytical damper's constants
+// are formed with the full dt at construction, so each of the two rate
+// constraint passes multiplies by exp(-nu dt).
+extern "C" int orc_step_velocity_verlet(const OrcRods* rods, double dt, int64_t n_steps, int n_threads) {
+  if (check(rods) != 0) return -1;
+  const OrcRods& R = *rods;
+#ifdef _OPENMP
+  const int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+#endif
+  {
+    Scratch sc;
+    std::vector<double> acc, alpha;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 16)
+#endif
+    for (int64_t r = 0; r < R.n_rods; ++r) {
+      const int64_t n = R.offset[r + 1] - R.offset[r] - 1;
+      acc.assign(3 * (n + 1), 0.0);
+      alpha.assign(3 * (n + 1), 0.0);
+      for (int64_t step = 0; step < n_steps; ++step) {
+        clamp_values(R, r);
+        compute_dynamics(R, r, sc, acc.data(), alpha.data());
+        dynamic_update(R, r, 0.5 * dt, sc, acc.data(), alpha.data(), dt);
+        kinematic(R, r, dt);
+        clamp_values(R, r);
+        compute_dynamics(R, r, sc, acc.data(), alpha.data());
+        if (step == n_steps - 1) write_diagnostics(R, r, sc, acc.data(), alpha.data());
+        dynamic_update(R, r, 0.5 * dt, sc, acc.data(), alpha.data(), dt);
+      }
     }
   }
   (void)n_threads;

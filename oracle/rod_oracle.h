@@ -74,6 +74,18 @@ typedef struct OrcRods {
   double* d_accel;        /* 3*S nodes */
   double* d_alpha;        /* 3*S elements */
   double* d_dimension;    /* S elements (radius) */
+
+  /* where the constraints and the forcing act (may be NULL: the clamp at
+   * node 0 / element 0 and the torque at element n - 1).  A clamp at index k
+   * fixes node k's position and, for k < n, element k's directors
+   * (value constraint), and zeroes their velocity and angular velocity
+   * (rate constraint), the pattern of DynamicCantileverCaseStudy.cpp:73-89
+   * applied at .at(k) (Simulator/Constraints/MakeConstraint.hpp:130-151). */
+  const int64_t* clamp_index;  /* 2*n_rods: index of clamp 0 (targets clamp_x, clamp_Q) and of
+                                  clamp 1 (targets clamp2_x, clamp2_Q); -1: none */
+  const double* clamp2_x;      /* 3*n_rods */
+  const double* clamp2_Q;      /* 9*n_rods */
+  const int64_t* torque_index; /* n_rods: element end_torque acts on; -1: element n - 1 */
 } OrcRods;
 
 /* Advance every rod by n_steps PositionVerlet steps of size dt.
@@ -83,6 +95,8 @@ int orc_step(const OrcRods* rods, double dt, int64_t n_steps, int n_threads);
 /* n_steps PEFRL steps (declared, not implemented, in the reference;
  * Omelyan, Mryglod and Folk 2002): four force evaluations per step. */
 int orc_step_pefrl(const OrcRods* rods, double dt, int64_t n_steps, int n_threads);
+/* VelocityVerlet steps (elastica/Time/SymplecticSteppers/Algorithms/VelocityVerlet.hpp:49-87) */
+int orc_step_velocity_verlet(const OrcRods* rods, double dt, int64_t n_steps, int n_threads);
 
 /* One force evaluation without any time update (the reference's
  * compute_internal_forces + compute_internal_torques + update_acceleration),

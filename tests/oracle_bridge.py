@@ -33,8 +33,15 @@ def oracle_from_workload(wl, damped: bool = False, diagnostics: bool = False):
             rods.set_rod("rest_kappa", r, wl.rest_curvature[r])
         if wl.clamp if isinstance(wl.clamp, bool) else wl.clamp[r]:
             rods.clamp[r] = 1
-            rods.clamp_x[3 * r:3 * r + 3] = init["x"][:, 0]
-            rods.clamp_Q[9 * r:9 * r + 9] = init["Q"][:, :, 0].ravel()
+            at = list(wl.clamp_at[r]) if getattr(wl, "clamp_at", None) is not None else [0]
+            rods.clamp_index[2 * r:2 * r + 2] = (at + [-1, -1])[:2]
+            # the targets: the initial state at those indices, as the clamp captures it
+            for c, k in enumerate(at[:2]):
+                tx, tq = (rods.clamp_x, rods.clamp_Q) if c == 0 else (rods.clamp2_x, rods.clamp2_Q)
+                tx[3 * r:3 * r + 3] = init["x"][:, k]
+                tq[9 * r:9 * r + 9] = init["Q"][:, :, min(k, n - 1)].ravel()
+        if getattr(wl, "torque_element", None) is not None:
+            rods.torque_index[r] = int(wl.torque_element[r])
         if wl.damper is not None:
             rods.damper_nu[2 * r:2 * r + 2] = wl.damper
         if wl.end_torque is not None:

@@ -65,3 +65,19 @@ def test_oracle_energies_equal_closed_forms(eb, oracle_mod):
     bt = oracle_from_workload(wl)
     bt.set_rod("Q", 0, A.bent_directors().reshape(9, A.N))
     assert abs(bt.energy()[0][3] - A.bend_energy()) <= 1e-9 * A.bend_energy()
+
+
+def test_oracle_velocity_verlet_damps_after_both_kicks(eb, oracle_mod):
+    """VelocityVerlet applies the rate constraints after each of its two
+    dynamic substeps, and the damper's constants hold the full dt
+    (AnalyticalLinearDamper.hpp:15-79): exp(-nu dt) twice a step."""
+    orc = oracle_from_workload(_workload(eb, damper=(A.NU_T, A.NU_R)))
+    orc.set_rod("v", 0, A.translating_velocity())
+    orc.set_rod("w", 0, A.spinning_omega())
+    k = 50
+    orc.step(A.DT, k, stepper="velocity_verlet")
+    tol = 16.0 * k * np.finfo(float).eps
+    v, w = orc.get_rod("v", 0, A.N + 1), orc.get_rod("w", 0, A.N)
+    assert A.rel(v, np.repeat(A.damped_velocity(2 * k)[:, None], A.N + 1, axis=1)) <= tol
+    assert A.rel(w[2], np.full(A.N, A.damped_spin(2 * k))) <= tol
+    assert np.max(np.abs(w[:2])) == 0.0 and np.max(np.abs(v[0])) == 0.0

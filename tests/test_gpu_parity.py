@@ -149,7 +149,8 @@ def small_uneven(n_rods=48, seed=7, n_range=(2, 40)):
     return wl
 
 
-@pytest.mark.parametrize("window,step_mode", [(0, "streaming"), (256, "streaming"), (0, "resident")])
+@pytest.mark.parametrize("window,step_mode", [(0, "streaming"), (128, "streaming"), (256, "streaming"),
+                                              (0, "resident")])
 def test_uneven_batch_1000_steps_vs_oracle(window, step_mode):
     """Clamped rods of uneven length with gravity and the analytical damper:
     the FP64 drop-in matches the oracle after 1000 steps."""

@@ -1,8 +1,8 @@
-"""PEFRL in the oracle.  The reference declares the stepper without an
-implementation, so there is no golden vector: the checks are its order of
-accuracy (error ratio about 16 per halving of dt for a fourth-order method,
-4 for PositionVerlet) on free, undamped rods, where no first-order
-constraint splitting masks it."""
+"""PEFRL and VelocityVerlet in the oracle.  The reference declares PEFRL
+without an implementation, so there is no golden vector: the checks are its
+order of accuracy (error ratio about 16 per halving of dt for a
+fourth-order method, 4 for PositionVerlet and VelocityVerlet) on free,
+undamped rods, where no first-order constraint splitting masks it."""
 import numpy as np
 import pytest
 
@@ -25,6 +25,7 @@ def _positions(wl, stepper, factor, horizon):
 
 
 @pytest.mark.parametrize("stepper,order,factors", [("position_verlet", 2, (2.0, 1.0, 0.5)),
+                                                   ("velocity_verlet", 2, (2.0, 1.0, 0.5)),
                                                    ("pefrl", 4, (4.0, 2.0, 1.0))])
 def test_order_of_accuracy(stepper, order, factors):
     wl = _free_batch()
@@ -44,3 +45,13 @@ def test_pefrl_more_accurate_than_verlet_at_equal_cost():
     e_pv = np.abs(_positions(wl, "position_verlet", 1.0, horizon) - ref).max()
     e_pe = np.abs(_positions(wl, "pefrl", 4.0, horizon) - ref).max()
     assert e_pe < e_pv
+
+
+def test_velocity_and_position_verlet_agree_to_second_order():
+    """Both second-order schemes approach the same trajectory: their
+    difference shrinks about 4x per halving of dt."""
+    wl = _free_batch()
+    horizon = 800 * wl.dt
+    d = [np.abs(_positions(wl, "velocity_verlet", f, horizon) - _positions(wl, "position_verlet", f, horizon)).max()
+         for f in (1.0, 0.5)]
+    assert 2.4 < d[0] / d[1] < 6.4, d
