@@ -87,8 +87,8 @@ def profile_traffic(kernel: str, workload: str, sources: tuple):
         return None, "no ncu summary"
     now = source_digest(*sources)
     if digest != now:
-        return None, f"ncu summary is of other kernel sources ({digest} != {now})"
-    return traffic, f"ncu capture of these sources ({now}), profiles/{kernel}_{workload}.txt"
+        return None, f"stale ncu summary ({digest} != {now})"
+    return traffic, f"ncu, sources {now}"
 
 
 class ClockSampler:
@@ -247,7 +247,7 @@ def workload_config(wl, world):
             "constraints": "clamp(node 0) + analytical damper 0.1", "gravity": list(wl.gravity or []),
             "parallelism": f"{world} element-balanced shards of one batch of {world} x the per-GPU rods "
                            "(Karmarkar-Karp partition, weak)" if world > 1 else "single GPU",
-            "l2": "no flush: state + parameters exceed the 126 MB L2 many times over"}
+            "l2": "no flush: inputs >> 126 MB L2"}
 
 
 def mixed_comparison(W, eb, torch, args, rank, local, barrier, pg):
@@ -543,7 +543,7 @@ def compact_sections(batched, contact, serving, cantilever, mixed):
                           "pefrl_default": batched["pefrl"]["default_plan"]["value"],
                           "pefrl_streaming": batched["pefrl"]["streaming"]["value"]}
     if contact is not None:
-        out["contact"] = _pick(contact, ("value", "ms_per_step", "candidate_pairs", "launches_per_step"))
+        out["contact"] = _pick(contact, ("value", "ms_per_step", "candidate_pairs"))
         if contact.get("cpu_baseline"):
             out["contact"]["cpu_value"] = contact["cpu_baseline"]["value"]
     if cantilever is not None:
@@ -552,7 +552,7 @@ def compact_sections(batched, contact, serving, cantilever, mixed):
                              "cpu_value": cantilever["cpu_baseline"]["value"]}
     if serving is not None:
         keys = ("rate_req_s", "arrival_window_s", "submitted", "completed", "censored", "p50_latency_s",
-                "p99_latency_s", "latency_percentiles", "p99_queueing_s", "value", "gpu_busy_frac", "fallbacks")
+                "p99_latency_s", "latency_percentiles", "p99_queueing_s", "value", "gpu_busy_frac")
         out["serving"] = {"stated": _pick(serving["stated_load"], keys),
                           "sustained": _pick(serving["sustained_load"], keys)}
     if mixed is not None:

@@ -204,6 +204,11 @@ struct eb_sim {
   // with one of the block configurations, chosen by timing both
   int plan_mode = 0;    // 0 undecided, 1 streaming, 2 resident, 3 resident per size bucket
   int plan_config = -1;
+  // the launch length (steps, at most one resident chunk) the plan was timed
+  // at, and whether it was chosen by timing (not forced by the flags, the
+  // collision system, connections or a configuration)
+  int plan_chunk = 0;
+  bool plan_timed = false;
   // per-size-bucket plan: bucket 0 holds the rods of at most 263 elements,
   // bucket 1 the rods of 264 to 519, bucket 2 the rods of 520 to 1039 (on
   // CTA pairs); per bucket and configuration a gathered work list (CTA
@@ -1642,7 +1647,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   // contact needs a global exchange every step, PEFRL four force evaluations
   // a step: the streaming kernel
   const bool force_stream = (s->cfg.flags & (EB_FLAG_STEP_STREAMING | EB_FLAG_REFERENCE_ROUNDING)) != 0 ||
-                            s->contact.on || s->jd.on || s->cfg.stepper == EB_STEPPER_VELOCITY_VERLET;
+                            s->contact.on || s->jd.on;
   if (force_stream) {
     s->plan_mode = 1;
     return EB_OK;
@@ -1700,6 +1705,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
             b.drift_pre = sub[j].pre * dt;
             b.kick = sub[j].kick * dt;
             b.drift_post = sub[j].post * dt;
+            b.damper_time = sub[j].damper * dt;
             EB_CUDA(launch_streaming(s, b, false));
           }
         EB_CUDA(cudaEventRecord(e1, s->stream));
@@ -1737,6 +1743,7 @@ eb_status plan_steps(eb_sim* s, double dt, int chunk) {
   cudaEventDestroy(e1);
   s->plan_mode = best_mode;
   s->plan_config = best_cfg;
+  s->plan_timed = true;
   return check_device_status(s);
 }
 
@@ -2013,8 +2020,17 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (eb_status st = set_device(s)) return st;
   if (eb_status st = damper_for_dt(s, dt)) return st;
   if (eb_status st = check_inverse_inertia(s)) return st;
-  if (s->plan_mode == 0)
-    if (eb_status st = plan_steps(s, dt, static_cast<int>(std::min<int64_t>(n_steps, kResidentChunk)))) return st;
+  {
+    // plan at the first call; plan again when a call's launches would be
+    // much longer than the ones the plan was timed at (a first call of a
+    // few steps favours the streaming kernel, whose launches carry no
+    // staging cost, for every later call)
+    const int chunk = static_cast<int>(std::min<int64_t>(n_steps, kResidentChunk));
+    if (s->plan_mode == 0 || (s->plan_timed && chunk >= 4 * s->plan_chunk)) {
+      if (eb_status st = plan_steps(s, dt, chunk)) return st;
+      s->plan_chunk = chunk;
+    }
+  }
   const bool diag = s->d_diag != nullptr;
   if (s->contact.on || s->jd.on) {
     if (eb_status st = step_with_contact(s, dt, n_steps, diag)) return st;

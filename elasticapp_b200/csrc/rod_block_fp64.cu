@@ -107,7 +107,8 @@ __device__ __forceinline__ int param_row(int f) {
 // kPair: cluster launch of CTA pairs; with kServe, CTAs 2i and 2i + 1 form a
 // pair when both serve entries say so and run the same step count, and are
 // single CTAs otherwise; without kServe every cluster is a pair
-// kPefrl: PEFRL's four force evaluations a step (PositionVerlet otherwise)
+// kStepper: 0 PositionVerlet, 1 PEFRL (four force evaluations a step), 2
+// VelocityVerlet (two: kick dt/2, drift dt, kick dt/2)
 // FP64 shared-memory rows per slot
 template <bool kDamped>
 constexpr int block_rows() { return kDamped ? 54 : 52; }
@@ -117,7 +118,7 @@ template <int kCap>
 constexpr int block_min_ctas() { return kCap <= 264 ? 2 : 1; }
 
 template <int kCap, int kThreads, bool kDamped, bool kSplit, bool kServe, bool kGather = false, bool kPair = false,
-          bool kPefrl = false>
+          int kStepper = 0>
 __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp64_kernel(const StepArgs a, const int64_t* cta_start,
                                                                     int n_steps_launch, const ServeCta* serve,
                                                                     const int32_t* gmap) {
@@ -207,8 +208,9 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
   }
   __syncthreads();
 
-  // drift of slot s by c (x += c v, Q <- exp(-c [w]x) Q), then, with
-  // `clamp`, the clamp's value constraint on a clamped rod's first slot
+  // drift of slot s by c (x += c v, Q <- exp(-c [w]x) Q; c = 0 leaves the
+  // slot as it is), then, with `clamp`, the value constraint of the clamp
+  // that holds the slot, if any
   auto drift = [&](int s, uint32_t meta, double c, bool clamp) {
     const D3 v = R.get3(bV, s);
     D3 x = R.get3(bX, s);
@@ -247,7 +249,8 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
 
   // Substeps: PositionVerlet (drift dt/2, kick dt, drift dt/2), or PEFRL's
   // four kicks with their drifts (in units of dt; compile-time constants)
-  constexpr int nsub = kPefrl ? 4 : 1;
+  constexpr bool kPefrl = kStepper == 1, kVelocity = kStepper == 2;
+  constexpr int nsub = kPefrl ? 4 : (kVelocity ? 2 : 1);
   auto pefrl_pre = [](int j) -> double {  // drift before force evaluation j
     return j == 0 ? kPefrlXi : (j == 2 ? 1.0 - 2.0 * (kPefrlChi + kPefrlXi) : kPefrlChi);
   };
@@ -256,7 +259,9 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
   };
 
   // ---- first drift of the first step and the clamp's value constraint
-  for (int s = tid; s < count; s += kThreads) drift(s, meta_s[s], kPefrl ? kPefrlXi * dt : hdt, true);
+  // (VelocityVerlet starts with a kick: no drift, the clamp's value alone)
+  for (int s = tid; s < count; s += kThreads)
+    drift(s, meta_s[s], kPefrl ? kPefrlXi * dt : (kVelocity ? 0.0 : hdt), true);
   sync_neighbours();
 
   // Two phases per force evaluation, one barrier after each: (1) element s
@@ -268,8 +273,12 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
   // them into one rotation is not an identity under the 1e-14 axis guard).
   for (int step = 0; step < n_steps; ++step)
   for (int sub = 0; sub < nsub; ++sub) {
-    const double kc = kPefrl ? pefrl_kick(sub) : 1.0;  // this kick, in units of dt
-    const double kdt = kPefrl ? kc * dt : dt;
+    const double kc = kPefrl ? pefrl_kick(sub) : (kVelocity ? 0.5 : 1.0);  // this kick, in units of dt
+    const double kdt = kc == 1.0 ? dt : kc * dt;
+    // the damper's time: the kick's share of dt for PEFRL, the full dt for
+    // VelocityVerlet (its constants hold dt and act after each kick)
+    const double dc = kVelocity ? 1.0 : kc;
+    const double ddt = dc == 1.0 ? dt : kdt;
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       D3 f{0.0, 0.0, 0.0}, tl{0.0, 0.0, 0.0};
@@ -366,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
           double em = 0.5 * (m + mn);
           if (first) em += 0.5 * m;
           if (meta & kLastElem) em += 0.5 * mn;
-          const double y = -ri->damper_r * em * kdt * e;
+          const double y = -ri->damper_r * em * ddt * e;
           w = {w.x * exp(y * ji.x), w.y * exp(y * ji.y), w.z * exp(y * ji.z)};
         }
       }
@@ -375,13 +384,16 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
         w = D3{0.0, 0.0, 0.0};
       }
       // exp(-nu_t dt) for a kick of dt; a fractional kick scales the exponent
-      if (hit & kHitDamper) v = scale(v, kc == 1.0 ? ri->damper_t : exp(log(ri->damper_t) * kc));
+      if (hit & kHitDamper) v = scale(v, dc == 1.0 ? ri->damper_t : exp(log(ri->damper_t) * dc));
       R.put3(bV, s, v);
       if (meta & kElem) R.put3(bW, s, w);
       if (sub + 1 < nsub) {
-        drift(s, meta, pefrl_pre(sub + 1) * dt, true);  // before the next force evaluation
+        // before the next force evaluation
+        drift(s, meta, kVelocity ? dt : pefrl_pre(sub + 1) * dt, true);
       } else if (step + 1 < n_steps) {
-        if (kPefrl) {
+        if (kVelocity) {
+          drift(s, meta, 0.0, true);  // the next step starts with a kick: the clamp's value alone
+        } else if (kPefrl) {
           drift(s, meta, kPefrlXi * dt, false);  // closing drift of this step, own slot
           drift(s, meta, kPefrlXi * dt, true);   // first drift of the next
         } else if (kSplit) {
@@ -399,7 +411,7 @@ __global__ void __launch_bounds__(kThreads, block_min_ctas<kCap>()) rod_block_fp
   }
 
   // ---- closing drift of the last step and write-back
-  const double fin = kPefrl ? kPefrlXi * dt : hdt;
+  const double fin = kPefrl ? kPefrlXi * dt : (kVelocity ? 0.0 : hdt);
   for (int s = tid; s < count; s += kThreads) {
     const uint32_t meta = meta_s[s];
     const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
@@ -458,9 +470,12 @@ cudaError_t launch_block_cfg(const StepArgs& args, const int64_t* cta_start, int
     }
   };
   if constexpr (!kServe) {  // serving launches are PositionVerlet
-    if (args.n_sub > 1)
-      return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair, true>)
-                    : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair, true>);
+    if (args.n_sub == 4)
+      return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair, 1>)
+                    : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair, 1>);
+    if (args.n_sub == 2)
+      return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair, 2>)
+                    : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair, 2>);
   }
   return damped ? go(rod_block_fp64_kernel<kCap, kThreads, true, kSplit, kServe, kGather, kPair>)
                 : go(rod_block_fp64_kernel<kCap, kThreads, false, kSplit, kServe, kGather, kPair>);

@@ -48,20 +48,36 @@ namespace {
 
 // shared-memory row of every staged input field: the 18 state rows, then the
 // parameter rows the variant needs (nu_f/nu_t only for explicitly damped
-// rods, the volume only when diagnostics are recorded)
-template <bool kDamped, bool kDiag>
+// rods, the volume only when diagnostics are recorded, the stored J^-1 only
+// when some stored J^-1 differs from 1 / J: otherwise 1 / J is formed, bit
+// identical to the stored value, which the initializer forms as 1.0 / J of
+// the same product)
+template <bool kDamped, bool kDiag, bool kStoredJinv>
 struct RowMap {
-  static constexpr int param(int f) {
-    return kStateFields + f - ((!kDamped && f > kNuF) ? 1 : 0) - ((!kDamped && f > kNuT) ? 1 : 0) -
-           ((!kDiag && f > kVol) ? 1 : 0);
-  }
   static constexpr bool needed(int f) {
-    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol));
+    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol) ||
+             (!kStoredJinv && f >= kJinv && f < kJinv + 3));
   }
-  static constexpr int rows() { return kStateFields + kParamFields - (kDamped ? 0 : 2) - (kDiag ? 0 : 1); }
+  static constexpr int param(int f) {
+    int r = kStateFields;
+    for (int k = 0; k < f; ++k) r += needed(k) ? 1 : 0;
+    return r;
+  }
+  static constexpr int rows() { return param(kParamFields); }
 };
 
 constexpr uint32_t kMaxPolls = 1u << 22;
+// polls of the wait that follows a timeout: far above any copy's duration
+// (seconds), so a CTA leaves only once the copies into its shared memory
+// are done
+constexpr uint32_t kDrainPolls = 1u << 30;
+
+// bounded wait for a barrier phase; a caller-set bound (StepArgs::max_polls)
+// polls without blocking, so a small one gives up before copies issued just
+// before can land (to exercise the timeout path)
+__device__ __forceinline__ bool wait_copies(const StepArgs& a, uint64_t* bar) {
+  return a.max_polls ? mbar_test_bounded(bar, 0, a.max_polls) : mbar_wait_bounded(bar, 0, kMaxPolls);
+}
 using D3 = Vec3<double>;
 
 template <int W>
@@ -124,9 +140,9 @@ __device__ __forceinline__ void clamp_value(const RodInfo& ri, uint32_t hits, ui
   }
 }
 
-template <int W, bool kDiag, bool kDamped, bool kContact>
+template <int W, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
 __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem) {
-  using M = RowMap<kDamped, kDiag>;
+  using M = RowMap<kDamped, kDiag, kStoredJinv>;
   constexpr int kTile = W - 4;  // interior slots stored per CTA (even)
   constexpr int kLeftHalo = 2;  // window starts 2 slots left of the tile
   constexpr int kRows = M::rows();
@@ -139,8 +155,9 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   // exchange rows, each over rows only the owning thread reads:
   //   f (written in phase 2) over the angular velocity rows (read in phase 1)
   //   l (phase 2) over the first rest-strain row (read earlier in phase 2)
-  //   g, h (phase 3) over the inertia and shear rigidity rows (read in phase 2)
-  constexpr int rF = rW, rL = rSig0, rG = rJ, rH = rShear;
+  //   g, h (phase 3) over the rest-curvature and bend-rigidity rows (read
+  //   earlier in phase 3), so the inertia rows J stay for phase 4's 1 / J
+  constexpr int rF = rW, rL = rSig0, rG = rKap0, rH = rBend;
 
   const Rows<W> R{smem};
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kRows * W);
@@ -186,14 +203,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     for (int f = 0; f < kParamFields; ++f)
       if (M::needed(f) && f != kMass) bulk_g2s(R.row(M::param(f)) + off, a.par + f * S + lo, bytes, bar + 1);
   }
-  if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
-    // a copy never completed: record it, give the copies one more bounded
-    // wait so none is left writing into this CTA's shared memory, and leave
-    if (s == 0) atomicOr(a.status, kStatusCopyTimeout);
-    (void)mbar_wait_bounded(bar, 0, kMaxPolls);
-    (void)mbar_wait_bounded(bar + 1, 0, kMaxPolls);
-    return;
-  }
+  const bool ok0 = wait_copies(a, bar);
 
   const double hdt = a.drift_pre;
 
@@ -204,7 +214,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 #pragma unroll
   for (int k = 0; k < 9; ++k) q[k] = 0.0;
   double m = 1.0;
-  if (valid) {
+  if (ok0 && valid) {
     v = R.get3(rV, s);
     const D3 x0 = R.get3(rX, s);
     x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
@@ -220,12 +230,16 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 #pragma unroll
     for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
   }
-  if (!mbar_wait_bounded(bar + 1, 0, kMaxPolls)) {
+  const bool ok1 = ok0 && wait_copies(a, bar + 1);
+  if (!__syncthreads_and(ok1)) {
+    // a copy did not land within the bound (every thread agrees): record it,
+    // wait for the copies issued into this CTA's shared memory so none is
+    // left writing there, and leave
     if (s == 0) atomicOr(a.status, kStatusCopyTimeout);
-    (void)mbar_wait_bounded(bar + 1, 0, kMaxPolls);
+    (void)mbar_wait_bounded(bar, 0, kDrainPolls);
+    (void)mbar_wait_bounded(bar + 1, 0, kDrainPolls);
     return;
   }
-  __syncthreads();
 
   // ---- phase 2: element geometry and internal stress
   // (CosseratRodSpanwiseGeometry.hpp:579-644, WithDiagonalLinearHyperElasticModel.hpp:198-238)
@@ -345,7 +359,12 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       const RodInfo& ri = a.rods[meta >> kRodShift];
       Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
     }
-    jinv = R.get3(rJinv, s);
+    if (kStoredJinv) {
+      jinv = R.get3(rJinv, s);
+    } else {
+      const D3 J = R.get3(rJ, s);
+      jinv = {1.0 / J.x, 1.0 / J.y, 1.0 / J.z};
+    }
     alpha = {(jinv.x * (T.x + Te.x)) * e, (jinv.y * (T.y + Te.y)) * e, (jinv.z * (T.z + Te.z)) * e};
   }
 
@@ -418,376 +437,17 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
 }
 
-// ---------------------------------------------------------------------------
-// Persistent form: a grid of (resident CTAs per SM) x (SMs) CTAs, each
-// walking the windows blockIdx.x, blockIdx.x + gridDim.x, ... with two stage
-// buffers.  While a CTA computes window i from one buffer, the bulk copies of
-// window i + 1 land in the other, so a CTA no longer waits for its inputs
-// after its first window; the slot's metadata word and its rod's constraint
-// data for window i + 1 are loaded during window i as well.  The stored
-// J^-1 rows are not read: 1 / J is formed instead (bit-identical to the
-// stored value, which the initializer forms as 1.0 / J of the same product;
-// when a caller has set J or J^-1 so that they disagree, the host selects
-// the kStoredJinv variant, which reads the stored rows).
-
-// rows of one stage buffer: the 18 state rows, then every parameter the
-// variant reads, in ParamField order
-template <bool kDamped, bool kDiag, bool kStoredJinv>
-struct StageMap {
-  static constexpr bool needed(int f) {
-    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol) ||
-             (!kStoredJinv && f >= kJinv && f < kJinv + 3));
-  }
-  static constexpr int param(int f) {
-    int r = kStateFields;
-    for (int k = 0; k < f; ++k) r += needed(k) ? 1 : 0;
-    return r;
-  }
-  static constexpr int rows() { return param(kParamFields); }
-};
-
-// polls of the wait that follows a timeout: far above any copy's duration
-// (seconds), so a CTA leaves only once the copies into its buffers are done
-constexpr uint32_t kDrainPolls = 1u << 30;
-
-template <int W, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
-__device__ __forceinline__ void rod_step_persistent(const StepArgs& a, double* smem) {
-  using M = StageMap<kDamped, kDiag, kStoredJinv>;
-  constexpr int kTile = W - 4;
-  constexpr int kLeftHalo = 2;
-  constexpr int kRows = M::rows();
-  constexpr int kStage = kRows * W;  // doubles per stage buffer
-  constexpr int rX = kStX, rV = kStV, rQ = kStQ, rW = kStW;
-  constexpr int rMass = M::param(kMass), rL0 = M::param(kL0), rD0 = M::param(kD0);
-  constexpr int rSig0 = M::param(kSig0), rKap0 = M::param(kKap0), rShear = M::param(kShear);
-  constexpr int rBend = M::param(kBend), rJ = M::param(kJ), rJinv = M::param(kJinv);
-  constexpr int rNuF = M::param(kNuF), rNuT = M::param(kNuT), rVol = M::param(kVol);
-  // exchange rows over rows only the owning thread reads (as in the
-  // windowed kernel): f over w, l over the first rest-strain row, g over J,
-  // h over the shear rigidity
-  constexpr int rF = rW, rL = rSig0, rG = rJ, rH = rShear;
-
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
-  const int s = threadIdx.x;
-  const int64_t S = a.stride;
-  const int64_t n_win = (a.n_slots + kTile - 1) / kTile;
-  const int64_t G = gridDim.x;
-  int64_t w = blockIdx.x;
-  if (w >= n_win) return;  // the same for every thread of the CTA
-
-  // thread 0: the bulk copies of window v's rows into stage buffer b
-  auto issue = [&](int64_t v, int b) {
-    const int64_t g0 = v * kTile - kLeftHalo;
-    const int64_t lo = g0 < 0 ? 0 : g0;
-    const int64_t hi = (g0 + W < S) ? g0 + W : S;
-    const uint32_t bytes = static_cast<uint32_t>((hi - lo) * sizeof(double));
-    const int off = static_cast<int>(lo - g0);
-    double* base = smem + b * kStage;
-    mbar_arrive_expect_tx(bar + b, bytes * static_cast<uint32_t>(kRows));
-#pragma unroll 1
-    for (int f = 0; f < kStateFields; ++f) bulk_g2s(base + f * W + off, a.in + f * S + lo, bytes, bar + b);
-#pragma unroll 1
-    for (int f = 0; f < kParamFields; ++f)
-      if (M::needed(f)) bulk_g2s(base + M::param(f) * W + off, a.par + f * S + lo, bytes, bar + b);
-  };
-  auto slot_of = [&](int64_t v) { return v * kTile - kLeftHalo + s; };
-  // the rod data a slot's constraints read: its hits (which clamp holds
-  // it, the torque, the damper) and the damper's constants
-  auto rod_data = [&](uint32_t m, int64_t gs, bool ok, uint32_t& hit, double& dt_, double& dr_) {
-    hit = 0;
-    dt_ = 1.0;
-    dr_ = 0.0;
-    if (ok && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
-      const RodInfo& ri = a.rods[m >> kRodShift];
-      hit = slot_hits(ri, gs);
-      dt_ = ri.damper_t;
-      dr_ = ri.damper_r;
-    }
-  };
-
-  if (s == 0) {
-    mbar_init(bar, 1);
-    mbar_init(bar + 1, 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  if (s == 0) issue(w, 0);
-  int64_t g = slot_of(w);
-  bool valid = g >= 0 && g < a.n_slots;
-  uint32_t meta = valid ? a.meta[g] : 0u;
-  uint32_t hits;
-  double damper_t, damper_r;
-  rod_data(meta, g, valid, hits, damper_t, damper_r);
-
-  for (int it = 0;; ++it) {
-    const int b = it & 1;
-    const uint32_t parity = static_cast<uint32_t>(it >> 1) & 1u;
-    const int64_t wn = w + G;
-    const bool has_next = wn < n_win;
-    // the next window's metadata word, consumed one window later
-    const int64_t gn = slot_of(wn);
-    const bool valid_n = has_next && gn >= 0 && gn < a.n_slots;
-    const uint32_t meta_n = valid_n ? a.meta[gn] : 0u;
-    const bool interior = valid && s >= kLeftHalo && s < kLeftHalo + kTile;
-    const Rows<W> R{smem + b * kStage};
-    const double hdt = a.drift_pre;
-
-    // ---- phase 1: first kinematic half step and clamp value constraint
-    // bounded wait; a caller-set bound polls without blocking, so a small
-    // one gives up before the copies land (to exercise the timeout path)
-    const bool ok = a.max_polls ? mbar_test_bounded(bar + b, parity, a.max_polls)
-                                : mbar_wait_bounded(bar + b, parity, kMaxPolls);
-    D3 x{0.0, 0.0, 0.0}, v{0.0, 0.0, 0.0}, wv{0.0, 0.0, 0.0};
-    double q[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) q[k] = 0.0;
-    double m = 1.0;
-    if (ok && valid) {
-      v = R.get3(rV, s);
-      const D3 x0 = R.get3(rX, s);
-      x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
-      m = R.at(rMass, s);
-      if (meta & kElem) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
-        wv = R.get3(rW, s);
-        so3(q, hdt * wv.x, hdt * wv.y, hdt * wv.z);
-      }
-      if (hits & (kHitClamp0 | kHitClamp1)) clamp_value(a.rods[meta >> kRodShift], hits, meta, x, q);
-      R.put3(rX, s, x);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
-    }
-    // this thread's reads and writes of the other buffer (the previous
-    // window) come before that buffer is refilled by bulk copies
-    fence_proxy_async_smem();
-    if (!__syncthreads_and(ok)) {
-      // a copy did not land within the bound: record it, wait for the
-      // copies into this buffer (the only ones issued and not yet waited
-      // for) and leave
-      if (s == 0) atomicOr(a.status, kStatusCopyTimeout);
-      (void)mbar_wait_bounded(bar + b, parity, kDrainPolls);
-      return;
-    }
-    if (s == 0 && has_next) issue(wn, b ^ 1);
-
-    // ---- phase 2: element geometry, internal stress, element-local torque
-    // terms (CosseratRodSpanwiseGeometry.hpp:579-644,
-    // WithDiagonalLinearHyperElasticModel.hpp:198-238, 341-384)
-    const bool elem = (meta & kElem) && s + 1 < W;
-    double l = 1.0, e = 1.0, l0 = 1.0;
-    D3 t{0.0, 0.0, 0.0}, sigma{0.0, 0.0, 0.0}, nl{0.0, 0.0, 0.0};
-    D3 t_shear{0.0, 0.0, 0.0}, t_lag{0.0, 0.0, 0.0}, t_unst{0.0, 0.0, 0.0};
-    D3 J{1.0, 1.0, 1.0};
-    {
-      D3 f{0.0, 0.0, 0.0};
-      if (elem) {
-        const D3 dx = R.get3(rX, s + 1) - x;
-        l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
-        t = div3(dx, l);
-        l0 = R.at(rL0, s);
-        e = l / l0;
-        const D3 qt = matvec(q, t);
-        sigma = {qt.x * e, qt.y * e, qt.z * e - 1.0};
-        const D3 d = sigma - R.get3(rSig0, s);
-        const D3 sh = R.get3(rShear, s);
-        nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
-        f = div3(mattranspvec(q, nl), e);
-        t_shear = scale(cross(qt, nl), l0);
-        J = R.get3(rJ, s);
-        const D3 jwe = div3(D3{J.x * wv.x, J.y * wv.y, J.z * wv.z}, e);
-        t_lag = cross(jwe, wv);
-        const D3 dv = R.get3(rV, s + 1) - v;
-        const double rate = dot(t, dv) / (e * l0);
-        t_unst = scale(jwe, rate);
-      }
-      R.at(rL, s) = l;
-      R.put3(rF, s, f);
-    }
-    __syncthreads();
-    // the next window's rod data (its metadata word has arrived by now),
-    // first read in that window's phase 1 (clamped first slots) or phase 4
-    uint32_t hits_n;
-    double damper_t_n, damper_r_n;
-    rod_data(meta_n, gn, valid_n, hits_n, damper_t_n, damper_r_n);
-
-    // ---- phase 3: Voronoi curvature and couple
-    // (CosseratRodSpanwiseGeometry.hpp:652-664, WithDiagonalLinearHyperElasticModel.hpp:293-338)
-    D3 kappa{0.0, 0.0, 0.0}, tau{0.0, 0.0, 0.0};
-    double eps = 1.0;
-    {
-      D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
-      if ((meta & kVor) && s + 1 < W) {
-        double qn[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) qn[k] = R.at(rQ + k, s + 1);
-        const double D0 = R.at(rD0, s);
-        kappa = curvature(q, qn, D0);
-        const double D = 0.5 * (l + R.at(rL, s + 1));
-        eps = D / D0;
-        const double ic = 1.0 / (eps * eps * eps);
-        const D3 dk = kappa - R.get3(rKap0, s);
-        const D3 B = R.get3(rBend, s);
-        tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
-        gg = scale(tau, ic);
-        hh = scale(cross(kappa, tau), ic * D0);
-      }
-      R.put3(rG, s, gg);
-      R.put3(rH, s, hh);
-    }
-    __syncthreads();
-
-    if (interior) {
-      // ---- phase 4: loads, update_acceleration (WithRodKinematics.hpp:684-714)
-      D3 F = R.get3(rF, s) - R.get3(rF, s - 1);
-      if (kDamped) {
-        const double c = m * R.at(rNuF, s);
-        F = {F.x - c * v.x, F.y - c * v.y, F.z - c * v.z};
-      }
-      D3 Fe{0.0, 0.0, 0.0};
-      if (a.sim_flags & kSimGravity)
-        Fe = {0.0 + a.gravity[0] * m, 0.0 + a.gravity[1] * m, 0.0 + a.gravity[2] * m};
-      if (kContact && a.contact_force) {
-        // Systems/Customization/CosseratRods/Transfer/Common.hpp:32-55
-        const double* __restrict__ cf = a.contact_force;
-        if (!(meta & kFirst))
-          Fe = {Fe.x + 0.5 * cf[g - 1], Fe.y + 0.5 * cf[S + g - 1], Fe.z + 0.5 * cf[2 * S + g - 1]};
-        if (meta & kElem) Fe = {Fe.x + 0.5 * cf[g], Fe.y + 0.5 * cf[S + g], Fe.z + 0.5 * cf[2 * S + g]};
-      }
-      if (kContact && a.joint_force) {
-        const double* __restrict__ jf = a.joint_force;
-        Fe = {Fe.x + jf[g], Fe.y + jf[S + g], Fe.z + jf[2 * S + g]};
-      }
-      const double inv_m = 1.0 / m;
-      const D3 acc = {(F.x + Fe.x) * inv_m, (F.y + Fe.y) * inv_m, (F.z + Fe.z) * inv_m};
-
-      D3 T{0.0, 0.0, 0.0}, alpha{0.0, 0.0, 0.0};
-      D3 jinv{0.0, 0.0, 0.0};
-      if (meta & kElem) {
-        T = R.get3(rG, s) - R.get3(rG, s - 1);                // two-point difference of g
-        const D3 h1 = R.get3(rH, s), h0 = R.get3(rH, s - 1);  // quadrature of h
-        T = T + D3{0.5 * (h1.x + h0.x), 0.5 * (h1.y + h0.y), 0.5 * (h1.z + h0.z)};
-        T = T + t_shear;
-        T = T + t_lag;
-        T = T + t_unst;
-        if (kDamped) {
-          const double em = 0.5 * (m + R.at(rMass, s + 1));
-          const double c = em * R.at(rNuT, s);
-          T = {T.x - c * wv.x, T.y - c * wv.y, T.z - c * wv.z};
-        }
-        D3 Te{0.0, 0.0, 0.0};
-        if (kContact && a.contact_torque) {
-          const double* __restrict__ ct = a.contact_torque;
-          Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
-        }
-        if (kContact && a.joint_torque) {
-          const double* __restrict__ jt = a.joint_torque;
-          Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
-        }
-        if (hits & kHitTorque) {
-          const RodInfo& ri = a.rods[meta >> kRodShift];
-          Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
-        }
-        if (kStoredJinv)
-          jinv = R.get3(rJinv, s);
-        else
-          jinv = {1.0 / J.x, 1.0 / J.y, 1.0 / J.z};
-        alpha = {(jinv.x * (T.x + Te.x)) * e, (jinv.y * (T.y + Te.y)) * e, (jinv.z * (T.z + Te.z)) * e};
-      }
-
-      // ---- dynamic step and rate constraints
-      const double dt = a.kick;
-      v = {v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z};
-      if (meta & kElem) wv = {wv.x + dt * alpha.x, wv.y + dt * alpha.y, wv.z + dt * alpha.z};
-      if (hits & (kHitClamp0 | kHitClamp1)) {
-        v = D3{0.0, 0.0, 0.0};
-        wv = D3{0.0, 0.0, 0.0};
-      }
-      if (hits & kHitDamper) {
-        // the damper's factors for its time (see StepArgs::damper_time)
-        const double ddt = a.damper_time;
-        double dmp = damper_t;
-        if (ddt != a.dt) dmp = exp(log(dmp) * (ddt / a.dt));
-        v = {v.x * dmp, v.y * dmp, v.z * dmp};
-        if (meta & kElem) {
-          // AnalyticalLinearDamper.hpp:40-75 (see the windowed kernel)
-          const double mn = R.at(rMass, s + 1);
-          double em = 0.5 * (m + mn);
-          if (meta & kFirst) em += 0.5 * m;
-          if (meta & kLastElem) em += 0.5 * mn;
-          const double nur = damper_r;
-#ifdef EB_FAST_FP64
-          wv = {wv.x * exp(e * (-nur * em * jinv.x * ddt)), wv.y * exp(e * (-nur * em * jinv.y * ddt)),
-                wv.z * exp(e * (-nur * em * jinv.z * ddt))};
-#else
-          wv = {wv.x * pow(exp(-nur * em * jinv.x * ddt), e), wv.y * pow(exp(-nur * em * jinv.y * ddt), e),
-                wv.z * pow(exp(-nur * em * jinv.z * ddt), e)};
-#endif
-        }
-      }
-
-      // ---- second kinematic half step and store
-      const double hdt2 = a.drift_post;
-      x = {x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z};
-      double* __restrict__ out = a.out;
-      st3(out + kStX * S, S, g, x);
-      st3(out + kStV * S, S, g, v);
-      if (meta & kElem) {
-        so3(q, hdt2 * wv.x, hdt2 * wv.y, hdt2 * wv.z);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) out[(kStQ + k) * S + g] = q[k];
-        st3(out + kStW * S, S, g, wv);
-      }
-
-      if (kDiag) {
-        double* __restrict__ dg = a.diag;
-        st3(dg + kDLoads * S, S, g, F);
-        st3(dg + kDAccel * S, S, g, acc);
-        if (meta & kElem) {
-          dg[kDLength * S + g] = e * l0;
-          dg[kDDil * S + g] = e;
-          st3(dg + kDTangent * S, S, g, t);
-          st3(dg + kDSigma * S, S, g, sigma);
-          st3(dg + kDStress * S, S, g, nl);
-          st3(dg + kDTorques * S, S, g, T);
-          st3(dg + kDAlpha * S, S, g, alpha);
-          dg[kDDim * S + g] = sqrt(M_1_PI * R.at(rVol, s) / l);
-        }
-        if (meta & kVor) {
-          dg[kDVDil * S + g] = eps;
-          st3(dg + kDKappa * S, S, g, kappa);
-          st3(dg + kDCouple * S, S, g, tau);
-        }
-      }
-    }
-    if (!has_next) break;
-    w = wn;
-    g = gn;
-    valid = valid_n;
-    meta = meta_n;
-    hits = hits_n;
-    damper_t = damper_t_n;
-    damper_r = damper_r_n;
-  }
+template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
+__global__ void __launch_bounds__(W, MinBlocks) rod_step_fp64_kernel(const StepArgs a) {
+  extern __shared__ __align__(128) double smem[];
+  rod_step_window<W, kDiag, kDamped, kContact, kStoredJinv>(a, smem);
 }
 
 template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
-__global__ void __launch_bounds__(W, MinBlocks) rod_step_persistent_kernel(const StepArgs a) {
-  extern __shared__ __align__(128) double smem[];
-  rod_step_persistent<W, kDiag, kDamped, kContact, kStoredJinv>(a, smem);
-}
-
-template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
-__global__ void __launch_bounds__(W, MinBlocks) rod_step_fp64_kernel(const StepArgs a) {
-  extern __shared__ __align__(128) double smem[];
-  rod_step_window<W, kDiag, kDamped, kContact>(a, smem);
-}
-
-template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
 cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   constexpr int kTile = W - 4;
-  constexpr size_t bytes = size_t(RowMap<kDamped, kDiag>::rows()) * W * sizeof(double) + 16;
-  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped, kContact>;
+  constexpr size_t bytes = size_t(RowMap<kDamped, kDiag, kStoredJinv>::rows()) * W * sizeof(double) + 16;
+  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped, kContact, kStoredJinv>;
   // the attribute is per device; setting it on every launch is cheap and
   // keeps multi-device use correct
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -797,13 +457,19 @@ cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <int W, int MinBlocks, bool kContact, bool kStoredJinv>
+cudaError_t launch_window_j(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
+  if (diag)
+    return damped ? launch_variant<W, MinBlocks, true, true, kContact, kStoredJinv>(args, stream)
+                  : launch_variant<W, MinBlocks, true, false, kContact, kStoredJinv>(args, stream);
+  return damped ? launch_variant<W, MinBlocks, false, true, kContact, kStoredJinv>(args, stream)
+                : launch_variant<W, MinBlocks, false, false, kContact, kStoredJinv>(args, stream);
+}
+
 template <int W, int MinBlocks, bool kContact>
 cudaError_t launch_window_c(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if (diag)
-    return damped ? launch_variant<W, MinBlocks, true, true, kContact>(args, stream)
-                  : launch_variant<W, MinBlocks, true, false, kContact>(args, stream);
-  return damped ? launch_variant<W, MinBlocks, false, true, kContact>(args, stream)
-                : launch_variant<W, MinBlocks, false, false, kContact>(args, stream);
+  return args.stored_jinv ? launch_window_j<W, MinBlocks, kContact, true>(args, diag, damped, stream)
+                          : launch_window_j<W, MinBlocks, kContact, false>(args, diag, damped, stream);
 }
 
 template <int W, int MinBlocks>
@@ -812,62 +478,6 @@ cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStre
   if ((args.contact_force && args.contact_torque) || (args.joint_force && args.joint_torque))
     return launch_window_c<W, MinBlocks, true>(args, diag, damped, stream);
   return launch_window_c<W, MinBlocks, false>(args, diag, damped, stream);
-}
-
-// persistent form: as many CTAs as fit on the device at once (at most one per
-// window); the resident count per SM is measured once per variant and device
-template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
-cudaError_t launch_persistent_variant(const StepArgs& args, cudaStream_t stream) {
-  constexpr int kTile = W - 4;
-  constexpr size_t bytes =
-      2 * size_t(StageMap<kDamped, kDiag, kStoredJinv>::rows()) * W * sizeof(double) + 2 * sizeof(uint64_t);
-  auto kern = rod_step_persistent_kernel<W, MinBlocks, kDiag, kDamped, kContact, kStoredJinv>;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  constexpr int kMaxDevices = 64;
-  static int blocks_per_sm[kMaxDevices] = {};
-  static int sms[kMaxDevices] = {};
-  if (dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  // the attribute is per device; setting it on every launch keeps
-  // multi-device use correct
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-  if (e != cudaSuccess) return e;
-  if (blocks_per_sm[dev] == 0) {
-    int n = 0, count = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, W, bytes);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    sms[dev] = count;
-    blocks_per_sm[dev] = n > 0 ? n : 1;
-  }
-  const int64_t windows = (args.n_slots + kTile - 1) / kTile;
-  const int64_t cap = static_cast<int64_t>(blocks_per_sm[dev]) * sms[dev];
-  const unsigned grid = static_cast<unsigned>(windows < cap ? windows : cap);
-  kern<<<grid, W, bytes, stream>>>(args);
-  return cudaGetLastError();
-}
-
-template <bool kContact, bool kStoredJinv>
-cudaError_t launch_persistent_j(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if (diag)
-    return damped ? launch_persistent_variant<128, 2, true, true, kContact, kStoredJinv>(args, stream)
-                  : launch_persistent_variant<128, 2, true, false, kContact, kStoredJinv>(args, stream);
-  return damped ? launch_persistent_variant<128, 3, false, true, kContact, kStoredJinv>(args, stream)
-                : launch_persistent_variant<128, 3, false, false, kContact, kStoredJinv>(args, stream);
-}
-
-template <bool kContact>
-cudaError_t launch_persistent_c(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  return args.stored_jinv ? launch_persistent_j<kContact, true>(args, diag, damped, stream)
-                          : launch_persistent_j<kContact, false>(args, diag, damped, stream);
-}
-
-cudaError_t launch_persistent(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if ((args.contact_force && args.contact_torque) || (args.joint_force && args.joint_torque))
-    return launch_persistent_c<true>(args, diag, damped, stream);
-  return launch_persistent_c<false>(args, diag, damped, stream);
 }
 
 }  // namespace
@@ -912,16 +522,15 @@ cudaError_t launch_check_inverse_inertia(int64_t stride, int64_t n_slots, const 
 #define EB_FP64_LAUNCHER launch_rod_step_fp64_reference
 #endif
 
-// window: 0 for the persistent kernel (128-slot windows, two stage
-// buffers); 128 or 256 for one CTA per window of that many slots
+// window: slots per CTA: 0 (128-slot windows, six CTAs an SM), 128 (five
+// CTAs an SM) or 256
 cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream) {
   if (args.n_slots <= 0) return cudaSuccess;
   // every field row of a window must start on a 16-byte boundary
   if ((args.stride & 1) || (reinterpret_cast<uintptr_t>(args.in) & 15) ||
       (reinterpret_cast<uintptr_t>(args.par) & 15))
     return cudaErrorMisalignedAddress;
-  if (window == 0) return launch_persistent(args, diag, damped, stream);
-  // the windowed kernels read the stored J^-1 rows
+  if (window == 0) return launch_window<128, 6>(args, diag, damped, stream);
   if (window == 128) return launch_window<128, 5>(args, diag, damped, stream);
   return launch_window<256, 2>(args, diag, damped, stream);
 }

@@ -95,8 +95,8 @@ typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
   int32_t precision;       /* eb_precision */
   uint32_t flags;          /* EB_FLAG_* */
-  int32_t step_window;     /* streaming kernel: 0 (default) persistent CTAs over 128-slot windows with
-                              double-buffered inputs; 128 or 256: one CTA per window of that many slots */
+  int32_t step_window;     /* streaming kernel, slots per CTA: 0 (default, 128 slots, six CTAs an SM),
+                              128 (five CTAs an SM) or 256 */
   int32_t resident_config; /* 0: chosen by timing; c > 0: resident configuration c - 1 */
   int32_t stepper;         /* eb_stepper (0: PositionVerlet) */
 } eb_config;
@@ -425,7 +425,7 @@ EB_API eb_status eb_step_plan(const struct eb_sim* sim, int32_t* mode, int32_t* 
                               int32_t count);
 
 /* Debug only: the number of polls after which the streaming step kernel's
- * waits for its bulk copies give up (0 restores the built-in bound, millions
+ * waits for its bulk copies give up (polled without blocking) (0 restores the built-in bound, millions
  * of polls).  A kernel that gives up records it in the simulator's status,
  * waits for the copies it issued and returns; the next call that reads the
  * status (eb_get_field, eb_synchronize, ...) returns EB_ERR_CUDA and the

@@ -30,12 +30,19 @@ def test_damper_decays_as_closed_form(eb, kw):
     rod.set("Velocity", A.translating_velocity())
     rod.set("AngularVelocity", A.spinning_omega())
     t, done = 0.0, 0
+    eps = np.finfo(float).eps
     for k in (1, 10, A.STEPS):
         t = sim.step(eb.PositionVerlet(), t, A.DT, k - done)
         done = k
         v, w = rod.get("Velocity"), rod.get("AngularVelocity")
-        tol = 8.0 * k * np.finfo(float).eps
-        assert A.rel(v, np.repeat(A.damped_velocity(k)[:, None], A.N + 1, axis=1)) <= tol, (k, kw)
+        tol = 8.0 * k * eps
+        # the fast build forms the tangent as dx * (1 / l), which can be one
+        # ulp off unit length: the end elements then carry a strain of eps,
+        # whose unbalanced load E A eps on the end nodes (mass rho A l0 / 2)
+        # moves v by 2 E eps dt / (rho l0 |v0|) relative a step
+        tol_v = tol if kw.get("reference_rounding") else \
+            4.0 * (tol + k * 2.0 * A.YOUNGS * eps * A.DT / (A.DENSITY * A.L0 * np.linalg.norm(A.V0)))
+        assert A.rel(v, np.repeat(A.damped_velocity(k)[:, None], A.N + 1, axis=1)) <= tol_v, (k, kw)
         assert A.rel(w[2], np.full(A.N, A.damped_spin(k))) <= tol, (k, kw)
         # the loads are zero up to the rounding of contracted multiply-adds
         assert np.max(np.abs(w[:2])) <= 1e-12 * A.W0 and np.max(np.abs(v[0])) <= 1e-12

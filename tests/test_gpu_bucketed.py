@@ -87,3 +87,24 @@ def test_bucketed_flag_falls_back_when_plan_does_not_apply(n_range, mode):
     sim = wl.build(step_mode="bucketed")
     sim.step(eb.PositionVerlet(), 0.0, wl.dt, 4)
     assert sim.step_plan()["mode"] in mode
+
+
+def test_plan_retimed_for_much_longer_calls():
+    """A plan chosen at a one-step call is timed again when a later call
+    runs 128-step launches (the resident kernels' staging cost is then
+    spread over 128 steps), and not again after that."""
+    import elasticapp_b200 as eb
+    from elasticapp_b200 import workloads as W
+
+    wl = W.uneven_batch(n_rods=600, seed=44, n_range=(32, 300))
+    sim = wl.build()
+    t = sim.step(eb.PositionVerlet(), 0.0, wl.dt, 1)
+    p1 = sim.step_plan()
+    t = sim.step(eb.PositionVerlet(), t, wl.dt, 256)
+    p2 = sim.step_plan()
+    t = sim.step(eb.PositionVerlet(), t, wl.dt, 256)
+    p3 = sim.step_plan()
+    assert p1["probe_ms"] != p2["probe_ms"]   # timed again at 128-step launches
+    assert p2["probe_ms"] == p3["probe_ms"]   # and kept
+    assert p2["mode"] in ("streaming", "resident", "bucketed")
+    sim.close()
