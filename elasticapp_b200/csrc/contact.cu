@@ -303,31 +303,22 @@ __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, in
     hi[d] = a.sorted_box[6 * e + 3 + d];
   }
   int32_t cnt = 0;
-  // one z-slice of the 27 neighbouring cells at a time: the nine bucket
-  // ranges are loaded together (independent loads in flight), then walked
-  for (int dz = -1; dz <= 1; ++dz) {
-    int32_t k0[9], k1[9];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-      const uint32_t b = cell_hash(cx + (c % 3) - 1, cy + (c / 3) - 1, cz + dz) & a.table_mask;
-      k0[c] = a.bucket_start[b];
-      k1[c] = a.bucket_start[b + 1];
-    }
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-      const int32_t nx = cx + (c % 3) - 1, ny = cy + (c / 3) - 1, nz = cz + dz;
-      const int32_t kend = min(k1[c], n_caps);
-      for (int32_t k = max(k0[c], 0); k < kend; ++k) {
-        if (a.sorted_cell[3 * k] != nx || a.sorted_cell[3 * k + 1] != ny || a.sorted_cell[3 * k + 2] != nz) continue;
-        const int32_t other = a.sorted_id[k];
-        if (other == id) continue;
-        const double* bx = a.sorted_box + 6 * k;
-        if (!overlaps(lo, hi, bx, bx + 3)) continue;
-        if (kPass == 1 || cnt < kFixedPartners) out[cnt] = other;
-        ++cnt;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int32_t nx = cx + dx, ny = cy + dy, nz = cz + dz;
+        const uint32_t b = cell_hash(nx, ny, nz) & a.table_mask;
+        const int32_t k0 = max(a.bucket_start[b], 0), k1 = min(a.bucket_start[b + 1], n_caps);
+        for (int32_t k = k0; k < k1; ++k) {
+          if (a.sorted_cell[3 * k] != nx || a.sorted_cell[3 * k + 1] != ny || a.sorted_cell[3 * k + 2] != nz) continue;
+          const int32_t other = a.sorted_id[k];
+          if (other == id) continue;
+          const double* bx = a.sorted_box + 6 * k;
+          if (!overlaps(lo, hi, bx, bx + 3)) continue;
+          if (kPass == 1 || cnt < kFixedPartners) out[cnt] = other;
+          ++cnt;
+        }
       }
-    }
-  }
   for (int32_t p = 0; p < a.n_planes; ++p) {
     if (!overlaps(lo, hi, a.planes[p].lo, a.planes[p].hi)) continue;
     if (kPass == 1 || cnt < kFixedPartners) out[cnt] = static_cast<int32_t>(a.n_slots) + p;

@@ -152,12 +152,16 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   constexpr int rSig0 = M::param(kSig0), rKap0 = M::param(kKap0), rShear = M::param(kShear);
   constexpr int rBend = M::param(kBend), rJ = M::param(kJ), rJinv = M::param(kJinv);
   constexpr int rNuF = M::param(kNuF), rNuT = M::param(kNuT), rVol = M::param(kVol);
-  // exchange rows, each over rows only the owning thread reads:
-  //   f (written in phase 2) over the angular velocity rows (read in phase 1)
-  //   l (phase 2) over the first rest-strain row (read earlier in phase 2)
-  //   g, h (phase 3) over the rest-curvature and bend-rigidity rows (read
-  //   earlier in phase 3), so the inertia rows J stay for phase 4's 1 / J
-  constexpr int rF = rW, rL = rSig0, rG = rKap0, rH = rBend;
+  // Exchange rows, each over rows only the owning thread reads and has read
+  // earlier in the same phase: f and l (phase 2) over the shear-rigidity
+  // rows and the first rest-strain row, g and h (phase 3) over the
+  // rest-curvature and bend-rigidity rows.  The state rows keep the slot's
+  // drifted position and directors (written in phase 1) and its velocity and
+  // angular velocity for the whole launch, and the mass and inertia rows stay
+  // too, so a thread re-reads its own slot from shared memory in each phase
+  // instead of holding it in registers across the barriers (registers, not
+  // shared-memory bandwidth, bound how many windows an SM runs at once).
+  constexpr int rF = rShear, rL = rSig0, rG = rKap0, rH = rBend;
 
   const Rows<W> R{smem};
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kRows * W);
@@ -167,18 +171,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const int64_t g = g0 + s;
   const int64_t S = a.stride;
   const bool valid = g >= 0 && g < a.n_slots;
-  const bool interior = valid && s >= kLeftHalo && s < kLeftHalo + kTile;
   const uint32_t meta = valid ? a.meta[g] : 0u;
   // per-rod constraint data, fetched while the bulk copies are in flight:
   // the slot's hits (which clamp holds it, the torque, the damper)
   uint32_t hits = 0;
-  double damper_t = 1.0, damper_r = 0.0;
-  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
-    const RodInfo& ri = a.rods[meta >> kRodShift];
-    hits = slot_hits(ri, g);
-    damper_t = ri.damper_t;
-    damper_r = ri.damper_r;
-  }
+  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) hits = slot_hits(a.rods[meta >> kRodShift], g);
 
   // ---- stage the window's inputs with bulk copies
   if (s == 0) {
@@ -205,30 +202,26 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
   const bool ok0 = wait_copies(a, bar);
 
-  const double hdt = a.drift_pre;
-
   // ---- phase 1: first kinematic half step and clamp value constraint,
-  // in place in shared memory
-  D3 x{0.0, 0.0, 0.0}, v{0.0, 0.0, 0.0}, w{0.0, 0.0, 0.0};
-  double q[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) q[k] = 0.0;
-  double m = 1.0;
+  // in place in shared memory (the velocity rows are left as they are)
   if (ok0 && valid) {
-    v = R.get3(rV, s);
+    const double hdt = a.drift_pre;
+    const D3 v = R.get3(rV, s);
     const D3 x0 = R.get3(rX, s);
-    x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
-    m = R.at(rMass, s);
+    D3 x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
+    double q[9];
     if (meta & kElem) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
-      w = R.get3(rW, s);
+      const D3 w = R.get3(rW, s);
       so3(q, hdt * w.x, hdt * w.y, hdt * w.z);
     }
     if (hits & (kHitClamp0 | kHitClamp1)) clamp_value(a.rods[meta >> kRodShift], hits, meta, x, q);
     R.put3(rX, s, x);
+    if (meta & kElem) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
+      for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
+    }
   }
   const bool ok1 = ok0 && wait_copies(a, bar + 1);
   if (!__syncthreads_and(ok1)) {
@@ -249,10 +242,18 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const bool elem = (meta & kElem) && s + 1 < W;
   double l = 1.0, e = 1.0, l0 = 1.0;
   D3 t{0.0, 0.0, 0.0}, sigma{0.0, 0.0, 0.0}, nl{0.0, 0.0, 0.0};
+#ifdef EB_FAST_FP64
+  D3 t_loc{0.0, 0.0, 0.0};  // shear + transport + dilatation terms, summed here
+#else
   D3 t_shear{0.0, 0.0, 0.0}, t_lag{0.0, 0.0, 0.0}, t_unst{0.0, 0.0, 0.0};
+#endif
   {
     D3 f{0.0, 0.0, 0.0};
     if (elem) {
+      double q[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
+      const D3 x = R.get3(rX, s);
       const D3 dx = R.get3(rX, s + 1) - x;
       l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
       t = div3(dx, l);
@@ -264,13 +265,18 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       const D3 sh = R.get3(rShear, s);
       nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
       f = div3(mattranspvec(q, nl), e);
-      t_shear = scale(cross(qt, nl), l0);
+      const D3 w = R.get3(rW, s);
       const D3 J = R.get3(rJ, s);
       const D3 jwe = div3(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
-      t_lag = cross(jwe, w);
-      const D3 dv = R.get3(rV, s + 1) - v;
+      const D3 dv = R.get3(rV, s + 1) - R.get3(rV, s);
       const double rate = dot(t, dv) / (e * l0);
+#ifdef EB_FAST_FP64
+      t_loc = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
+#else
+      t_shear = scale(cross(qt, nl), l0);
+      t_lag = cross(jwe, w);
       t_unst = scale(jwe, rate);
+#endif
     }
     R.at(rL, s) = l;
     R.put3(rF, s, f);
@@ -284,9 +290,12 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   {
     D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
     if ((meta & kVor) && s + 1 < W) {
-      double qn[9];
+      double q[9], qn[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) qn[k] = R.at(rQ + k, s + 1);
+      for (int k = 0; k < 9; ++k) {
+        q[k] = R.at(rQ + k, s);
+        qn[k] = R.at(rQ + k, s + 1);
+      }
       const double D0 = R.at(rD0, s);
       kappa = curvature(q, qn, D0);
       const double D = 0.5 * (l + R.at(rL, s + 1));
@@ -303,9 +312,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
   __syncthreads();
 
-  if (!interior) return;
+  if (!(valid && s >= kLeftHalo && s < kLeftHalo + kTile)) return;  // halo: computed, not stored
 
   // ---- phase 4: loads, update_acceleration (WithRodKinematics.hpp:684-714)
+  const double m = R.at(rMass, s);
+  D3 v = R.get3(rV, s);
   D3 F = R.get3(rF, s) - R.get3(rF, s - 1);
   if (kDamped) {
     const double c = m * R.at(rNuF, s);
@@ -332,31 +343,45 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 
   D3 T{0.0, 0.0, 0.0}, alpha{0.0, 0.0, 0.0};
   D3 jinv{0.0, 0.0, 0.0};
+  D3 w{0.0, 0.0, 0.0};
   if (meta & kElem) {
+    w = R.get3(rW, s);
     T = R.get3(rG, s) - R.get3(rG, s - 1);                // two-point difference of g
     const D3 h1 = R.get3(rH, s), h0 = R.get3(rH, s - 1);  // quadrature of h
     T = T + D3{0.5 * (h1.x + h0.x), 0.5 * (h1.y + h0.y), 0.5 * (h1.z + h0.z)};
+#ifdef EB_FAST_FP64
+    T = T + t_loc;
+#else
     T = T + t_shear;
     T = T + t_lag;
     T = T + t_unst;
+#endif
     if (kDamped) {
       const double em = 0.5 * (m + R.at(rMass, s + 1));
       const double c = em * R.at(rNuT, s);
       T = {T.x - c * w.x, T.y - c * w.y, T.z - c * w.z};
     }
     D3 Te{0.0, 0.0, 0.0};
-    if (kContact && a.contact_torque) {
-      // the capsule torque recast into the material frame: Q tau
-      const double* __restrict__ ct = a.contact_torque;
-      Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
-    }
-    if (kContact && a.joint_torque) {
-      // the connections' torque (summed in the lab frame), recast the same way
-      const double* __restrict__ jt = a.joint_torque;
-      Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
+    if (kContact && (a.contact_torque || a.joint_torque)) {
+      double q[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
+      if (a.contact_torque) {
+        // the capsule torque recast into the material frame: Q tau
+        const double* __restrict__ ct = a.contact_torque;
+        Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
+      }
+      if (a.joint_torque) {
+        // the connections' torque (summed in the lab frame), recast the same way
+        const double* __restrict__ jt = a.joint_torque;
+        Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
+      }
     }
     if (hits & kHitTorque) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
+      double q[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
       Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
     }
     if (kStoredJinv) {
@@ -377,9 +402,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     w = D3{0.0, 0.0, 0.0};
   }
   if (hits & kHitDamper) {
+    const RodInfo& ri = a.rods[meta >> kRodShift];
     // exp(-nu_t dt) for a damper time of dt; another damper time (PEFRL's
     // fractional kicks) scales the exponent
     const double ddt = a.damper_time;
+    double damper_t = ri.damper_t;
     if (ddt != a.dt) damper_t = exp(log(damper_t) * (ddt / a.dt));
     v = {v.x * damper_t, v.y * damper_t, v.z * damper_t};
     if (meta & kElem) {
@@ -391,7 +418,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       double em = 0.5 * (m + mn);
       if (meta & kFirst) em += 0.5 * m;
       if (meta & kLastElem) em += 0.5 * mn;
-      const double nur = damper_r;
+      const double nur = ri.damper_r;
 #ifdef EB_FAST_FP64
       w = {w.x * exp(e * (-nur * em * jinv.x * ddt)), w.y * exp(e * (-nur * em * jinv.y * ddt)),
            w.z * exp(e * (-nur * em * jinv.z * ddt))};
@@ -404,11 +431,16 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 
   // ---- second kinematic half step and store
   const double hdt2 = a.drift_post;
-  x = {x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z};
   double* __restrict__ out = a.out;
-  st3(out + kStX * S, S, g, x);
+  {
+    const D3 x = R.get3(rX, s);
+    st3(out + kStX * S, S, g, D3{x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z});
+  }
   st3(out + kStV * S, S, g, v);
   if (meta & kElem) {
+    double q[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
     so3(q, hdt2 * w.x, hdt2 * w.y, hdt2 * w.z);
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[(kStQ + k) * S + g] = q[k];

@@ -42,7 +42,10 @@ def test_velocity_verlet_parity_with_oracle(eb, W, kw):
     sim = wl.build(stepper=eb.VelocityVerlet(), **kw)
     t = sim.step(eb.VelocityVerlet(), 0.0, wl.dt, steps)
     assert t == pytest.approx(steps * wl.dt, rel=1e-12)
-    assert sim.step_plan()["mode"] == kw["step_mode"]
+    # rods of more than 519 elements fit no whole-batch resident
+    # configuration: a resident request then runs the per-size-bucket plan
+    want_mode = {"resident": ("resident", "bucketed")}.get(kw["step_mode"], (kw["step_mode"],))
+    assert sim.step_plan()["mode"] in want_mode
     want = state_slots(base)
     for name, place in (("Position", 0), ("Velocity", 0), ("Director", 1), ("AngularVelocity", 1)):
         err = max_rel_error_per_rod(sim.get_slots(name), want[name], wl.n_elements, place)
