@@ -691,8 +691,7 @@ def main(argv=None) -> int:
     alg = algorithmic_bytes(wl.n_elements, damped=False)
     per_launch_s = (ms / 1e3) / args.steps
     achieved = alg / per_launch_s / 1e9
-    traffic, traffic_note = profile_traffic("rod_step_fp64", wl.name,
-                                            ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh", "eb_internal.h"))
+    traffic, traffic_note = profile_traffic("rod_step_fp64", wl.name, ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh"))
 
     # ---- end to end through the public API with host buffers: each cycle
     # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE

@@ -33,8 +33,9 @@
 //   the damper factors exp(x) from their Taylor series for |x| < 0.01
 // The reference's 1e-14 guards (in the rotation axis and in sin(theta +
 // 1e-14)) are dropped: each moves a director by ~1e-14 per step, far below
-// this path's tolerance.  theta / sin(theta) comes from its series
-// 1 + y/3 + 2y^2/15 in y = 1 - cos(theta) below y = 1e-3.  The second half
+// this path's tolerance.  theta / sin(theta) comes from its series in
+// y = 1 - cos(theta) through y^7 below y = 0.25 (relative rotations up to
+// 0.72 rad a Voronoi point; truncation below 2e-8).  The second half
 // drift of a step and the first half drift of the next use the same velocity
 // and angular velocity and are applied as one full drift.
 //
@@ -412,9 +413,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 #pragma unroll
           for (int k = 0; k < 9; ++k) sq += dd[k] * dd[k];
           const float y = 0.25f * sq + 1e-10f;
-          float ratio;  // theta / sin(theta)
-          if (y < 1e-3f) {
-            ratio = 1.f + y * (1.f / 3.f + y * (2.f / 15.f));
+          float ratio;  // theta / sin(theta), theta = acos(1 - y)
+          if (y < 0.25f) {
+            // its Taylor series in y = 1 - cos(theta) through y^7 (the
+            // first omitted term is below 2e-8 for y < 0.25, under FP32's
+            // rounding), which covers relative rotations up to 0.72 rad a
+            // Voronoi point without the arcsine
+            ratio = 1.f + y * (1.f / 3.f + y * (2.f / 15.f + y * (2.f / 35.f + y * (8.f / 315.f +
+                    y * (8.f / 693.f + y * (16.f / 3003.f + y * (16.f / 6435.f)))))));
           } else {
             ratio = 2.f * asinf(sqrtf(0.5f * y)) * rsqrtf(y * (2.f - y));
           }

@@ -173,9 +173,17 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const bool valid = g >= 0 && g < a.n_slots;
   const uint32_t meta = valid ? a.meta[g] : 0u;
   // per-rod constraint data, fetched while the bulk copies are in flight:
-  // the slot's hits (which clamp holds it, the torque, the damper)
+  // the slot's hits (which clamp holds it, the torque, the damper) and the
+  // damper's constants (read in phase 4; loaded here, their latency hides
+  // behind the copies)
   uint32_t hits = 0;
-  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) hits = slot_hits(a.rods[meta >> kRodShift], g);
+  double damper_t = 1.0, damper_r = 0.0;
+  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
+    const RodInfo& ri = a.rods[meta >> kRodShift];
+    hits = slot_hits(ri, g);
+    damper_t = ri.damper_t;
+    damper_r = ri.damper_r;
+  }
 
   // ---- stage the window's inputs with bulk copies
   if (s == 0) {
@@ -402,11 +410,9 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     w = D3{0.0, 0.0, 0.0};
   }
   if (hits & kHitDamper) {
-    const RodInfo& ri = a.rods[meta >> kRodShift];
     // exp(-nu_t dt) for a damper time of dt; another damper time (PEFRL's
     // fractional kicks) scales the exponent
     const double ddt = a.damper_time;
-    double damper_t = ri.damper_t;
     if (ddt != a.dt) damper_t = exp(log(damper_t) * (ddt / a.dt));
     v = {v.x * damper_t, v.y * damper_t, v.z * damper_t};
     if (meta & kElem) {
@@ -418,7 +424,7 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       double em = 0.5 * (m + mn);
       if (meta & kFirst) em += 0.5 * m;
       if (meta & kLastElem) em += 0.5 * mn;
-      const double nur = ri.damper_r;
+      const double nur = damper_r;
 #ifdef EB_FAST_FP64
       w = {w.x * exp(e * (-nur * em * jinv.x * ddt)), w.y * exp(e * (-nur * em * jinv.y * ddt)),
            w.z * exp(e * (-nur * em * jinv.z * ddt))};

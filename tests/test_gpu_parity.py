@@ -290,11 +290,16 @@ def test_full_size_uneven_batch_sampled_parity(step_mode):
     orc, spread = B.oracle_spread(sub, 1000)
     bounds = B.parity_bounds(spread)
     offs = sim.slot_offsets()
+    margins = {}
     for name, key, place in B.STATE_FIELDS:
         full = sim.get_slots(name)
         got = np.concatenate([full[:, offs[k]:offs[k + 1]] for k in pick], axis=1)
         err = B.max_rel_error_per_rod(got, orc.comp(key), sub.n_elements, place)
+        # the margin: the error against the oracle's own one-ulp envelope
+        margins[name] = {"error": err, "envelope": spread[name], "ratio": err / spread[name] if spread[name] else None,
+                         "bound": bounds[name]}
         assert err <= bounds[name], (name, err, bounds[name])
+    print(f"full-size parity margins ({step_mode}): {margins}")
 
 
 def test_step_planner_times_every_candidate():
