@@ -110,15 +110,14 @@ __host__ __device__ __forceinline__ bool clamp_position(const RodInfo& ri, int64
   return true;
 }
 
+// (every field is read up front and the test is branch free, so the loads
+// go out together)
 __host__ __device__ __forceinline__ uint32_t slot_hits(const RodInfo& ri, int64_t g) {
-  uint32_t h = 0;
-  if (ri.flags & kRodClamp) {
-    if (g == ri.clamp_slot[0]) h |= kHitClamp0;
-    if (g == ri.clamp_slot[1]) h |= kHitClamp1;
-  }
-  if ((ri.flags & kRodEndTorque) && g == ri.torque_slot) h |= kHitTorque;
-  if (ri.flags & kRodDamper) h |= kHitDamper;
-  return h;
+  const uint32_t fl = ri.flags;
+  const int64_t c0 = ri.clamp_slot[0], c1 = ri.clamp_slot[1], ts = ri.torque_slot;
+  const bool clamp = (fl & kRodClamp) != 0;
+  return ((clamp & (g == c0)) ? kHitClamp0 : 0u) | ((clamp & (g == c1)) ? kHitClamp1 : 0u) |
+         ((((fl & kRodEndTorque) != 0) & (g == ts)) ? kHitTorque : 0u) | ((fl & kRodDamper) ? kHitDamper : 0u);
 }
 
 struct StepArgs {

@@ -117,16 +117,6 @@ __device__ __forceinline__ D3 curvature(const double qc[9], const double qn[9], 
 #endif
 }
 
-// a / d for three numerators (the fast build forms one reciprocal)
-__device__ __forceinline__ D3 div3(D3 a, double d) {
-#ifdef EB_FAST_FP64
-  const double r = 1.0 / d;
-  return {a.x * r, a.y * r, a.z * r};
-#else
-  return divide(a, d);
-#endif
-}
-
 // the clamp's value constraint on a slot a clamp holds: the node's position
 // and, where the slot holds an element, its directors
 __device__ __forceinline__ void clamp_value(const RodInfo& ri, uint32_t hits, uint32_t meta, D3& x, double q[9]) {
@@ -264,23 +254,33 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       const D3 x = R.get3(rX, s);
       const D3 dx = R.get3(rX, s + 1) - x;
       l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
-      t = div3(dx, l);
       l0 = R.at(rL0, s);
       e = l / l0;
+#ifdef EB_FAST_FP64
+      // one reciprocal each of l and e; the dilatation rate (t . dv) / (e l0)
+      // as (t . dv) / l (e l0 = l)
+      const double il = 1.0 / l, ie = 1.0 / e;
+      t = scale(dx, il);
+#else
+      t = divide(dx, l);
+#endif
       const D3 qt = matvec(q, t);
       sigma = {qt.x * e, qt.y * e, qt.z * e - 1.0};
       const D3 d = sigma - R.get3(rSig0, s);
       const D3 sh = R.get3(rShear, s);
       nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
-      f = div3(mattranspvec(q, nl), e);
       const D3 w = R.get3(rW, s);
       const D3 J = R.get3(rJ, s);
-      const D3 jwe = div3(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
       const D3 dv = R.get3(rV, s + 1) - R.get3(rV, s);
-      const double rate = dot(t, dv) / (e * l0);
 #ifdef EB_FAST_FP64
+      f = scale(mattranspvec(q, nl), ie);
+      const D3 jwe = scale(D3{J.x * w.x, J.y * w.y, J.z * w.z}, ie);
+      const double rate = dot(t, dv) * il;
       t_loc = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
 #else
+      f = divide(mattranspvec(q, nl), e);
+      const D3 jwe = divide(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
+      const double rate = dot(t, dv) / (e * l0);
       t_shear = scale(cross(qt, nl), l0);
       t_lag = cross(jwe, w);
       t_unst = scale(jwe, rate);
@@ -308,7 +308,12 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       kappa = curvature(q, qn, D0);
       const double D = 0.5 * (l + R.at(rL, s + 1));
       eps = D / D0;
+#ifdef EB_FAST_FP64
+      const double ie = D0 / D;  // 1 / eps
+      const double ic = ie * ie * ie;
+#else
       const double ic = 1.0 / (eps * eps * eps);
+#endif
       const D3 dk = kappa - R.get3(rKap0, s);
       const D3 B = R.get3(rBend, s);
       tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
@@ -561,7 +566,7 @@ cudaError_t launch_check_inverse_inertia(int64_t stride, int64_t n_slots, const 
 #endif
 
 // window: slots per CTA: 0 (128-slot windows, six CTAs an SM), 128 (five
-// CTAs an SM) or 256
+// CTAs an SM) or 256 (three CTAs an SM)
 cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream) {
   if (args.n_slots <= 0) return cudaSuccess;
   // every field row of a window must start on a 16-byte boundary
@@ -570,7 +575,7 @@ cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int w
     return cudaErrorMisalignedAddress;
   if (window == 0) return launch_window<128, 6>(args, diag, damped, stream);
   if (window == 128) return launch_window<128, 5>(args, diag, damped, stream);
-  return launch_window<256, 2>(args, diag, damped, stream);
+  return launch_window<256, 3>(args, diag, damped, stream);
 }
 
 }  // namespace eb
