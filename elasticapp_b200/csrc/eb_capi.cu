@@ -25,8 +25,6 @@
 
 namespace eb {
 cudaError_t launch_rod_step_fp64(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream);
-cudaError_t launch_check_inverse_inertia(int64_t stride, int64_t n_slots, const double* par, const uint32_t* meta,
-                                         uint32_t* mismatch, cudaStream_t stream);
 cudaError_t launch_rod_step_fp64_reference(const StepArgs& args, bool diag, bool damped, int window,
                                            cudaStream_t stream);
 int block_config_count();
@@ -190,12 +188,6 @@ struct eb_sim {
   int64_t* d_offsets = nullptr;
   double* d_energy = nullptr;
   uint32_t* d_status = nullptr;
-  // the streaming kernel forms 1 / J unless a stored J^-1 differs from it
-  // (a caller set J or J^-1 after the initializer): then it reads the stored
-  // rows.  jinv_dirty: J or J^-1 changed on the device since the last check
-  bool stored_jinv = false;
-  bool jinv_dirty = false;
-  uint32_t* d_jinv_flag = nullptr;
   uint32_t max_polls = 0;  // bounded-wait polls of the streaming kernel (0: built in)
   int cur = 0;
   double damper_dt = -1.0;
@@ -416,8 +408,6 @@ void host_free(eb_sim* s) {
   if (s->d_energy) cudaFree(s->d_energy);
   if (s->d_status) cudaFree(s->d_status);
   s->d_status = nullptr;
-  if (s->d_jinv_flag) cudaFree(s->d_jinv_flag);
-  s->d_jinv_flag = nullptr;
   {
     std::vector<void*> owned;
     for (auto* p : s->d_cta_start) owned.push_back(p);
@@ -771,7 +761,6 @@ EB_API eb_status eb_set_field(eb_sim* s, int64_t rod, int32_t field, const doubl
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, *fi);
   if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
-  if (fi->kind == kParam && (fi->offset == eb::kJ || fi->offset == eb::kJinv)) s->jinv_dirty = true;
   EB_CUDA(cudaMemcpy2DAsync(base + s->offsets[rod], s->stride * sizeof(double), values,
                             per * sizeof(double), per * sizeof(double), fi->ncomp,
                             cudaMemcpyHostToDevice, s->stream));
@@ -824,7 +813,6 @@ static eb_status batch_copy(eb_sim* s, int32_t field, int32_t layout, double* ho
   if (eb_status st = set_device(s)) return st;
   double* base = device_base(s, fi);
   if (!base) return fail(EB_ERR_UNSUPPORTED, "derived fields need EB_FLAG_RECORD_DIAGNOSTICS");
-  if (to_device && fi.kind == kParam && (fi.offset == eb::kJ || fi.offset == eb::kJinv)) s->jinv_dirty = true;
   const size_t pitch = static_cast<size_t>(s->stride) * sizeof(double);
   if (layout == EB_LAYOUT_SLOTS) {
     if (count != fi.ncomp * s->n_slots)
@@ -1130,17 +1118,9 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   std::vector<double> hd;
   if (want_diag) hd.assign(static_cast<size_t>(eb::kDiagFields * S), 0.0);
   std::vector<uint32_t> meta(static_cast<size_t>(S), 0u);
-  s->stored_jinv = false;
-  s->jinv_dirty = false;
   for (int64_t r = 0; r < nr; ++r) {
     const RodHost& R = s->rods[r];
     const int64_t W = R.n + 1, o = s->offsets[r];
-    for (int d = 0; d < 3 && !s->stored_jinv; ++d)
-      for (int64_t i = 0; i < R.n; ++i)
-        if (R.param[static_cast<size_t>((eb::kJinv + d) * W + i)] != 1.0 / R.param[static_cast<size_t>((eb::kJ + d) * W + i)]) {
-          s->stored_jinv = true;
-          break;
-        }
     for (int f = 0; f < eb::kStateFields; ++f)
       std::memcpy(&hs[static_cast<size_t>(f * S + o)], &R.state[static_cast<size_t>(f * W)], W * sizeof(double));
     for (int f = 0; f < eb::kParamFields; ++f)
@@ -1171,7 +1151,6 @@ EB_API eb_status eb_finalize(eb_sim* s) {
   alloc(reinterpret_cast<void**>(&s->d_offsets), static_cast<size_t>(nr + 1) * sizeof(int64_t));
   alloc(reinterpret_cast<void**>(&s->d_energy), static_cast<size_t>(4 * nr) * sizeof(double));
   alloc(reinterpret_cast<void**>(&s->d_status), sizeof(uint32_t));
-  alloc(reinterpret_cast<void**>(&s->d_jinv_flag), sizeof(uint32_t));
   if (e != cudaSuccess) {
     host_free(s);
     return fail(e == cudaErrorMemoryAllocation ? EB_ERR_OUT_OF_MEMORY : EB_ERR_CUDA,
@@ -1222,7 +1201,6 @@ eb::StepArgs step_args(eb_sim* s, double dt) {
   for (int d = 0; d < 3; ++d) a.gravity[d] = s->gravity[d];
   a.sim_flags = s->sim_flags;
   a.status = s->d_status;
-  a.stored_jinv = s->stored_jinv ? 1u : 0u;
   a.max_polls = s->max_polls;
   return a;
 }
@@ -1250,22 +1228,6 @@ void drop_graphs(eb_sim* s) {
     }
 }
 
-// After J or J^-1 changed on the device: does every stored J^-1 still equal
-// 1.0 / J?  Captured graphs hold the kernel variant, so they are dropped
-// when the answer changes.
-eb_status check_inverse_inertia(eb_sim* s) {
-  if (!s->jinv_dirty) return EB_OK;
-  uint32_t mismatch = 0;
-  EB_CUDA(eb::launch_check_inverse_inertia(s->stride, s->n_slots, s->d_param, s->d_meta, s->d_jinv_flag,
-                                           s->stream));
-  EB_CUDA(cudaMemcpyAsync(&mismatch, s->d_jinv_flag, sizeof(mismatch), cudaMemcpyDeviceToHost, s->stream));
-  EB_CUDA(cudaStreamSynchronize(s->stream));
-  const bool stored = mismatch != 0;
-  if (stored != s->stored_jinv) drop_graphs(s);
-  s->stored_jinv = stored;
-  s->jinv_dirty = false;
-  return EB_OK;
-}
 
 cudaError_t launch_streaming(eb_sim* s, eb::StepArgs& a, bool rec) {
   a.diag = rec ? s->d_diag : nullptr;
@@ -2019,7 +1981,6 @@ EB_API eb_status eb_step(eb_sim* s, double* time, double dt, int64_t n_steps) {
   if (n_steps == 0) return EB_OK;
   if (eb_status st = set_device(s)) return st;
   if (eb_status st = damper_for_dt(s, dt)) return st;
-  if (eb_status st = check_inverse_inertia(s)) return st;
   {
     // plan at the first call; plan again when a call's launches would be
     // much longer than the ones the plan was timed at (a first call of a
@@ -2367,7 +2328,6 @@ EB_API eb_status eb_snapshot_load(eb_sim* s, const void* buffer, uint64_t bytes)
   EB_CUDA(cudaMemcpyAsync(s->d_rods, p, s->rods.size() * sizeof(eb::RodInfo), cudaMemcpyHostToDevice, s->stream));
   EB_CUDA(cudaStreamSynchronize(s->stream));
   s->damper_dt = -1.0;  // the damper factors are refreshed for the next step's dt
-  s->jinv_dirty = true;  // restored parameters: check J^-1 against 1 / J again
   return check_device_status(s);
 }
 

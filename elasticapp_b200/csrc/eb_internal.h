@@ -155,9 +155,6 @@ struct StepArgs {
   // node slot, torques per element slot; or nullptr without connections
   const double* joint_force;
   const double* joint_torque;
-  // streaming kernel: read the stored J^-1 rows (1) or form 1 / J (0; bit
-  // identical while every stored J^-1 equals 1.0 / J, which the host checks)
-  uint32_t stored_jinv;
   // bound on the polls of a bounded wait for bulk copies (0: the built-in
   // bound); a small value exercises the timeout path
   uint32_t max_polls;

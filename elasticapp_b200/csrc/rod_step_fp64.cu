@@ -29,9 +29,14 @@
 // mbarriers: the state and the node mass (all the first drift reads), then
 // the other parameters, which land while the drift's rotation updates run.
 // (Splitting the copies this way took the kernel from 9.97 to 10.9 G
-// element-steps/s; a finer split, one stage per phase, lost a third.)  The
-// 128-slot windows run 5 CTAs per SM (96 registers a thread, 40 KB of shared
-// memory a CTA).  Every field row of
+// element-steps/s; a finer split, one stage per phase, lost a third.)  Both
+// waits are bounded; the threads vote on them, and a CTA whose copies did
+// not land in time records it in the status word, waits for the copies it
+// issued and leaves.  The 128-slot windows run 5 CTAs per SM (96 registers a
+// thread, 40 KB of shared memory a CTA); a thread keeps its slot's state in
+// registers from phase to phase.  (Re-reading the slot from shared memory
+// instead, at 80 registers and six CTAs an SM with 1 / J formed from J,
+// measured 6% slower.)  Every field row of
 // a window is 16-byte aligned in global memory because windows start on an
 // even slot and every field array starts on a 256-byte boundary.  The values
 // exchanged between neighbouring threads (element lengths, Q^T n_L / e, the
@@ -48,22 +53,17 @@ namespace {
 
 // shared-memory row of every staged input field: the 18 state rows, then the
 // parameter rows the variant needs (nu_f/nu_t only for explicitly damped
-// rods, the volume only when diagnostics are recorded, the stored J^-1 only
-// when some stored J^-1 differs from 1 / J: otherwise 1 / J is formed, bit
-// identical to the stored value, which the initializer forms as 1.0 / J of
-// the same product)
-template <bool kDamped, bool kDiag, bool kStoredJinv>
+// rods, the volume only when diagnostics are recorded)
+template <bool kDamped, bool kDiag>
 struct RowMap {
-  static constexpr bool needed(int f) {
-    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol) ||
-             (!kStoredJinv && f >= kJinv && f < kJinv + 3));
-  }
   static constexpr int param(int f) {
-    int r = kStateFields;
-    for (int k = 0; k < f; ++k) r += needed(k) ? 1 : 0;
-    return r;
+    return kStateFields + f - ((!kDamped && f > kNuF) ? 1 : 0) - ((!kDamped && f > kNuT) ? 1 : 0) -
+           ((!kDiag && f > kVol) ? 1 : 0);
   }
-  static constexpr int rows() { return param(kParamFields); }
+  static constexpr bool needed(int f) {
+    return !((!kDamped && (f == kNuF || f == kNuT)) || (!kDiag && f == kVol));
+  }
+  static constexpr int rows() { return kStateFields + kParamFields - (kDamped ? 0 : 2) - (kDiag ? 0 : 1); }
 };
 
 constexpr uint32_t kMaxPolls = 1u << 22;
@@ -130,9 +130,9 @@ __device__ __forceinline__ void clamp_value(const RodInfo& ri, uint32_t hits, ui
   }
 }
 
-template <int W, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
+template <int W, bool kDiag, bool kDamped, bool kContact>
 __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem) {
-  using M = RowMap<kDamped, kDiag, kStoredJinv>;
+  using M = RowMap<kDamped, kDiag>;
   constexpr int kTile = W - 4;  // interior slots stored per CTA (even)
   constexpr int kLeftHalo = 2;  // window starts 2 slots left of the tile
   constexpr int kRows = M::rows();
@@ -142,16 +142,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   constexpr int rSig0 = M::param(kSig0), rKap0 = M::param(kKap0), rShear = M::param(kShear);
   constexpr int rBend = M::param(kBend), rJ = M::param(kJ), rJinv = M::param(kJinv);
   constexpr int rNuF = M::param(kNuF), rNuT = M::param(kNuT), rVol = M::param(kVol);
-  // Exchange rows, each over rows only the owning thread reads and has read
-  // earlier in the same phase: f and l (phase 2) over the shear-rigidity
-  // rows and the first rest-strain row, g and h (phase 3) over the
-  // rest-curvature and bend-rigidity rows.  The state rows keep the slot's
-  // drifted position and directors (written in phase 1) and its velocity and
-  // angular velocity for the whole launch, and the mass and inertia rows stay
-  // too, so a thread re-reads its own slot from shared memory in each phase
-  // instead of holding it in registers across the barriers (registers, not
-  // shared-memory bandwidth, bound how many windows an SM runs at once).
-  constexpr int rF = rShear, rL = rSig0, rG = rKap0, rH = rBend;
+  // exchange rows, each over rows only the owning thread reads:
+  //   f (written in phase 2) over the angular velocity rows (read in phase 1)
+  //   l (phase 2) over the first rest-strain row (read earlier in phase 2)
+  //   g, h (phase 3) over the inertia and shear rigidity rows (read in phase 2)
+  constexpr int rF = rW, rL = rSig0, rG = rJ, rH = rShear;
 
   const Rows<W> R{smem};
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kRows * W);
@@ -161,28 +156,15 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const int64_t g = g0 + s;
   const int64_t S = a.stride;
   const bool valid = g >= 0 && g < a.n_slots;
-  const uint32_t meta = valid ? a.meta[g] : 0u;
-  // per-rod constraint data, fetched while the bulk copies are in flight:
-  // the slot's hits (which clamp holds it, the torque, the damper) and the
-  // damper's constants (read in phase 4; loaded here, their latency hides
-  // behind the copies)
-  uint32_t hits = 0;
-  double damper_t = 1.0, damper_r = 0.0;
-  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
-    const RodInfo& ri = a.rods[meta >> kRodShift];
-    hits = slot_hits(ri, g);
-    damper_t = ri.damper_t;
-    damper_r = ri.damper_r;
-  }
-
-  // ---- stage the window's inputs with bulk copies
+  const bool interior = valid && s >= kLeftHalo && s < kLeftHalo + kTile;
+  // ---- stage the window's inputs with bulk copies, first thing: thread 0
+  // initialises the barriers and issues every copy before any load of its
+  // own (the slot data below depends on the metadata word, a round trip
+  // that would otherwise delay the copies)
   if (s == 0) {
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
     mbar_fence_init();
-  }
-  __syncthreads();
-  if (s == 0) {
     const int64_t lo = g0 < 0 ? 0 : g0;
     const int64_t hi = (g0 + W < S) ? g0 + W : S;
     const uint32_t bytes = static_cast<uint32_t>((hi - lo) * sizeof(double));
@@ -198,28 +180,47 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     for (int f = 0; f < kParamFields; ++f)
       if (M::needed(f) && f != kMass) bulk_g2s(R.row(M::param(f)) + off, a.par + f * S + lo, bytes, bar + 1);
   }
+  // the barriers are initialised before any thread tests them
+  __syncthreads();
+
+  const uint32_t meta = valid ? a.meta[g] : 0u;
+  // per-rod constraint data, fetched while the bulk copies are in flight:
+  // the slot's hits (which clamp holds it, the torque, the damper) and the
+  // damper's constants
+  uint32_t hits = 0;
+  double damper_t = 1.0, damper_r = 0.0;
+  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
+    const RodInfo& ri = a.rods[meta >> kRodShift];
+    hits = slot_hits(ri, g);
+    damper_t = ri.damper_t;
+    damper_r = ri.damper_r;
+  }
   const bool ok0 = wait_copies(a, bar);
 
+  const double hdt = a.drift_pre;
+
   // ---- phase 1: first kinematic half step and clamp value constraint,
-  // in place in shared memory (the velocity rows are left as they are)
+  // in place in shared memory
+  D3 x{0.0, 0.0, 0.0}, v{0.0, 0.0, 0.0}, w{0.0, 0.0, 0.0};
+  double q[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) q[k] = 0.0;
+  double m = 1.0;
   if (ok0 && valid) {
-    const double hdt = a.drift_pre;
-    const D3 v = R.get3(rV, s);
+    v = R.get3(rV, s);
     const D3 x0 = R.get3(rX, s);
-    D3 x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
-    double q[9];
+    x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
+    m = R.at(rMass, s);
     if (meta & kElem) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
-      const D3 w = R.get3(rW, s);
+      w = R.get3(rW, s);
       so3(q, hdt * w.x, hdt * w.y, hdt * w.z);
     }
     if (hits & (kHitClamp0 | kHitClamp1)) clamp_value(a.rods[meta >> kRodShift], hits, meta, x, q);
     R.put3(rX, s, x);
-    if (meta & kElem) {
 #pragma unroll
-      for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
-    }
+    for (int k = 0; k < 9; ++k) R.at(rQ + k, s) = q[k];
   }
   const bool ok1 = ok0 && wait_copies(a, bar + 1);
   if (!__syncthreads_and(ok1)) {
@@ -240,18 +241,10 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const bool elem = (meta & kElem) && s + 1 < W;
   double l = 1.0, e = 1.0, l0 = 1.0;
   D3 t{0.0, 0.0, 0.0}, sigma{0.0, 0.0, 0.0}, nl{0.0, 0.0, 0.0};
-#ifdef EB_FAST_FP64
-  D3 t_loc{0.0, 0.0, 0.0};  // shear + transport + dilatation terms, summed here
-#else
   D3 t_shear{0.0, 0.0, 0.0}, t_lag{0.0, 0.0, 0.0}, t_unst{0.0, 0.0, 0.0};
-#endif
   {
     D3 f{0.0, 0.0, 0.0};
     if (elem) {
-      double q[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
-      const D3 x = R.get3(rX, s);
       const D3 dx = R.get3(rX, s + 1) - x;
       l = sqrt(dx.x * dx.x + dx.y * dx.y + dx.z * dx.z);
       l0 = R.at(rL0, s);
@@ -269,22 +262,20 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
       const D3 d = sigma - R.get3(rSig0, s);
       const D3 sh = R.get3(rShear, s);
       nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
-      const D3 w = R.get3(rW, s);
+      t_shear = scale(cross(qt, nl), l0);
       const D3 J = R.get3(rJ, s);
-      const D3 dv = R.get3(rV, s + 1) - R.get3(rV, s);
+      const D3 dv = R.get3(rV, s + 1) - v;
 #ifdef EB_FAST_FP64
       f = scale(mattranspvec(q, nl), ie);
       const D3 jwe = scale(D3{J.x * w.x, J.y * w.y, J.z * w.z}, ie);
       const double rate = dot(t, dv) * il;
-      t_loc = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
 #else
       f = divide(mattranspvec(q, nl), e);
       const D3 jwe = divide(D3{J.x * w.x, J.y * w.y, J.z * w.z}, e);
       const double rate = dot(t, dv) / (e * l0);
-      t_shear = scale(cross(qt, nl), l0);
+#endif
       t_lag = cross(jwe, w);
       t_unst = scale(jwe, rate);
-#endif
     }
     R.at(rL, s) = l;
     R.put3(rF, s, f);
@@ -298,12 +289,9 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   {
     D3 gg{0.0, 0.0, 0.0}, hh{0.0, 0.0, 0.0};
     if ((meta & kVor) && s + 1 < W) {
-      double q[9], qn[9];
+      double qn[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        q[k] = R.at(rQ + k, s);
-        qn[k] = R.at(rQ + k, s + 1);
-      }
+      for (int k = 0; k < 9; ++k) qn[k] = R.at(rQ + k, s + 1);
       const double D0 = R.at(rD0, s);
       kappa = curvature(q, qn, D0);
       const double D = 0.5 * (l + R.at(rL, s + 1));
@@ -325,11 +313,9 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
   __syncthreads();
 
-  if (!(valid && s >= kLeftHalo && s < kLeftHalo + kTile)) return;  // halo: computed, not stored
+  if (!interior) return;
 
   // ---- phase 4: loads, update_acceleration (WithRodKinematics.hpp:684-714)
-  const double m = R.at(rMass, s);
-  D3 v = R.get3(rV, s);
   D3 F = R.get3(rF, s) - R.get3(rF, s - 1);
   if (kDamped) {
     const double c = m * R.at(rNuF, s);
@@ -356,53 +342,34 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 
   D3 T{0.0, 0.0, 0.0}, alpha{0.0, 0.0, 0.0};
   D3 jinv{0.0, 0.0, 0.0};
-  D3 w{0.0, 0.0, 0.0};
   if (meta & kElem) {
-    w = R.get3(rW, s);
     T = R.get3(rG, s) - R.get3(rG, s - 1);                // two-point difference of g
     const D3 h1 = R.get3(rH, s), h0 = R.get3(rH, s - 1);  // quadrature of h
     T = T + D3{0.5 * (h1.x + h0.x), 0.5 * (h1.y + h0.y), 0.5 * (h1.z + h0.z)};
-#ifdef EB_FAST_FP64
-    T = T + t_loc;
-#else
     T = T + t_shear;
     T = T + t_lag;
     T = T + t_unst;
-#endif
     if (kDamped) {
       const double em = 0.5 * (m + R.at(rMass, s + 1));
       const double c = em * R.at(rNuT, s);
       T = {T.x - c * w.x, T.y - c * w.y, T.z - c * w.z};
     }
     D3 Te{0.0, 0.0, 0.0};
-    if (kContact && (a.contact_torque || a.joint_torque)) {
-      double q[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
-      if (a.contact_torque) {
-        // the capsule torque recast into the material frame: Q tau
-        const double* __restrict__ ct = a.contact_torque;
-        Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
-      }
-      if (a.joint_torque) {
-        // the connections' torque (summed in the lab frame), recast the same way
-        const double* __restrict__ jt = a.joint_torque;
-        Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
-      }
+    if (kContact && a.contact_torque) {
+      // the capsule torque recast into the material frame: Q tau
+      const double* __restrict__ ct = a.contact_torque;
+      Te = Te + matvec(q, D3{ct[g], ct[S + g], ct[2 * S + g]});
+    }
+    if (kContact && a.joint_torque) {
+      // the connections' torque (summed in the lab frame), recast the same way
+      const double* __restrict__ jt = a.joint_torque;
+      Te = Te + matvec(q, D3{jt[g], jt[S + g], jt[2 * S + g]});
     }
     if (hits & kHitTorque) {
       const RodInfo& ri = a.rods[meta >> kRodShift];
-      double q[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
       Te = Te + matvec(q, D3{ri.end_torque[0], ri.end_torque[1], ri.end_torque[2]});
     }
-    if (kStoredJinv) {
-      jinv = R.get3(rJinv, s);
-    } else {
-      const D3 J = R.get3(rJ, s);
-      jinv = {1.0 / J.x, 1.0 / J.y, 1.0 / J.z};
-    }
+    jinv = R.get3(rJinv, s);
     alpha = {(jinv.x * (T.x + Te.x)) * e, (jinv.y * (T.y + Te.y)) * e, (jinv.z * (T.z + Te.z)) * e};
   }
 
@@ -442,16 +409,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 
   // ---- second kinematic half step and store
   const double hdt2 = a.drift_post;
+  x = {x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z};
   double* __restrict__ out = a.out;
-  {
-    const D3 x = R.get3(rX, s);
-    st3(out + kStX * S, S, g, D3{x.x + hdt2 * v.x, x.y + hdt2 * v.y, x.z + hdt2 * v.z});
-  }
+  st3(out + kStX * S, S, g, x);
   st3(out + kStV * S, S, g, v);
   if (meta & kElem) {
-    double q[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
     so3(q, hdt2 * w.x, hdt2 * w.y, hdt2 * w.z);
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[(kStQ + k) * S + g] = q[k];
@@ -480,17 +442,17 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   }
 }
 
-template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
+template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
 __global__ void __launch_bounds__(W, MinBlocks) rod_step_fp64_kernel(const StepArgs a) {
   extern __shared__ __align__(128) double smem[];
-  rod_step_window<W, kDiag, kDamped, kContact, kStoredJinv>(a, smem);
+  rod_step_window<W, kDiag, kDamped, kContact>(a, smem);
 }
 
-template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact, bool kStoredJinv>
+template <int W, int MinBlocks, bool kDiag, bool kDamped, bool kContact>
 cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   constexpr int kTile = W - 4;
-  constexpr size_t bytes = size_t(RowMap<kDamped, kDiag, kStoredJinv>::rows()) * W * sizeof(double) + 16;
-  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped, kContact, kStoredJinv>;
+  constexpr size_t bytes = size_t(RowMap<kDamped, kDiag>::rows()) * W * sizeof(double) + 16;
+  auto kern = rod_step_fp64_kernel<W, MinBlocks, kDiag, kDamped, kContact>;
   // the attribute is per device; setting it on every launch is cheap and
   // keeps multi-device use correct
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -500,19 +462,13 @@ cudaError_t launch_variant(const StepArgs& args, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-template <int W, int MinBlocks, bool kContact, bool kStoredJinv>
-cudaError_t launch_window_j(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  if (diag)
-    return damped ? launch_variant<W, MinBlocks, true, true, kContact, kStoredJinv>(args, stream)
-                  : launch_variant<W, MinBlocks, true, false, kContact, kStoredJinv>(args, stream);
-  return damped ? launch_variant<W, MinBlocks, false, true, kContact, kStoredJinv>(args, stream)
-                : launch_variant<W, MinBlocks, false, false, kContact, kStoredJinv>(args, stream);
-}
-
 template <int W, int MinBlocks, bool kContact>
 cudaError_t launch_window_c(const StepArgs& args, bool diag, bool damped, cudaStream_t stream) {
-  return args.stored_jinv ? launch_window_j<W, MinBlocks, kContact, true>(args, diag, damped, stream)
-                          : launch_window_j<W, MinBlocks, kContact, false>(args, diag, damped, stream);
+  if (diag)
+    return damped ? launch_variant<W, MinBlocks, true, true, kContact>(args, stream)
+                  : launch_variant<W, MinBlocks, true, false, kContact>(args, stream);
+  return damped ? launch_variant<W, MinBlocks, false, true, kContact>(args, stream)
+                : launch_variant<W, MinBlocks, false, false, kContact>(args, stream);
 }
 
 template <int W, int MinBlocks>
@@ -536,46 +492,20 @@ cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStre
 // matches the reference's short-horizon golden vectors at its own tolerance.
 #ifdef EB_FAST_FP64
 #define EB_FP64_LAUNCHER launch_rod_step_fp64
-
-namespace {
-// *mismatch |= 1 if any element slot's stored J^-1 differs from 1.0 / J
-__global__ void check_inverse_inertia_kernel(int64_t stride, int64_t n_slots, const double* __restrict__ par,
-                                             const uint32_t* __restrict__ meta, uint32_t* mismatch) {
-  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_slots;
-       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (!(meta[g] & kElem)) continue;
-    bool bad = false;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) bad |= par[(kJinv + d) * stride + g] != 1.0 / par[(kJ + d) * stride + g];
-    if (bad) atomicOr(mismatch, 1u);
-  }
-}
-}  // namespace
-
-cudaError_t launch_check_inverse_inertia(int64_t stride, int64_t n_slots, const double* par, const uint32_t* meta,
-                                         uint32_t* mismatch, cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(mismatch, 0, sizeof(uint32_t), stream);
-  if (e != cudaSuccess || n_slots <= 0) return e;
-  const int64_t blocks = (n_slots + 255) / 256;
-  check_inverse_inertia_kernel<<<static_cast<unsigned>(blocks < 4096 ? blocks : 4096), 256, 0, stream>>>(
-      stride, n_slots, par, meta, mismatch);
-  return cudaGetLastError();
-}
 #else
 #define EB_FP64_LAUNCHER launch_rod_step_fp64_reference
 #endif
 
-// window: slots per CTA: 0 (128-slot windows, six CTAs an SM), 128 (five
-// CTAs an SM) or 256 (three CTAs an SM)
+// window: slots per CTA: 0 or 128 (the default: 128-slot windows, five CTAs
+// an SM) or 256 (two CTAs an SM)
 cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream) {
   if (args.n_slots <= 0) return cudaSuccess;
   // every field row of a window must start on a 16-byte boundary
   if ((args.stride & 1) || (reinterpret_cast<uintptr_t>(args.in) & 15) ||
       (reinterpret_cast<uintptr_t>(args.par) & 15))
     return cudaErrorMisalignedAddress;
-  if (window == 0) return launch_window<128, 6>(args, diag, damped, stream);
-  if (window == 128) return launch_window<128, 5>(args, diag, damped, stream);
-  return launch_window<256, 3>(args, diag, damped, stream);
+  if (window == 256) return launch_window<256, 2>(args, diag, damped, stream);
+  return launch_window<128, 5>(args, diag, damped, stream);
 }
 
 }  // namespace eb

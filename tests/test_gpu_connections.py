@@ -88,3 +88,36 @@ def test_connect_argument_checks():
         sim.connect(a, 0).to(b, 0).using(eb.FreeJoint(1.0))
     assert e.value.status == 2  # after finalize
     sim.close()
+
+
+@pytest.mark.parametrize("joint", ["free", "hinge"])
+def test_joint_keeps_total_momentum_on_gpu(joint):
+    """A pin of the joint rules that needs no reference value: the joint
+    force acts equal and opposite on its two nodes (and the hinge torques
+    are internal too), so two free, unloaded rods joined by a stretched
+    joint keep their total linear momentum to rounding, while the joint
+    moves them (the gap changes)."""
+    import elasticapp_b200 as eb
+    from test_oracle_connections import two_free_rods
+    from elasticapp_b200.simulator import FreeJoint, HingeJoint
+
+    rng = np.random.default_rng(7)
+    v = [rng.normal(0, 1e-2, (3, 9)), rng.normal(0, 1e-2, (3, 9))]
+    j = FreeJoint(1e3, 0.0) if joint == "free" else HingeJoint(1e3, 0.0, 1e-3, (0.0, 0.0, 1.0))
+    wl = two_free_rods((0.01, 0.005, -0.002), j, v=v)
+    sim = wl.build()
+    m = np.concatenate([r.get("Mass") for r in sim.rods])
+
+    def momentum():
+        vel = np.concatenate([r.get("Velocity") for r in sim.rods], axis=1)
+        return (vel * m[None, :]).sum(axis=1)
+
+    p0 = momentum()
+    x0 = sim.rods[1].get("Position")[:, 0] - sim.rods[0].get("Position")[:, -1]
+    sim.step(eb.PositionVerlet(), 0.0, wl.dt, 2000)
+    p1 = momentum()
+    x1 = sim.rods[1].get("Position")[:, 0] - sim.rods[0].get("Position")[:, -1]
+    scale = np.abs(v[0]).max() * m.sum()
+    assert np.max(np.abs(p1 - p0)) <= 1e-12 * scale
+    assert np.linalg.norm(x1 - x0) > 1e-6  # the joint acted
+    sim.close()

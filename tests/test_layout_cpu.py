@@ -43,22 +43,21 @@ def test_rod_table_index_width():
     assert (1 << (32 - 5)) > 65536 * 1024
 
 
-def window_rows(damped, diag, stored_jinv):
+def window_rows(damped, diag):
     """Rows of a window's shared memory (RowMap): 18 state rows and every
     parameter row the variant reads."""
-    return 18 + 24 - (0 if damped else 2) - (0 if diag else 1) - (0 if stored_jinv else 3)
+    return 18 + 24 - (0 if damped else 2) - (0 if diag else 1)
 
 
-@pytest.mark.parametrize("W,per_sm", [(128, 6), (128, 5), (256, 2)])
+@pytest.mark.parametrize("W,per_sm", [(128, 5), (256, 2)])
 @pytest.mark.parametrize("damped", [False, True])
 @pytest.mark.parametrize("diag", [False, True])
-@pytest.mark.parametrize("stored", [False, True])
-def test_window_shared_memory(W, per_sm, damped, diag, stored):
+def test_window_shared_memory(W, per_sm, damped, diag):
     """Bytes of a window's rows plus its two mbarriers; the plain variant
-    (undamped, no diagnostics, J^-1 formed) fits the CTAs an SM its launch
-    bound asks for (228 KB an SM, 1 KB reserved a CTA)."""
-    total = window_rows(damped, diag, stored) * W * 8 + 16
+    (undamped, no diagnostics) fits the CTAs an SM its launch bound asks for
+    (228 KB an SM, 1 KB reserved a CTA)."""
+    total = window_rows(damped, diag) * W * 8 + 16
     assert (W * 8) % 16 == 0  # every row starts 16-byte aligned
     assert total <= 227 * 1024
-    if not (damped or diag or stored):
+    if not (damped or diag):
         assert per_sm * (total + 1024) <= 228 * 1024
