@@ -636,8 +636,9 @@ EB_API eb_status eb_sim_create(const eb_config* config, eb_sim** out) {
     return fail(EB_ERR_INVALID_ARGUMENT, "unknown precision");
   if (cfg.resident_config < 0 || cfg.resident_config > eb::block_config_count())
     return fail(EB_ERR_INVALID_ARGUMENT, "resident_config out of range");
-  if (cfg.step_window != 0 && cfg.step_window != 128 && cfg.step_window != 256)
-    return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 128 or 256");
+  if (cfg.step_window != 0 && cfg.step_window != 64 && cfg.step_window != 96 && cfg.step_window != 128 &&
+      cfg.step_window != 256)
+    return fail(EB_ERR_INVALID_ARGUMENT, "step_window must be 0 (default), 64, 96, 128 or 256");
   if (cfg.precision == EB_PRECISION_MIXED && (cfg.flags & (EB_FLAG_REFERENCE_ROUNDING | EB_FLAG_STEP_STREAMING)))
     return fail(EB_ERR_INVALID_ARGUMENT, "mixed precision runs on the resident kernels only");
   if (cfg.stepper != EB_STEPPER_POSITION_VERLET && cfg.stepper != EB_STEPPER_PEFRL &&

@@ -157,14 +157,28 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   const int64_t S = a.stride;
   const bool valid = g >= 0 && g < a.n_slots;
   const bool interior = valid && s >= kLeftHalo && s < kLeftHalo + kTile;
-  // ---- stage the window's inputs with bulk copies, first thing: thread 0
-  // initialises the barriers and issues every copy before any load of its
-  // own (the slot data below depends on the metadata word, a round trip
-  // that would otherwise delay the copies)
+  const uint32_t meta = valid ? a.meta[g] : 0u;
+  // per-rod constraint data, fetched while the bulk copies are in flight:
+  // the slot's hits (which clamp holds it, the torque, the damper) and the
+  // damper's constants
+  uint32_t hits = 0;
+  double damper_t = 1.0, damper_r = 0.0;
+  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
+    const RodInfo& ri = a.rods[meta >> kRodShift];
+    hits = slot_hits(ri, g);
+    damper_t = ri.damper_t;
+    damper_r = ri.damper_r;
+  }
+
+  // ---- stage the window's inputs with bulk copies (issuing them before the
+  // loads above, which wait on the metadata word, measured no faster)
   if (s == 0) {
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
     mbar_fence_init();
+  }
+  __syncthreads();
+  if (s == 0) {
     const int64_t lo = g0 < 0 ? 0 : g0;
     const int64_t hi = (g0 + W < S) ? g0 + W : S;
     const uint32_t bytes = static_cast<uint32_t>((hi - lo) * sizeof(double));
@@ -179,21 +193,6 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 #pragma unroll 1
     for (int f = 0; f < kParamFields; ++f)
       if (M::needed(f) && f != kMass) bulk_g2s(R.row(M::param(f)) + off, a.par + f * S + lo, bytes, bar + 1);
-  }
-  // the barriers are initialised before any thread tests them
-  __syncthreads();
-
-  const uint32_t meta = valid ? a.meta[g] : 0u;
-  // per-rod constraint data, fetched while the bulk copies are in flight:
-  // the slot's hits (which clamp holds it, the torque, the damper) and the
-  // damper's constants
-  uint32_t hits = 0;
-  double damper_t = 1.0, damper_r = 0.0;
-  if (valid && (a.sim_flags & (kSimClamp | kSimDamper | kSimEndTorque))) {
-    const RodInfo& ri = a.rods[meta >> kRodShift];
-    hits = slot_hits(ri, g);
-    damper_t = ri.damper_t;
-    damper_r = ri.damper_r;
   }
   const bool ok0 = wait_copies(a, bar);
 
@@ -497,7 +496,7 @@ cudaError_t launch_window(const StepArgs& args, bool diag, bool damped, cudaStre
 #endif
 
 // window: slots per CTA: 0 or 128 (the default: 128-slot windows, five CTAs
-// an SM) or 256 (two CTAs an SM)
+// an SM), 64 (ten), 96 (six) or 256 (two)
 cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int window, cudaStream_t stream) {
   if (args.n_slots <= 0) return cudaSuccess;
   // every field row of a window must start on a 16-byte boundary
@@ -505,6 +504,8 @@ cudaError_t EB_FP64_LAUNCHER(const StepArgs& args, bool diag, bool damped, int w
       (reinterpret_cast<uintptr_t>(args.par) & 15))
     return cudaErrorMisalignedAddress;
   if (window == 256) return launch_window<256, 2>(args, diag, damped, stream);
+  if (window == 96) return launch_window<96, 6>(args, diag, damped, stream);
+  if (window == 64) return launch_window<64, 10>(args, diag, damped, stream);
   return launch_window<128, 5>(args, diag, damped, stream);
 }
 

@@ -95,7 +95,7 @@ typedef struct eb_config {
   int32_t device;          /* CUDA device ordinal */
   int32_t precision;       /* eb_precision */
   uint32_t flags;          /* EB_FLAG_* */
-  int32_t step_window;     /* streaming kernel, slots per CTA: 0 (default) or 128, or 256 */
+  int32_t step_window;     /* streaming kernel, slots per CTA: 0 (default) or 128, or 64, 96, 256 */
   int32_t resident_config; /* 0: chosen by timing; c > 0: resident configuration c - 1 */
   int32_t stepper;         /* eb_stepper (0: PositionVerlet) */
 } eb_config;

@@ -19,7 +19,7 @@ def windows(n_slots, W):
         yield b, g0, lo, hi, S, T
 
 
-@pytest.mark.parametrize("W", [128, 256])
+@pytest.mark.parametrize("W", [64, 96, 128, 256])
 def test_window_copies_aligned_and_cover_every_slot(W):
     for n_slots in list(range(3, 2000, 7)) + [4458875, 10_517_000 + 3]:
         covered = 0
@@ -49,7 +49,7 @@ def window_rows(damped, diag):
     return 18 + 24 - (0 if damped else 2) - (0 if diag else 1)
 
 
-@pytest.mark.parametrize("W,per_sm", [(128, 5), (256, 2)])
+@pytest.mark.parametrize("W,per_sm", [(64, 10), (96, 6), (128, 5), (256, 2)])
 @pytest.mark.parametrize("damped", [False, True])
 @pytest.mark.parametrize("diag", [False, True])
 def test_window_shared_memory(W, per_sm, damped, diag):
