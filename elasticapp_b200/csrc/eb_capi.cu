@@ -1752,9 +1752,6 @@ eb::ContactArgs contact_args(eb_sim* s, double dt) {
   return a;
 }
 
-// Steps with the collision system, in chunks: the chunk's starting state is
-// kept, and a chunk whose candidate pairs overflowed the partner buffer is
-// run again from it with a larger buffer.
 // Streaming steps with external loads evaluated at every force evaluation's
 // drifted state: the collision system (in chunks of kContactChunk steps,
 // rerun with a larger pair buffer on overflow) and/or the connections.
@@ -1778,12 +1775,15 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
   while (done < n_steps) {
     const int64_t k = contact ? std::min<int64_t>(kContactChunk, n_steps - done) : n_steps - done;
     const int c0 = s->cur;
-    if (contact)
+    const Substep* sub;
+    const int ns = substeps(s, &sub);
+    // the chunk's starting state is kept for a rerun; a chunk of one launch
+    // leaves it untouched in the buffer the launch reads
+    const bool keep = contact && k * ns > 1;
+    if (keep)
       EB_CUDA(cudaMemcpyAsync(c.backup, s->d_state[c0], state_bytes, cudaMemcpyDeviceToDevice, s->stream));
     eb::ContactArgs ca{};
     if (contact) ca = contact_args(s, dt);
-    const Substep* sub;
-    const int ns = substeps(s, &sub);
     for (int64_t i = 0; i < k; ++i) {
       for (int j = 0; j < ns; ++j) {
         // one contact evaluation per force evaluation, at its drifted state
@@ -1831,7 +1831,8 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
       const uint32_t cleared = st & ~static_cast<uint32_t>(eb::kStatusPairOverflow);
       EB_CUDA(cudaMemcpyAsync(s->d_status, &cleared, sizeof(cleared), cudaMemcpyHostToDevice, s->stream));
       EB_CUDA(cudaMemsetAsync(c.required, 0, sizeof(unsigned long long), s->stream));
-      EB_CUDA(cudaMemcpyAsync(s->d_state[c0], c.backup, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+      if (keep)
+        EB_CUDA(cudaMemcpyAsync(s->d_state[c0], c.backup, state_bytes, cudaMemcpyDeviceToDevice, s->stream));
       EB_CUDA(cudaStreamSynchronize(s->stream));
       s->cur = c0;
       continue;
