@@ -14,8 +14,10 @@
 //   FP32: lengths, tangents, dilatations, constitutive products, internal
 //         loads and couples, accelerations, the damping factors.
 //
-// FP32 copies of the director and angular velocity are refreshed whenever
-// the FP64 values change, so each is converted once per step, and the
+// The element phase converts the FP64 director and angular velocity it has
+// loaded anyway to FP32 (FP32 shadow rows of both, refreshed whenever the
+// FP64 values changed, cost 12 shared-memory stores and 12 loads a slot and
+// step for the same values and 48 B of shared memory a slot), and the
 // divisions of the element math are reciprocal square roots and rounded
 // reciprocals (the reciprocals of the masses and Voronoi rest lengths are
 // formed each step rather than stored: shared memory per slot, not the
@@ -67,15 +69,14 @@ using F3 = Vec3<float>;
 enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dSig0 = 19, dRowsD = 22 };
 // shared-memory rows of FP32 values per slot
 template <bool kDamped>
-constexpr int mixed_rows_f() { return kDamped ? 44 : 42; }
+constexpr int mixed_rows_f() { return kDamped ? 32 : 30; }
 
 // FP32 rows
 enum MixedRowF : int {
   fMass = 0, fL0 = 1, fD0 = 2, fKap0 = 3, fShear = 6, fBend = 9, fJ = 12, fJinv = 15,
   fF = 18, fP = 21, fM = 24, fE = 27, fDampR = 28,
   fDampC = 29,  // 1 - exp(-nu_t dt) of the rod's analytical damper
-  fQ = 30, fW = 39,
-  fNuF = 42, fNuT = 43  // explicit damping only: the last rows, not allocated for undamped rods
+  fNuF = 30, fNuT = 31  // explicit damping only: the last rows, not allocated for undamped rods
 };
 
 template <int kCap>
@@ -137,7 +138,7 @@ __device__ __forceinline__ float exp_small(float x) {
   return expf(x);
 }
 
-// x += c v; Q <- exp(-c [w]x) Q for element slots; FP32 copy of Q refreshed
+// x += c v; Q <- exp(-c [w]x) Q for element slots
 template <int kCap>
 __device__ __forceinline__ void drift(const MRows<kCap>& R, int s, uint32_t meta, double c, D3 v, D3 w) {
   const D3 x = R.d3(dX, s);
@@ -148,10 +149,7 @@ __device__ __forceinline__ void drift(const MRows<kCap>& R, int s, uint32_t meta
     for (int k = 0; k < 9; ++k) q[k] = R.ad(dQ + k, s);
     so3_series(q, c * w.x, c * w.y, c * w.z);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      R.ad(dQ + k, s) = q[k];
-      R.af(fQ + k, s) = static_cast<float>(q[k]);
-    }
+    for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = q[k];
   }
 }
 
@@ -165,10 +163,7 @@ __device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, uint32_
   R.pd3(dX, s, D3{tx[0], tx[1], tx[2]});
   if (!(meta & kElem)) return;
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    R.ad(dQ + k, s) = tq[k];
-    R.af(fQ + k, s) = static_cast<float>(tq[k]);
-  }
+  for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = tq[k];
 }
 
 // Neighbour access for rod pairs: slot indices at or past `count` continue in
@@ -322,10 +317,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     R.af(fDampR, s) = dr;
 #pragma unroll 1
     for (int f = 0; f < kStateFields; ++f) R.ad(f, s) = a.in[f * S + g];
-#pragma unroll 1
-    for (int k = 0; k < 9; ++k) R.af(fQ + k, s) = static_cast<float>(R.ad(dQ + k, s));
-#pragma unroll 1
-    for (int k = 0; k < 3; ++k) R.af(fW + k, s) = static_cast<float>(R.ad(dW + k, s));
     const double il0 = 1.0 / a.par[kL0 * S + g];
     R.ad(dInvL0, s) = il0;
     // the rest strain, with the unit axial strain of sigma = Q dx / l0 - z folded in
@@ -388,10 +379,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const F3 nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
         float qf[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) qf[k] = R.af(fQ + k, s);
+        for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
         f = scale(mattranspvec(qf, nl), ie);
         const F3 qt = matvec(qf, t);
-        const F3 w = R.f3(fW, s);
+        const F3 w = tof(R.d3(dW, s));
         const F3 J = R.f3(fJ, s);
         const F3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
         const F3 dv = tof((kPair ? N.d3(dV, s + 1) : R.d3(dV, s + 1)) - R.d3(dV, s));
@@ -478,14 +469,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         if (!first) T = T - (kPair ? N.f3(fM, s - 1) : R.f3(fM, s - 1));
         if (kDamped) {
           const float ct = 0.5f * (m + (kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1))) * R.af(fNuT, s);
-          const F3 wf = R.f3(fW, s);
+          const F3 wf = tof(w);
           T = {T.x - ct * wf.x, T.y - ct * wf.y, T.z - ct * wf.z};
         }
         if (rf & kHitTorque) {
           const RodInfo& ri = a.rods[meta >> kRodShift];
           float qf[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) qf[k] = R.af(fQ + k, s);
+          for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
           T = T + matvec(qf, F3{static_cast<float>(ri.end_torque[0]), static_cast<float>(ri.end_torque[1]),
                                 static_cast<float>(ri.end_torque[2])});
         }
@@ -509,10 +500,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       }
       if (rf & kHitDamper) v = scale(v, 1.0 - static_cast<double>(R.af(fDampC, s)));
       R.pd3(dV, s, v);
-      if (meta & kElem) {
-        R.pd3(dW, s, w);
-        R.pf3(fW, s, tof(w));
-      }
+      if (meta & kElem) R.pd3(dW, s, w);
       drift(R, s, meta, last ? hdt : dt, v, w);
       if (clamped) clamp_value(R, s, meta, rf, a.rods[meta >> kRodShift]);
       if (last) {
@@ -590,8 +578,9 @@ cudaError_t launch_rod_block_mixed_pairs(const StepArgs& args, const int64_t* ct
 // Resident launches: CTA c owns the slots gmap[cta_start[c] .. cta_start[c +
 // 1]), whole rods (the host packs them best fit decreasing).  The same
 // configurations as the FP64 resident kernel (0/1: 520 slots, 2: 264, 3:
-// 320); 352 B of shared memory per slot (360 with explicit damping) allows
-// two CTAs per SM at 264 and 320 slots.
+// 320); 304 B of shared memory per slot (312 with explicit damping) allows
+// two CTAs per SM at 264 and 320 slots (two of 352 slots on 352 threads
+// measured 1% slower than 320 on the mixed batch).
 cudaError_t launch_rod_block_mixed_gather(const StepArgs& args, const int64_t* cta_start, const int32_t* gmap,
                                           int n_ctas, int n_steps, int config, bool damped, cudaStream_t stream) {
   if (n_ctas <= 0 || n_steps <= 0) return cudaSuccess;
