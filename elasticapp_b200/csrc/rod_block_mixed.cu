@@ -65,43 +65,66 @@ namespace {
 using D3 = Vec3<double>;
 using F3 = Vec3<float>;
 
-// FP64 rows
-enum MixedRowD : int { dX = 0, dV = 3, dQ = 6, dW = 15, dInvL0 = 18, dSig0 = 19, dRowsD = 22 };
-// shared-memory rows of FP32 values per slot
-template <bool kDamped>
-constexpr int mixed_rows_f() { return kDamped ? 32 : 30; }
-
-// FP32 rows
-enum MixedRowF : int {
-  fMass = 0, fL0 = 1, fD0 = 2, fKap0 = 3, fShear = 6, fBend = 9, fJ = 12, fJinv = 15,
-  fF = 18, fP = 21, fM = 24, fE = 27, fDampR = 28,
-  fDampC = 29,  // 1 - exp(-nu_t dt) of the rod's analytical damper
-  fNuF = 30, fNuT = 31  // explicit damping only: the last rows, not allocated for undamped rods
+// Shared-memory layout, per slot (kCap entries a row):
+//   FP64 rows: position, velocity, angular velocity, 1 / rest length and the
+//   rest strain (with the unit axial strain folded in);
+//   the director as five double2 rows (Q0 Q1 | Q2 Q3 | Q4 Q5 | Q6 Q7 | Q8 -);
+//   FP32 float4 rows, each read or written with one 128-bit access: the
+//   element phase's parameters, the kick's parameters and the exchanged terms.
+// A warp's 128-bit accesses to one row cover 512 contiguous bytes, so they
+// take four wavefronts without bank conflicts, as four 32-bit rows would, in
+// a quarter of the instructions.
+enum MixedRowD : int { dX = 0, dV = 3, dW = 6, dInvL0 = 9, dSig0 = 10, dRowsD = 13 };
+constexpr int kQRows = 5;  // double2 rows of the director
+enum MixedRowP : int {
+  pA1 = 0,  // rest length, shear rigidity (3)
+  pA2 = 1,  // inertia J (3), Voronoi rest length
+  pA3 = 2,  // rest curvature (3), -
+  pA4 = 3,  // bend rigidity (3), -
+  pB1 = 4,  // J^-1 (3), mass
+  pB2 = 5,  // damper rate nu_r, 1 - exp(-nu_t dt), explicit damping nu_f, nu_t
+  pFE = 6,  // internal load (3), dilatation (exchanged)
+  pPP = 7,  // torque terms differenced ahead (3), - (own)
+  pMM = 8,  // couple terms differenced behind (3), - (exchanged)
+  kRowsP = 9
 };
+// bytes of shared memory a slot: 13 FP64 rows, 5 double2, 9 float4, two words
+constexpr int kMixedSlotBytes = dRowsD * 8 + kQRows * 16 + kRowsP * 16 + 8;
 
 template <int kCap>
 struct MRows {
   double* d;
-  float* f;
+  double2* q;
+  float4* p;
   __device__ __forceinline__ double& ad(int r, int s) const { return d[r * kCap + s]; }
-  __device__ __forceinline__ float& af(int r, int s) const { return f[r * kCap + s]; }
   __device__ __forceinline__ D3 d3(int r, int s) const { return {ad(r, s), ad(r + 1, s), ad(r + 2, s)}; }
   __device__ __forceinline__ void pd3(int r, int s, D3 v) const {
     ad(r, s) = v.x;
     ad(r + 1, s) = v.y;
     ad(r + 2, s) = v.z;
   }
-  __device__ __forceinline__ F3 f3(int r, int s) const { return {af(r, s), af(r + 1, s), af(r + 2, s)}; }
-  __device__ __forceinline__ void pf3(int r, int s, F3 v) const {
-    af(r, s) = v.x;
-    af(r + 1, s) = v.y;
-    af(r + 2, s) = v.z;
+  __device__ __forceinline__ void ldq(int s, double o[9]) const {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = q[k * kCap + s];
+      o[2 * k] = v.x;
+      o[2 * k + 1] = v.y;
+    }
+    o[8] = q[4 * kCap + s].x;
   }
+  __device__ __forceinline__ void stq(int s, const double o[9]) const {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k * kCap + s] = make_double2(o[2 * k], o[2 * k + 1]);
+    q[4 * kCap + s] = make_double2(o[8], 0.0);
+  }
+  __device__ __forceinline__ float4 p4(int r, int s) const { return p[r * kCap + s]; }
+  __device__ __forceinline__ void sp4(int r, int s, float4 v) const { p[r * kCap + s] = v; }
 };
 
 __device__ __forceinline__ F3 tof(D3 a) {
   return {static_cast<float>(a.x), static_cast<float>(a.y), static_cast<float>(a.z)};
 }
+__device__ __forceinline__ F3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 
 // FP64 director update Q <- exp(-[u]x) Q (Rodrigues' formula of
 // Systems/States/Expressions/backends/blaze/SO3PrimitiveAddAssign/Scalar.hpp:41-95),
@@ -145,11 +168,9 @@ __device__ __forceinline__ void drift(const MRows<kCap>& R, int s, uint32_t meta
   R.pd3(dX, s, D3{x.x + c * v.x, x.y + c * v.y, x.z + c * v.z});
   if (meta & kElem) {
     double q[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) q[k] = R.ad(dQ + k, s);
+    R.ldq(s, q);
     so3_series(q, c * w.x, c * w.y, c * w.z);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = q[k];
+    R.stq(s, q);
   }
 }
 
@@ -162,8 +183,10 @@ __device__ __forceinline__ void clamp_value(const MRows<kCap>& R, int s, uint32_
   const double* tq = (hits & kHitClamp0) ? ri.clamp_Q : ri.clamp2_Q;
   R.pd3(dX, s, D3{tx[0], tx[1], tx[2]});
   if (!(meta & kElem)) return;
+  double q[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) R.ad(dQ + k, s) = tq[k];
+  for (int k = 0; k < 9; ++k) q[k] = tq[k];
+  R.stq(s, q);
 }
 
 // Neighbour access for rod pairs: slot indices at or past `count` continue in
@@ -184,21 +207,17 @@ struct MPair {
     }
     return own;
   }
-  __device__ __forceinline__ double ad(int r, int s) const {
-    const MRows<kCap>& X = rows(s);
-    return X.ad(r, s);
-  }
-  __device__ __forceinline__ float af(int r, int s) const {
-    const MRows<kCap>& X = rows(s);
-    return X.af(r, s);
-  }
   __device__ __forceinline__ D3 d3(int r, int s) const {
     const MRows<kCap>& X = rows(s);
     return X.d3(r, s);
   }
-  __device__ __forceinline__ F3 f3(int r, int s) const {
+  __device__ __forceinline__ void ldq(int s, double o[9]) const {
     const MRows<kCap>& X = rows(s);
-    return X.f3(r, s);
+    X.ldq(s, o);
+  }
+  __device__ __forceinline__ float4 p4(int r, int s) const {
+    const MRows<kCap>& X = rows(s);
+    return X.p4(r, s);
   }
 };
 
@@ -209,23 +228,6 @@ __device__ __forceinline__ float element_length(const Rows& R, int s) {
   const F3 dxf = tof(R.d3(dX, s + 1) - R.d3(dX, s));
   const float l2 = dot(dxf, dxf);
   return l2 * rsqrtf(l2);
-}
-
-__device__ __forceinline__ int mixed_param_row(int f) {
-  switch (f) {
-    case kMass: return fMass;
-    case kL0: return fL0;
-    case kD0: return fD0;
-    case kNuF: return fNuF;
-    case kNuT: return fNuT;
-    default: break;
-  }
-  if (f >= kKap0 && f < kKap0 + 3) return fKap0 + (f - kKap0);
-  if (f >= kShear && f < kShear + 3) return fShear + (f - kShear);
-  if (f >= kBend && f < kBend + 3) return fBend + (f - kBend);
-  if (f >= kJ && f < kJ + 3) return fJ + (f - kJ);
-  if (f >= kJinv && f < kJinv + 3) return fJinv + (f - kJinv);
-  return -1;
 }
 
 // kServe: the CTA's slot range, step count, time step and environment come
@@ -239,8 +241,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     rod_block_mixed_kernel(const StepArgs a, const int64_t* cta_start, int n_steps_launch, const ServeCta* serve,
                            const int32_t* gmap) {
   extern __shared__ __align__(128) double smem[];
-  const MRows<kCap> R{smem, reinterpret_cast<float*>(smem + dRowsD * kCap)};
-  uint32_t* meta_s = reinterpret_cast<uint32_t*>(R.f + mixed_rows_f<kDamped>() * kCap);
+  double2* const qbase = reinterpret_cast<double2*>(smem + dRowsD * kCap);
+  float4* const pbase = reinterpret_cast<float4*>(qbase + kQRows * kCap);
+  const MRows<kCap> R{smem, qbase, pbase};
+  uint32_t* meta_s = reinterpret_cast<uint32_t*>(pbase + kRowsP * kCap);
   uint32_t* rflag_s = meta_s + kCap;
 
   const int tid = threadIdx.x;
@@ -282,8 +286,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     }
     if (paired) {
       cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-      N.peer.d = cl.map_shared_rank(R.d, cl.block_rank() ^ 1u);
-      N.peer.f = cl.map_shared_rank(R.f, cl.block_rank() ^ 1u);
+      const unsigned pr = cl.block_rank() ^ 1u;
+      N.peer.d = cl.map_shared_rank(R.d, pr);
+      N.peer.q = cl.map_shared_rank(R.q, pr);
+      N.peer.p = cl.map_shared_rank(R.p, pr);
     }
   }
   // orders a phase's writes before the next phase's neighbour reads
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     __syncthreads();
   };
 
-  // ---- stage state, parameters, reciprocals, FP32 copies and rod data
+  // ---- stage state, parameters, reciprocals and rod data
   const bool any_rod = (flags & (kSimClamp | kSimDamper | kSimEndTorque)) != 0;
   for (int s = tid; s < count; s += kThreads) {
     const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
@@ -313,22 +319,30 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       dr = static_cast<float>(ri.damper_r);
     }
     rflag_s[s] = rf;  // the slot's SlotHits
-    R.af(fDampC, s) = static_cast<float>(1.0 - dtc);
-    R.af(fDampR, s) = dr;
-#pragma unroll 1
-    for (int f = 0; f < kStateFields; ++f) R.ad(f, s) = a.in[f * S + g];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      R.ad(dX + k, s) = a.in[(kStX + k) * S + g];
+      R.ad(dV + k, s) = a.in[(kStV + k) * S + g];
+      R.ad(dW + k, s) = a.in[(kStW + k) * S + g];
+    }
+    double q[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q[k] = a.in[(kStQ + k) * S + g];
+    R.stq(s, q);
     const double il0 = 1.0 / a.par[kL0 * S + g];
     R.ad(dInvL0, s) = il0;
     // the rest strain, with the unit axial strain of sigma = Q dx / l0 - z folded in
     R.ad(dSig0, s) = a.par[kSig0 * S + g];
     R.ad(dSig0 + 1, s) = a.par[(kSig0 + 1) * S + g];
     R.ad(dSig0 + 2, s) = a.par[(kSig0 + 2) * S + g] + 1.0;
-#pragma unroll 1
-    for (int f = 0; f < kParamFields; ++f) {
-      const int r = mixed_param_row(f);
-      if (r < 0 || (!kDamped && (f == kNuF || f == kNuT))) continue;
-      R.af(r, s) = static_cast<float>(a.par[f * S + g]);
-    }
+    auto pf = [&](int f) { return static_cast<float>(a.par[f * S + g]); };
+    R.sp4(pA1, s, make_float4(pf(kL0), pf(kShear), pf(kShear + 1), pf(kShear + 2)));
+    R.sp4(pA2, s, make_float4(pf(kJ), pf(kJ + 1), pf(kJ + 2), pf(kD0)));
+    R.sp4(pA3, s, make_float4(pf(kKap0), pf(kKap0 + 1), pf(kKap0 + 2), 0.f));
+    R.sp4(pA4, s, make_float4(pf(kBend), pf(kBend + 1), pf(kBend + 2), 0.f));
+    R.sp4(pB1, s, make_float4(pf(kJinv), pf(kJinv + 1), pf(kJinv + 2), pf(kMass)));
+    R.sp4(pB2, s, make_float4(dr, static_cast<float>(1.0 - dtc), kDamped ? pf(kNuF) : 0.f,
+                              kDamped ? pf(kNuT) : 0.f));
   }
   __syncthreads();
 
@@ -359,10 +373,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       float e = 1.f;
       if (meta & kElem) {
         const D3 dx = (kPair ? N.d3(dX, s + 1) : R.d3(dX, s + 1)) - R.d3(dX, s);
+        double q[9];
+        R.ldq(s, q);
         double qd[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-          qd[k] = R.ad(dQ + 3 * k, s) * dx.x + R.ad(dQ + 3 * k + 1, s) * dx.y + R.ad(dQ + 3 * k + 2, s) * dx.z;
+        for (int k = 0; k < 3; ++k) qd[k] = q[3 * k] * dx.x + q[3 * k + 1] * dx.y + q[3 * k + 2] * dx.z;
         const double il0 = R.ad(dInvL0, s);
         const F3 d = {static_cast<float>(qd[0] * il0 - R.ad(dSig0, s)),
                       static_cast<float>(qd[1] * il0 - R.ad(dSig0 + 1, s)),
@@ -372,19 +387,18 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         const float il = rsqrtf(l2);
         const float l = l2 * il;
         const F3 t = scale(dxf, il);
-        const float l0 = R.af(fL0, s);
+        const float4 a1 = R.p4(pA1, s), a2 = R.p4(pA2, s);
+        const float l0 = a1.x;
         e = l * static_cast<float>(il0);
         const float ie = l0 * il;
-        const F3 sh = R.f3(fShear, s);
-        const F3 nl = {sh.x * d.x, sh.y * d.y, sh.z * d.z};
+        const F3 nl = {a1.y * d.x, a1.z * d.y, a1.w * d.z};
         float qf[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
+        for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(q[k]);
         f = scale(mattranspvec(qf, nl), ie);
         const F3 qt = matvec(qf, t);
         const F3 w = tof(R.d3(dW, s));
-        const F3 J = R.f3(fJ, s);
-        const F3 jwe = {J.x * w.x * ie, J.y * w.y * ie, J.z * w.z * ie};
+        const F3 jwe = {a2.x * w.x * ie, a2.y * w.y * ie, a2.z * w.z * ie};
         const F3 dv = tof((kPair ? N.d3(dV, s + 1) : R.d3(dV, s + 1)) - R.d3(dV, s));
         const float rate = dot(t, dv) * il;
         p = scale(cross(qt, nl), l0) + cross(jwe, w) + scale(jwe, rate);
@@ -396,10 +410,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           // and 1 - cos(theta) = 1.5 - tr/2 = |dd|^2/4 for unit rows (their
           // norms stay within 1e-14 of one, below the reference's 1e-10 shift);
           // both forms are free of the cancellation of the original products.
+          double qn[9];
+          if constexpr (kPair) N.ldq(s + 1, qn);
+          else R.ldq(s + 1, qn);
           float dd[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k)
-            dd[k] = static_cast<float>((kPair ? N.ad(dQ + k, s + 1) : R.ad(dQ + k, s + 1)) - R.ad(dQ + k, s));
+          for (int k = 0; k < 9; ++k) dd[k] = static_cast<float>(qn[k] - q[k]);
           float sq = 0.f;
 #pragma unroll
           for (int k = 0; k < 9; ++k) sq += dd[k] * dd[k];
@@ -415,7 +431,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           } else {
             ratio = 2.f * asinf(sqrtf(0.5f * y)) * rsqrtf(y * (2.f - y));
           }
-          const float D0 = R.af(fD0, s);
+          const float D0 = a2.w;
           const float st = 0.5f * ratio * __frcp_rn(D0);
           const F3 d1{qf[0], qf[1], qf[2]}, d2{qf[3], qf[4], qf[5]}, d3{qf[6], qf[7], qf[8]};
           const F3 e1{dd[0], dd[1], dd[2]}, e2{dd[3], dd[4], dd[5]}, e3{dd[6], dd[7], dd[8]};
@@ -425,8 +441,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           const float ieps =
               __fdividef(D0, 0.5f * (l + (kPair ? element_length(N, s + 1) : element_length(R, s + 1))));
           const float ic = ieps * ieps * ieps;
-          const F3 dk = kappa - R.f3(fKap0, s);
-          const F3 B = R.f3(fBend, s);
+          const F3 dk = kappa - xyz(R.p4(pA3, s));
+          const F3 B = xyz(R.p4(pA4, s));
           const F3 tau = {B.x * dk.x, B.y * dk.y, B.z * dk.z};
           // the couple's two parts: G = tau / eps^3 (differenced) and
           // H = (kappa x tau) D0 / eps^3 (averaged) enter torque s as
@@ -437,22 +453,26 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
           mm = gg - hh;
         }
       }
-      R.af(fE, s) = e;
-      R.pf3(fF, s, f);
-      R.pf3(fP, s, p);
-      R.pf3(fM, s, mm);
+      R.sp4(pFE, s, make_float4(f.x, f.y, f.z, e));
+      R.sp4(pPP, s, make_float4(p.x, p.y, p.z, 0.f));
+      R.sp4(pMM, s, make_float4(mm.x, mm.y, mm.z, 0.f));
     }
     sync_neighbours();
 
     for (int s = tid; s < count; s += kThreads) {
       const uint32_t meta = meta_s[s];
       const bool first = (meta & kFirst) != 0;
-      const float m = R.af(fMass, s);
+      const float4 b1 = R.p4(pB1, s);
+      const float m = b1.w;
       D3 v = R.d3(dV, s);
-      F3 F = R.f3(fF, s);
-      if (!first) F = F - (kPair ? N.f3(fF, s - 1) : R.f3(fF, s - 1));
+      const float4 fe = R.p4(pFE, s);
+      F3 F = xyz(fe);
+      if (!first) F = F - xyz(kPair ? N.p4(pFE, s - 1) : R.p4(pFE, s - 1));
+      const uint32_t rf = rflag_s[s];
+      float4 b2 = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (kDamped || (rf & kHitDamper)) b2 = R.p4(pB2, s);
       if (kDamped) {
-        const float cf = m * R.af(fNuF, s);
+        const float cf = m * b2.z;
         const F3 vf = tof(v);
         F = {F.x - cf * vf.x, F.y - cf * vf.y, F.z - cf * vf.z};
       }
@@ -461,34 +481,35 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       v = {v.x + dt * static_cast<double>(F.x * im), v.y + dt * static_cast<double>(F.y * im),
            v.z + dt * static_cast<double>(F.z * im)};
       D3 w{0.0, 0.0, 0.0};
-      const uint32_t rf = rflag_s[s];
       if (meta & kElem) {
-        const float e = R.af(fE, s);
+        const float e = fe.w;
         w = R.d3(dW, s);
-        F3 T = R.f3(fP, s);
-        if (!first) T = T - (kPair ? N.f3(fM, s - 1) : R.f3(fM, s - 1));
+        F3 T = xyz(R.p4(pPP, s));
+        if (!first) T = T - xyz(kPair ? N.p4(pMM, s - 1) : R.p4(pMM, s - 1));
+        const float mn = (kDamped || (rf & kHitDamper)) ? (kPair ? N.p4(pB1, s + 1) : R.p4(pB1, s + 1)).w : 0.f;
         if (kDamped) {
-          const float ct = 0.5f * (m + (kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1))) * R.af(fNuT, s);
+          const float ct = 0.5f * (m + mn) * b2.w;
           const F3 wf = tof(w);
           T = {T.x - ct * wf.x, T.y - ct * wf.y, T.z - ct * wf.z};
         }
         if (rf & kHitTorque) {
           const RodInfo& ri = a.rods[meta >> kRodShift];
+          double q[9];
+          R.ldq(s, q);
           float qf[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(R.ad(dQ + k, s));
+          for (int k = 0; k < 9; ++k) qf[k] = static_cast<float>(q[k]);
           T = T + matvec(qf, F3{static_cast<float>(ri.end_torque[0]), static_cast<float>(ri.end_torque[1]),
                                 static_cast<float>(ri.end_torque[2])});
         }
-        const F3 ji = R.f3(fJinv, s);
+        const F3 ji = xyz(b1);
         w = {w.x + dt * static_cast<double>(ji.x * T.x * e), w.y + dt * static_cast<double>(ji.y * T.y * e),
              w.z + dt * static_cast<double>(ji.z * T.z * e)};
         if (rf & kHitDamper) {
-          const float mn = kPair ? N.af(fMass, s + 1) : R.af(fMass, s + 1);
           float em = 0.5f * (m + mn);
           if (first) em += 0.5f * m;
           if (meta & kLastElem) em += 0.5f * mn;
-          const float y = -R.af(fDampR, s) * em * dtf * e;
+          const float y = -b2.x * em * dtf * e;
           w = {w.x * static_cast<double>(exp_small(y * ji.x)), w.y * static_cast<double>(exp_small(y * ji.y)),
                w.z * static_cast<double>(exp_small(y * ji.z))};
         }
@@ -498,7 +519,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         v = D3{0.0, 0.0, 0.0};
         w = D3{0.0, 0.0, 0.0};
       }
-      if (rf & kHitDamper) v = scale(v, 1.0 - static_cast<double>(R.af(fDampC, s)));
+      if (rf & kHitDamper) v = scale(v, 1.0 - static_cast<double>(b2.y));
       R.pd3(dV, s, v);
       if (meta & kElem) R.pd3(dW, s, w);
       drift(R, s, meta, last ? hdt : dt, v, w);
@@ -506,10 +527,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       if (last) {
         const int64_t g = kGather ? static_cast<int64_t>(gmap[g0 + s]) : g0 + s;
 #pragma unroll
-        for (int fld = 0; fld < 6; ++fld) a.out[fld * S + g] = R.ad(fld, s);
+        for (int k = 0; k < 3; ++k) {
+          a.out[(kStX + k) * S + g] = R.ad(dX + k, s);
+          a.out[(kStV + k) * S + g] = R.ad(dV + k, s);
+        }
         if (meta & kElem) {
+          double q[9];
+          R.ldq(s, q);
 #pragma unroll
-          for (int fld = 6; fld < kStateFields; ++fld) a.out[fld * S + g] = R.ad(fld, s);
+          for (int k = 0; k < 9; ++k) a.out[(kStQ + k) * S + g] = q[k];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) a.out[(kStW + k) * S + g] = R.ad(dW + k, s);
         }
       }
     }
@@ -520,9 +548,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 template <int kCap, int kThreads, int kMinBlocks, bool kServe = false, bool kGather = false, bool kPair = false>
 cudaError_t launch_mixed_cfg(const StepArgs& args, const int64_t* cta_start, int n_ctas, int n_steps, bool damped,
                              cudaStream_t stream, const ServeCta* serve = nullptr, const int32_t* gmap = nullptr) {
-  const int rows_f = damped ? mixed_rows_f<true>() : mixed_rows_f<false>();
-  const size_t bytes = size_t(dRowsD) * kCap * sizeof(double) + size_t(rows_f) * kCap * sizeof(float) +
-                       2 * size_t(kCap) * sizeof(uint32_t);
+  const size_t bytes = size_t(kMixedSlotBytes) * kCap;
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
     if (e != cudaSuccess) return e;
