@@ -250,13 +250,12 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) 
     atomicOr(a.status, kStatusContactIndex);
     return;
   }
-  a.sorted_id[pos] = static_cast<int32_t>(s);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    a.sorted_cell[3 * pos + d] = a.cell[d * S + s];
-    a.sorted_box[6 * pos + d] = a.cap[(kCapLo + d) * S + s];
-    a.sorted_box[6 * pos + 3 + d] = a.cap[(kCapHi + d) * S + s];
-  }
+  double* rec = a.sorted_rec + static_cast<int64_t>(kSortedRecDoubles) * pos;
+  *reinterpret_cast<int4*>(rec) = make_int4(a.cell[s], a.cell[S + s], a.cell[2 * S + s], static_cast<int32_t>(s));
+  double2* box = reinterpret_cast<double2*>(rec + 2);
+  box[0] = make_double2(a.cap[kCapLo * S + s], a.cap[(kCapLo + 1) * S + s]);
+  box[1] = make_double2(a.cap[(kCapLo + 2) * S + s], a.cap[kCapHi * S + s]);
+  box[2] = make_double2(a.cap[(kCapHi + 1) * S + s], a.cap[(kCapHi + 2) * S + s]);
 }
 
 // ---- stage 3: candidate pairs ----------------------------------------------
@@ -274,14 +273,21 @@ __device__ __forceinline__ void sort_ids(int32_t* v, int32_t n) {
 }
 
 // kPass 0: count and fill the fixed-stride list; kPass 1: overflow lists of
-// the capsules with more than kFixedPartners partners
+// the capsules with more than kFixedPartners partners.  The search is bound
+// by dependent round trips to L2: every entry of a neighbouring bucket is
+// one 64-byte record read whole before it is tested (its cell, slot and box
+// were three dependent loads when kept in separate arrays), and the bucket
+// range of the next neighbouring cell is loaded while the current one's
+// entries are scanned.
 template <int kPass>
 __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps_max) {
   // entries filed this evaluation (the capsules with finite boxes)
   const int32_t n_caps = min(a.bucket_start[a.table_mask + 1], n_caps_max);
   const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
   if (e >= n_caps) return;
-  const int32_t id = a.sorted_id[e];
+  const double* own = a.sorted_rec + static_cast<int64_t>(kSortedRecDoubles) * e;
+  const int4 me = *reinterpret_cast<const int4*>(own);
+  const int32_t id = me.w;
   int32_t* out;
   if (kPass == 1) {
     if (a.pair_count[id] <= kFixedPartners) return;
@@ -295,30 +301,45 @@ __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, in
   } else {
     out = a.fixed + static_cast<int64_t>(id) * kFixedPartners;
   }
-  const int32_t cx = a.sorted_cell[3 * e], cy = a.sorted_cell[3 * e + 1], cz = a.sorted_cell[3 * e + 2];
+  const int32_t cx = me.x, cy = me.y, cz = me.z;
   double lo[3], hi[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    lo[d] = a.sorted_box[6 * e + d];
-    hi[d] = a.sorted_box[6 * e + 3 + d];
+  {
+    const double2* ob = reinterpret_cast<const double2*>(own + 2);
+    const double2 o0 = ob[0], o1 = ob[1], o2 = ob[2];
+    lo[0] = o0.x;
+    lo[1] = o0.y;
+    lo[2] = o1.x;
+    hi[0] = o1.y;
+    hi[1] = o2.x;
+    hi[2] = o2.y;
   }
   int32_t cnt = 0;
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int32_t nx = cx + dx, ny = cy + dy, nz = cz + dz;
-        const uint32_t b = cell_hash(nx, ny, nz) & a.table_mask;
-        const int32_t k0 = max(a.bucket_start[b], 0), k1 = min(a.bucket_start[b + 1], n_caps);
-        for (int32_t k = k0; k < k1; ++k) {
-          if (a.sorted_cell[3 * k] != nx || a.sorted_cell[3 * k + 1] != ny || a.sorted_cell[3 * k + 2] != nz) continue;
-          const int32_t other = a.sorted_id[k];
-          if (other == id) continue;
-          const double* bx = a.sorted_box + 6 * k;
-          if (!overlaps(lo, hi, bx, bx + 3)) continue;
-          if (kPass == 1 || cnt < kFixedPartners) out[cnt] = other;
-          ++cnt;
-        }
-      }
+  // neighbour cell c: dx = c % 3 - 1 fastest, then dy, then dz
+  uint32_t b = cell_hash(cx - 1, cy - 1, cz - 1) & a.table_mask;
+  int32_t next0 = a.bucket_start[b], next1 = a.bucket_start[b + 1];
+  for (int c = 0; c < 27; ++c) {
+    const int32_t nx = cx + c % 3 - 1, ny = cy + (c / 3) % 3 - 1, nz = cz + c / 9 - 1;
+    const int32_t k0 = max(next0, 0), k1 = min(next1, n_caps);
+    if (c + 1 < 27) {
+      b = cell_hash(cx + (c + 1) % 3 - 1, cy + ((c + 1) / 3) % 3 - 1, cz + (c + 1) / 9 - 1) & a.table_mask;
+      next0 = a.bucket_start[b];
+      next1 = a.bucket_start[b + 1];
+    }
+    for (int32_t k = k0; k < k1; ++k) {
+      const double* r = a.sorted_rec + static_cast<int64_t>(kSortedRecDoubles) * k;
+      const int4 h = *reinterpret_cast<const int4*>(r);
+      const double2* rb = reinterpret_cast<const double2*>(r + 2);
+      const double2 b0 = rb[0], b1 = rb[1], b2 = rb[2];
+      // every part of the record is used whatever the cell, so all four
+      // loads issue together
+      const bool in_cell = (h.x == nx) & (h.y == ny) & (h.z == nz) & (h.w != id);
+      const bool apart = (b0.x > hi[0]) | (b0.y > hi[1]) | (b1.x > hi[2]) | (b1.y < lo[0]) | (b2.x < lo[1]) |
+                         (b2.y < lo[2]);
+      if (!in_cell || apart) continue;
+      if (kPass == 1 || cnt < kFixedPartners) out[cnt] = h.w;
+      ++cnt;
+    }
+  }
   for (int32_t p = 0; p < a.n_planes; ++p) {
     if (!overlaps(lo, hi, a.planes[p].lo, a.planes[p].hi)) continue;
     if (kPass == 1 || cnt < kFixedPartners) out[cnt] = static_cast<int32_t>(a.n_slots) + p;

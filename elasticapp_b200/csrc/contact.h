@@ -23,6 +23,8 @@ enum CapsuleRow : int {
   kCapRows = 20
 };
 
+constexpr int kSortedRecDoubles = 8;
+
 // partners a capsule keeps in its fixed-stride list; a capsule with more
 // (a pile-up) gets its whole list in the overflow lists instead
 constexpr int kFixedPartners = 32;
@@ -59,9 +61,10 @@ struct ContactArgs {
   uint32_t table_mask;               // hash table size - 1 (power of two)
   int32_t* bucket_count;             // table size (zero between steps)
   int32_t* bucket_start;             // table size + 1
-  int32_t* sorted_id;                // capsules grouped by bucket
-  int32_t* sorted_cell;              // 3 per entry
-  double* sorted_box;                // 6 per entry
+  // the capsules grouped by bucket, one 64-byte record an entry: cell
+  // (3 x int32) and slot (int32) in the first 16 bytes, then the box's lower
+  // and upper corners (6 doubles)
+  double* sorted_rec;                // kSortedRecDoubles per entry
   int32_t* pair_count;               // stride (zero outside capsules): partners per capsule
   int32_t* fixed;                    // kFixedPartners x stride: partner lists of up to kFixedPartners
   int32_t* ovf_count;                // stride: the count of capsules beyond kFixedPartners, else 0

@@ -133,9 +133,7 @@ struct ContactDevice {
   uint32_t* bucket = nullptr;
   int32_t* bucket_count = nullptr;
   int32_t* bucket_start = nullptr;
-  int32_t* sorted_id = nullptr;
-  int32_t* sorted_cell = nullptr;
-  double* sorted_box = nullptr;
+  double* sorted_rec = nullptr;
   int32_t* pair_count = nullptr;
   int32_t* fixed = nullptr;
   int32_t* ovf_count = nullptr;
@@ -448,7 +446,7 @@ void host_free(eb_sim* s) {
     }
   ContactDevice& c = s->contact;
   void* cptrs[] = {c.cap, c.cap_material, c.extent, c.cell, c.bucket, c.bucket_count, c.bucket_start,
-                   c.sorted_id, c.sorted_cell, c.sorted_box, c.pair_count, c.fixed, c.ovf_count, c.pair_offset,
+                   c.sorted_rec, c.pair_count, c.fixed, c.ovf_count, c.pair_offset,
                    c.partners,
                    c.required, c.planes, c.pair_table, c.loads, c.scan_blocks, c.backup};
   for (void* p : cptrs)
@@ -578,9 +576,7 @@ eb_status setup_contact(eb_sim* s) {
   alloc(&c.bucket, static_cast<size_t>(S) * sizeof(uint32_t));
   alloc(&c.bucket_count, static_cast<size_t>(table) * sizeof(int32_t));
   alloc(&c.bucket_start, static_cast<size_t>(table + 1) * sizeof(int32_t));
-  alloc(&c.sorted_id, static_cast<size_t>(n_caps) * sizeof(int32_t));
-  alloc(&c.sorted_cell, static_cast<size_t>(3 * n_caps) * sizeof(int32_t));
-  alloc(&c.sorted_box, static_cast<size_t>(6 * n_caps) * sizeof(double));
+  alloc(&c.sorted_rec, static_cast<size_t>(eb::kSortedRecDoubles * n_caps) * sizeof(double));
   alloc(&c.pair_count, static_cast<size_t>(S) * sizeof(int32_t));
   alloc(&c.fixed, static_cast<size_t>(S) * eb::kFixedPartners * sizeof(int32_t));
   alloc(&c.ovf_count, static_cast<size_t>(S) * sizeof(int32_t));
@@ -1730,9 +1726,7 @@ eb::ContactArgs contact_args(eb_sim* s, double dt) {
   a.table_mask = c.table_mask;
   a.bucket_count = c.bucket_count;
   a.bucket_start = c.bucket_start;
-  a.sorted_id = c.sorted_id;
-  a.sorted_cell = c.sorted_cell;
-  a.sorted_box = c.sorted_box;
+  a.sorted_rec = c.sorted_rec;
   a.pair_count = c.pair_count;
   a.fixed = c.fixed;
   a.ovf_count = c.ovf_count;
