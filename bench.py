@@ -69,13 +69,14 @@ def source_digest(*names: str) -> str:
     return h.hexdigest()[:16]
 
 
-def profile_traffic(kernel: str, workload: str, sources: tuple):
+def profile_traffic(kernel: str, workload: str, sources: tuple, elements: int):
     """DRAM bytes per launch from the committed ncu summary of this kernel
     and workload, if its recorded source digest matches the kernel sources
-    as they are now (a summary of an older kernel is not reported).
+    as they are now (a summary of an older kernel is not reported) and it
+    covers a launch over the same number of elements.
     Returns (bytes or None, note)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
-    traffic, digest = None, None
+    traffic, digest, covered = None, None, None
     try:
         with open(path, encoding="utf-8") as f:
             for line in f:
@@ -83,11 +84,15 @@ def profile_traffic(kernel: str, workload: str, sources: tuple):
                     traffic = float(line.split(":", 1)[1].strip())
                 elif line.startswith("source_digest:"):
                     digest = line.split(":", 1)[1].strip()
+                elif line.startswith("elements_per_launch:"):
+                    covered = int(line.split(":", 1)[1].strip())
     except OSError:
         return None, "no ncu summary"
     now = source_digest(*sources)
     if digest != now:
         return None, f"stale ncu summary ({digest} != {now})"
+    if covered != elements:
+        return None, f"ncu summary covers {covered} elements, this launch {elements}"
     return traffic, f"ncu, sources {now}"
 
 
@@ -691,7 +696,8 @@ def main(argv=None) -> int:
     alg = algorithmic_bytes(wl.n_elements, damped=False)
     per_launch_s = (ms / 1e3) / args.steps
     achieved = alg / per_launch_s / 1e9
-    traffic, traffic_note = profile_traffic("rod_step_fp64", wl.name, ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh"))
+    traffic, traffic_note = profile_traffic("rod_step_fp64", wl.name, ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh"),
+                                            int(sum(wl.n_elements)))
 
     # ---- end to end through the public API with host buffers: each cycle
     # uploads the dynamic state from pinned memory, runs E2E_STEPS_PER_CYCLE
