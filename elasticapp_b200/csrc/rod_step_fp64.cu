@@ -33,10 +33,15 @@
 // waits are bounded; the threads vote on them, and a CTA whose copies did
 // not land in time records it in the status word, waits for the copies it
 // issued and leaves.  The 128-slot windows run 5 CTAs per SM (96 registers a
-// thread, 40 KB of shared memory a CTA); a thread keeps its slot's state in
-// registers from phase to phase.  (Re-reading the slot from shared memory
-// instead, at 80 registers and six CTAs an SM with 1 / J formed from J,
-// measured 6% slower.)  Every field row of
+// thread, 40 KB of shared memory a CTA); a thread keeps its slot's directors
+// and angular velocity in registers from phase to phase.  (Re-reading all of
+// the slot from shared memory instead, at 80 registers and six CTAs an SM
+// with 1 / J formed from J, measured 6% slower; re-reading the directors as
+// well as the values below, 2% slower.)  What a thread carries across the barriers is kept
+// small: the position, velocity and mass are re-read from their rows in the
+// last phase, and in the default build the three element-local torque terms
+// travel as one sum; with no register spills left this took the step from
+// 0.408 to 0.383 ms on the uneven batch.  Every field row of
 // a window is 16-byte aligned in global memory because windows start on an
 // even slot and every field array starts on a 256-byte boundary.  The values
 // exchanged between neighbouring threads (element lengths, Q^T n_L / e, the
@@ -209,7 +214,6 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     v = R.get3(rV, s);
     const D3 x0 = R.get3(rX, s);
     x = {x0.x + hdt * v.x, x0.y + hdt * v.y, x0.z + hdt * v.z};
-    m = R.at(rMass, s);
     if (meta & kElem) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) q[k] = R.at(rQ + k, s);
@@ -275,6 +279,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
 #endif
       t_lag = cross(jwe, w);
       t_unst = scale(jwe, rate);
+#ifdef EB_FAST_FP64
+      // one vector instead of three carried to phase 4 (the sum is
+      // associated differently: a rounding-level change)
+      t_shear = t_shear + t_lag + t_unst;
+#endif
     }
     R.at(rL, s) = l;
     R.put3(rF, s, f);
@@ -313,6 +322,11 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
   __syncthreads();
 
   if (!interior) return;
+  // the slot's drifted position, velocity and mass from its rows (phase 1
+  // left them there), not carried in registers across the barriers
+  x = R.get3(rX, s);
+  v = R.get3(rV, s);
+  m = R.at(rMass, s);
 
   // ---- phase 4: loads, update_acceleration (WithRodKinematics.hpp:684-714)
   D3 F = R.get3(rF, s) - R.get3(rF, s - 1);
@@ -346,8 +360,10 @@ __device__ __forceinline__ void rod_step_window(const StepArgs& a, double* smem)
     const D3 h1 = R.get3(rH, s), h0 = R.get3(rH, s - 1);  // quadrature of h
     T = T + D3{0.5 * (h1.x + h0.x), 0.5 * (h1.y + h0.y), 0.5 * (h1.z + h0.z)};
     T = T + t_shear;
+#ifndef EB_FAST_FP64
     T = T + t_lag;
     T = T + t_unst;
+#endif
     if (kDamped) {
       const double em = 0.5 * (m + R.at(rMass, s + 1));
       const double c = em * R.at(rNuT, s);
