@@ -114,3 +114,26 @@ def test_compact_line_fits_the_tail():
                                                     "sustained_load": serving["sustained_load"]}, cant, mixed)
     assert list(sec)[-1] == "mixed"
     assert len(json.dumps(sec, separators=(",", ":"))) < 1500
+
+
+def test_profile_traffic_only_for_the_profiled_launch():
+    """The committed ncu traffic figure of the step kernel is reported for a
+    launch over the element count its summary covers, with the sources it
+    was captured from, and for nothing else."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    srcs = ("rod_step_fp64.cu", "rod_math.cuh", "bulk_copy.cuh")
+    path = os.path.join(ROOT, "profiles", "rod_step_fp64_uneven_batch.txt")
+    covered = None
+    with open(path, encoding="utf-8") as f:
+        for line in f:
+            if line.startswith("elements_per_launch:"):
+                covered = int(line.split(":", 1)[1])
+    assert covered is not None
+    traffic, note = bench.profile_traffic("rod_step_fp64", "uneven_batch", srcs, covered)
+    assert traffic is not None and traffic > 0, note
+    traffic, note = bench.profile_traffic("rod_step_fp64", "uneven_batch", srcs, covered // 8)
+    assert traffic is None and "covers" in note
+    traffic, note = bench.profile_traffic("rod_step_fp64", "no_such_workload", srcs, covered)
+    assert traffic is None and note == "no ncu summary"
