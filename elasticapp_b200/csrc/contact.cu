@@ -282,31 +282,48 @@ __device__ __forceinline__ void sort_ids(int32_t* v, int32_t n) {
 // were three dependent loads when kept in separate arrays), and the bucket
 // range of the next neighbouring cell is loaded while the current one's
 // entries are scanned.
+// kPass 0 runs a thread per filed entry and takes the capsule's cell and box
+// from its record; kPass 1 runs a thread per slot and leaves at once unless
+// the slot's count (coalesced) is above kFixedPartners, taking the cell and
+// box from the slot-major rows the records were written from.
 template <int kPass>
 __global__ void __launch_bounds__(kThreads) pairs_kernel(const ContactArgs a, int32_t n_caps_max) {
   // entries filed this evaluation (the capsules with finite boxes)
   const int32_t n_caps = min(a.bucket_start[a.table_mask + 1], n_caps_max);
-  const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
-  if (e >= n_caps) return;
-  const double* own = a.sorted_rec + static_cast<int64_t>(kSortedRecDoubles) * e;
-  const int4 me = *reinterpret_cast<const int4*>(own);
-  const int32_t id = me.w;
+  int32_t id, cx, cy, cz;
+  double lo[3], hi[3];
   int32_t* out;
   if (kPass == 1) {
-    if (a.pair_count[id] <= kFixedPartners) return;
+    const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    // only filed capsules have a count; the others hold zero
+    if (s >= a.n_slots || a.pair_count[s] <= kFixedPartners) return;
     const int64_t total = a.pair_offset[a.n_slots];
     if (total > a.capacity) {
       atomicOr(a.status, kStatusPairOverflow);
       atomicMax(a.required, static_cast<unsigned long long>(total));
       return;
     }
-    out = a.partners + a.pair_offset[id];  // within [0, capacity)
+    out = a.partners + a.pair_offset[s];  // within [0, capacity)
+    const int64_t S = a.stride;
+    id = static_cast<int32_t>(s);
+    cx = a.cell[s];
+    cy = a.cell[S + s];
+    cz = a.cell[2 * S + s];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = a.cap[(kCapLo + d) * S + s];
+      hi[d] = a.cap[(kCapHi + d) * S + s];
+    }
   } else {
+    const int32_t e = static_cast<int32_t>(blockIdx.x) * kThreads + threadIdx.x;
+    if (e >= n_caps) return;
+    const double* own = a.sorted_rec + static_cast<int64_t>(kSortedRecDoubles) * e;
+    const int4 me = *reinterpret_cast<const int4*>(own);
+    id = me.w;
     out = a.fixed + static_cast<int64_t>(id) * kFixedPartners;
-  }
-  const int32_t cx = me.x, cy = me.y, cz = me.z;
-  double lo[3], hi[3];
-  {
+    cx = me.x;
+    cy = me.y;
+    cz = me.z;
     const double2* ob = reinterpret_cast<const double2*>(own + 2);
     const double2 o0 = ob[0], o1 = ob[1], o2 = ob[2];
     lo[0] = o0.x;
@@ -694,7 +711,7 @@ cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* l
   *launches += 2;
   e = exclusive_scan<int64_t>(a.ovf_count, a.pair_offset, a.n_slots, a.scan_blocks, false, stream, launches);
   if (e != cudaSuccess) return e;
-  if (ge > 0) pairs_kernel<1><<<ge, kThreads, 0, stream>>>(a, a.n_caps);
+  pairs_kernel<1><<<gs, kThreads, 0, stream>>>(a, a.n_caps);
   force_kernel<<<static_cast<unsigned>((a.n_slots + kForceThreads - 1) / kForceThreads), kForceThreads, 0, stream>>>(a);
   *launches += 2;
   return cudaGetLastError();
