@@ -1853,12 +1853,12 @@ eb_status damper_for_dt(eb_sim* s, double dt) {
 // whole-batch configuration; mode 3: each size bucket's): the rods in order
 // cut into contiguous runs of about equal slot counts, each packed on its own
 // the way the plan packs the whole batch (a group's CTAs touch only its
-// slots, so its launches need only its copies).  One group per three waves
-// of 512-slot CTAs, at most sixteen (the first group's upload and the last
-// one's download overlap no launch; halving them against groups of six
-// waves, at most eight, took the uneven batch's exchange from 13.5 to 14.1 G
-// element-steps/s); a single group means no overlap and the exchange runs
-// its copies and steps in sequence.
+// slots, so its launches need only its copies).  One group per two waves of
+// 512-slot CTAs, at most 32 (the first group's upload and the last one's
+// download overlap no launch; against groups of six waves, at most eight,
+// that took the uneven batch's exchange from 13.5 to 14.3 G element-steps/s,
+// 14.1 G with groups of three waves); a single group means no overlap and
+// the exchange runs its copies and steps in sequence.
 eb_status upload_list(eb_sim* s, const std::vector<int64_t>& off, const std::vector<int32_t>& map, int64_t** d_off,
                       int32_t** d_map) {
   EB_CUDA(cudaMalloc(reinterpret_cast<void**>(d_off), off.size() * sizeof(int64_t)));
@@ -1886,8 +1886,8 @@ eb_status build_exchange_groups(eb_sim* s) {
   s->xplan = plan;
   int sms = 0;
   EB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device));
-  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * 512 * 3;
-  const int64_t n_groups = std::min<int64_t>(16, std::max<int64_t>(1, s->n_slots / per_group));
+  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * 512 * 2;
+  const int64_t n_groups = std::min<int64_t>(32, std::max<int64_t>(1, s->n_slots / per_group));
   if (n_groups < 2 || s->rods.size() < 2) return EB_OK;
   std::vector<std::vector<size_t>> members(1);
   std::vector<int64_t> cut(1, 0);
