@@ -1853,12 +1853,13 @@ eb_status damper_for_dt(eb_sim* s, double dt) {
 // whole-batch configuration; mode 3: each size bucket's): the rods in order
 // cut into contiguous runs of about equal slot counts, each packed on its own
 // the way the plan packs the whole batch (a group's CTAs touch only its
-// slots, so its launches need only its copies).  One group per two waves of
-// 512-slot CTAs, at most 32 (the first group's upload and the last one's
-// download overlap no launch; against groups of six waves, at most eight,
-// that took the uneven batch's exchange from 13.5 to 14.3 G element-steps/s,
-// 14.1 G with groups of three waves); a single group means no overlap and
-// the exchange runs its copies and steps in sequence.
+// slots, so its launches need only its copies).  The first group's upload and
+// the last one's download overlap no launch, so the groups are small at
+// either end and larger in between (1, 2, then about 4 waves of 512-slot
+// CTAs each, then 2 and 1): against equal groups of six waves, at most eight,
+// that took the uneven batch's exchange from 13.5 to 14.5 G element-steps/s
+// (14.1 G with equal groups of three waves, 14.3 G of two).  A single group
+// means no overlap and the exchange runs its copies and steps in sequence.
 eb_status upload_list(eb_sim* s, const std::vector<int64_t>& off, const std::vector<int32_t>& map, int64_t** d_off,
                       int32_t** d_map) {
   EB_CUDA(cudaMalloc(reinterpret_cast<void**>(d_off), off.size() * sizeof(int64_t)));
@@ -1886,14 +1887,37 @@ eb_status build_exchange_groups(eb_sim* s) {
   s->xplan = plan;
   int sms = 0;
   EB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device));
-  const int64_t per_group = static_cast<int64_t>(std::max(sms, 1)) * 512 * 2;
-  const int64_t n_groups = std::min<int64_t>(32, std::max<int64_t>(1, s->n_slots / per_group));
-  if (n_groups < 2 || s->rods.size() < 2) return EB_OK;
+  // group sizes in waves of 512-slot CTAs: 1 and 2 at either end (their
+  // copies overlap no launch), equal groups of about four in between
+  const double units = static_cast<double>(s->n_slots) / (static_cast<double>(std::max(sms, 1)) * 512.0);
+  if (units < 2.0 || s->rods.size() < 2) return EB_OK;
+  std::vector<double> wts;
+  if (units >= 12.0) {
+    const double mid = units - 6.0;
+    const int m = std::max(1, static_cast<int>(std::llround(mid / 4.0)));
+    wts = {1.0, 2.0};
+    for (int i = 0; i < m; ++i) wts.push_back(mid / m);
+    wts.push_back(2.0);
+    wts.push_back(1.0);
+  } else {
+    wts.assign(static_cast<size_t>(units / 2.0), 1.0);
+  }
+  const int64_t n_groups = static_cast<int64_t>(wts.size());
+  if (n_groups < 2) return EB_OK;
+  std::vector<int64_t> bound(1, 0);
+  {
+    double tot = 0.0, acc = 0.0;
+    for (double w : wts) tot += w;
+    for (double w : wts) {
+      acc += w;
+      bound.push_back(static_cast<int64_t>(static_cast<double>(s->n_slots) * (acc / tot)));
+    }
+  }
   std::vector<std::vector<size_t>> members(1);
   std::vector<int64_t> cut(1, 0);
   for (size_t r = 0; r < s->rods.size(); ++r) {
     const int64_t j = static_cast<int64_t>(members.size());
-    if (!members.back().empty() && j < n_groups && s->offsets[r] >= j * s->n_slots / n_groups) {
+    if (!members.back().empty() && j < n_groups && s->offsets[r] >= bound[static_cast<size_t>(j)]) {
       members.emplace_back();
       cut.push_back(s->offsets[r]);
     }
