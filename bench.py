@@ -197,11 +197,11 @@ def bench_workload(args, W, rank, world):
     if world > 1:
         from elasticapp_b200 import dist as ebdist
         per = args.rods if args.rods is not None else 16384
-        return ebdist.shard(W.CONFIGS[args.workload](n_rods=per * world, seed=1002), rank, world)
+        return ebdist.shard(W.WORKLOADS[args.workload](n_rods=per * world, seed=1002), rank, world)
     kw = {"seed": 1002 + rank}
     if args.rods is not None:
         kw["n_rods"] = args.rods
-    return W.CONFIGS[args.workload](**kw)
+    return W.WORKLOADS[args.workload](**kw)
 
 
 def run_reference(args, W):

@@ -220,5 +220,5 @@ def contact_batch(n_rods: int = 8192, seed: int = 1004, n_elements: int = 64, bo
                     planes=unit_cube_walls(box))
 
 
-CONFIGS = {"cantilever": cantilever, "uneven_batch": uneven_batch, "mixed_batch": mixed_batch,
+WORKLOADS = {"cantilever": cantilever, "uneven_batch": uneven_batch, "mixed_batch": mixed_batch,
            "contact_batch": contact_batch}
