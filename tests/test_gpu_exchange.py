@@ -27,8 +27,8 @@ def pinned(shape):
 
 @pytest.fixture(scope="module")
 def batch():
-    # about 1.6 M slots: three groups of whole rods for the 520-slot
-    # configurations on 148 SMs
+    # about 1.6 M slots, 21 waves of 512-slot CTAs on 148 SMs: groups of
+    # 1, 2, about 4 ... 4, 2 and 1 waves
     return W.uneven_batch(n_rods=6000, seed=41, n_range=(32, 512), n_steps=200)
 
 
@@ -75,6 +75,27 @@ def test_exchange_equals_sequential_calls(batch, precision, config, n_steps):
     xch.step(eb.PositionVerlet(), t_x, batch.dt, 3)
     for name in STATE:
         assert np.array_equal(xch.get_slots(name), seq.get_slots(name)), name
+
+
+def test_exchange_equal_groups_equals_sequential_calls():
+    """A batch of fewer than twelve waves of 512-slot CTAs (about 440 k
+    slots on 148 SMs) is cut into equal groups instead of the tapered ones;
+    the result is the same bit for bit."""
+    wl = W.uneven_batch(n_rods=1600, seed=47, n_range=(32, 512), n_steps=200)
+    seq = planned(wl, step_mode="resident", resident_config=1)
+    xch = planned(wl, step_mode="resident", resident_config=1)
+    host = perturbed_state(seq, seed=7)
+    for name in STATE:
+        seq.set_slots(name, host[name])
+    t_seq = seq.step(eb.PositionVerlet(), 0.5, wl.dt, 200)
+    want = {name: seq.get_slots(name) for name in STATE}
+    out = {name: pinned(host[name].shape) for name in STATE}
+    before = xch.launch_count()
+    t_x = xch.step_host_state(eb.PositionVerlet(), 0.5, wl.dt, 200, inputs=host, outputs=out)
+    assert xch.launch_count() - before >= 2 * 2  # two chunks in each of at least two groups
+    assert t_x == t_seq
+    for name in STATE:
+        assert np.array_equal(out[name], want[name]), name
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
