@@ -18,9 +18,9 @@
 //   3. pairs_kernel<0>: every capsule tests the capsules filed in its 27
 //      neighbouring cells, then every plane, in one pass, writing up to
 //      kFixedPartners partners into its fixed-stride list (sorted) and its
-//      count; pairs_kernel<1> (after a scan of the larger counts) writes the
-//      whole sorted list of a capsule with more partners into the overflow
-//      lists.  Two boxes that overlap have lower corners less
+//      count; a capsule with more partners takes a region of the overflow
+//      lists (one atomic on their total), and pairs_kernel<1> writes its
+//      whole sorted list there.  Two boxes that overlap have lower corners less
 //      than one cell apart on each axis, so the candidate set equals the
 //      exhaustive search's (Detection/Coarse/ExhaustiveSearch.hpp:322-435,
 //      closed intervals of BoundingBox.hpp:532-540), which the reference's
@@ -226,7 +226,6 @@ __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
   if (!finite) {
     a.bucket[s] = 0xffffffffu;
     a.pair_count[s] = 0;
-    a.ovf_count[s] = 0;
     return;
   }
   const double ih = inverse_cell(a);
@@ -277,17 +276,17 @@ __device__ __forceinline__ void sort_ids(int32_t* v, int32_t n) {
   }
 }
 
-// kPass 0: count and fill the fixed-stride list; kPass 1: overflow lists of
-// the capsules with more than kFixedPartners partners.  The search is bound
-// by dependent round trips to L2: every entry of a neighbouring bucket is
-// one 64-byte record read whole before it is tested (its cell, slot and box
-// were three dependent loads when kept in separate arrays), and the bucket
-// range of the next neighbouring cell is loaded while the current one's
-// entries are scanned.
-// kPass 0 runs a thread per filed entry and takes the capsule's cell and box
-// from its record; kPass 1 runs a thread per slot and leaves at once unless
-// the slot's count (coalesced) is above kFixedPartners, taking the cell and
-// box from the slot-major rows the records were written from.
+// The search of one capsule.  kPass 0 (idx: a filed entry, the capsule's
+// cell and box from its record) counts the partners and fills the
+// fixed-stride list; kPass 1 (idx: a slot, leaving at once unless its
+// coalesced count is above kFixedPartners; the cell and box from the
+// slot-major rows the records were written from) writes the overflow list of
+// a capsule with more partners.  The search is bound by dependent round
+// trips to L2: every entry of a neighbouring bucket is one 64-byte record
+// read whole before it is tested (its cell, slot and box were three
+// dependent loads when kept in separate arrays), and the bucket range of the
+// next neighbouring cell is loaded while the current one's entries are
+// scanned.
 template <int kPass>
 __device__ __forceinline__ void search_one(const ContactArgs& a, int32_t n_caps, int64_t idx) {
   int32_t id, cx, cy, cz;
@@ -367,7 +366,11 @@ __device__ __forceinline__ void search_one(const ContactArgs& a, int32_t n_caps,
   }
   if (kPass == 0) {
     a.pair_count[id] = cnt;
-    a.ovf_count[id] = cnt > kFixedPartners ? cnt : 0;
+    // a capsule with more partners takes a region of the overflow lists
+    // (in whatever order the atomics come; every list is whole and sorted)
+    if (cnt > kFixedPartners)
+      a.pair_offset[id] = static_cast<int64_t>(atomicAdd(
+          reinterpret_cast<unsigned long long*>(a.pair_offset + a.n_slots), static_cast<unsigned long long>(cnt)));
     if (cnt <= kFixedPartners) sort_ids(out, cnt);  // ascending partner order
   } else {
     sort_ids(out, cnt);
@@ -714,6 +717,9 @@ cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* l
   const unsigned gs = static_cast<unsigned>((a.n_slots + kThreads - 1) / kThreads);
   cudaError_t e = cudaMemsetAsync(a.extent_bits, 0, sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
+  // the running total of the overflow lists
+  e = cudaMemsetAsync(a.pair_offset + a.n_slots, 0, sizeof(int64_t), stream);
+  if (e != cudaSuccess) return e;
   // the bucket counts: the scatter of the previous evaluation left them at
   // the bucket sizes
   const int64_t table = static_cast<int64_t>(a.table_mask) + 1;
@@ -734,8 +740,6 @@ cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* l
   const unsigned pblocks = static_cast<unsigned>(std::min<int64_t>(ge, static_cast<int64_t>(psms) * std::max(pper, 1)));
   if (ge > 0) pairs_kernel<0><<<pblocks, kThreads, 0, stream>>>(a, a.n_caps);
   *launches += 2;
-  e = exclusive_scan<int64_t>(a.ovf_count, a.pair_offset, a.n_slots, a.scan_blocks, false, stream, launches);
-  if (e != cudaSuccess) return e;
   pairs_kernel<1><<<gs, kThreads, 0, stream>>>(a, a.n_caps);
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -67,8 +67,8 @@ struct ContactArgs {
   double* sorted_rec;                // kSortedRecDoubles per entry
   int32_t* pair_count;               // stride (zero outside capsules): partners per capsule
   int32_t* fixed;                    // kFixedPartners x stride: partner lists of up to kFixedPartners
-  int32_t* ovf_count;                // stride: the count of capsules beyond kFixedPartners, else 0
-  int64_t* pair_offset;              // n_slots + 1: offsets of the overflow lists
+  int64_t* pair_offset;              // n_slots + 1: a capsule's overflow list (if it has more than
+                                     // kFixedPartners partners); [n_slots] their total
   int32_t* partners;                 // capacity: overflow lists
   int64_t capacity;
   unsigned long long* required;      // largest pair total seen when over capacity

@@ -136,7 +136,6 @@ struct ContactDevice {
   double* sorted_rec = nullptr;
   int32_t* pair_count = nullptr;
   int32_t* fixed = nullptr;
-  int32_t* ovf_count = nullptr;
   int64_t* pair_offset = nullptr;
   int32_t* partners = nullptr;
   unsigned long long* required = nullptr;
@@ -446,7 +445,7 @@ void host_free(eb_sim* s) {
     }
   ContactDevice& c = s->contact;
   void* cptrs[] = {c.cap, c.cap_material, c.extent, c.cell, c.bucket, c.bucket_count, c.bucket_start,
-                   c.sorted_rec, c.pair_count, c.fixed, c.ovf_count, c.pair_offset,
+                   c.sorted_rec, c.pair_count, c.fixed, c.pair_offset,
                    c.partners,
                    c.required, c.planes, c.pair_table, c.loads, c.scan_blocks, c.backup};
   for (void* p : cptrs)
@@ -579,7 +578,6 @@ eb_status setup_contact(eb_sim* s) {
   alloc(&c.sorted_rec, static_cast<size_t>(eb::kSortedRecDoubles * n_caps) * sizeof(double));
   alloc(&c.pair_count, static_cast<size_t>(S) * sizeof(int32_t));
   alloc(&c.fixed, static_cast<size_t>(S) * eb::kFixedPartners * sizeof(int32_t));
-  alloc(&c.ovf_count, static_cast<size_t>(S) * sizeof(int32_t));
   alloc(&c.pair_offset, static_cast<size_t>(s->n_slots + 1) * sizeof(int64_t));
   alloc(&c.partners, static_cast<size_t>(c.capacity) * sizeof(int32_t));
   alloc(&c.required, sizeof(unsigned long long));
@@ -1729,7 +1727,6 @@ eb::ContactArgs contact_args(eb_sim* s, double dt) {
   a.sorted_rec = c.sorted_rec;
   a.pair_count = c.pair_count;
   a.fixed = c.fixed;
-  a.ovf_count = c.ovf_count;
   a.pair_offset = c.pair_offset;
   a.partners = c.partners;
   a.capacity = c.capacity;
