@@ -239,7 +239,9 @@ __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
   }
   const uint32_t b = cell_hash(c[0], c[1], c[2]) & a.table_mask;
   a.bucket[s] = b;
-  atomicAdd(a.bucket_count + b, 1);
+  // the capsule's rank in its bucket, kept in its pair count until the
+  // scatter has filed it (the pair search then writes the count)
+  a.pair_count[s] = atomicAdd(a.bucket_count + b, 1);
 }
 
 __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) {
@@ -248,8 +250,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) 
   const int64_t S = a.stride;
   const uint32_t b = a.bucket[s];
   if (b > a.table_mask) return;  // excluded (not finite)
-  // bucket_count was zeroed by the scan and now serves as the fill cursor
-  const int32_t pos = a.bucket_start[b] + atomicAdd(a.bucket_count + b, 1);
+  const int32_t pos = a.bucket_start[b] + a.pair_count[s];  // the rank the cell kernel took
   if (pos < 0 || pos >= a.n_caps) {  // cannot happen with consistent counts; never write out of range
     atomicOr(a.status, kStatusContactIndex);
     return;
@@ -720,11 +721,9 @@ cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* l
   // the running total of the overflow lists
   e = cudaMemsetAsync(a.pair_offset + a.n_slots, 0, sizeof(int64_t), stream);
   if (e != cudaSuccess) return e;
-  // the bucket counts: the scatter of the previous evaluation left them at
-  // the bucket sizes
+  // the bucket counts are zero here: allocated zeroed, and the scan sets
+  // each back to zero as it reads it
   const int64_t table = static_cast<int64_t>(a.table_mask) + 1;
-  e = cudaMemsetAsync(a.bucket_count, 0, static_cast<size_t>(table) * sizeof(int32_t), stream);
-  if (e != cudaSuccess) return e;
   capsule_kernel<<<gs, kThreads, 0, stream>>>(a);
   cell_kernel<<<gs, kThreads, 0, stream>>>(a);
   *launches += 2;

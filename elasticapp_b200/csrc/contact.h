@@ -65,7 +65,8 @@ struct ContactArgs {
   // (3 x int32) and slot (int32) in the first 16 bytes, then the box's lower
   // and upper corners (6 doubles)
   double* sorted_rec;                // kSortedRecDoubles per entry
-  int32_t* pair_count;               // stride (zero outside capsules): partners per capsule
+  int32_t* pair_count;               // stride (zero outside capsules): partners per capsule (between
+                                     // the cell kernel and the scatter: the capsule's rank in its bucket)
   int32_t* fixed;                    // kFixedPartners x stride: partner lists of up to kFixedPartners
   int64_t* pair_offset;              // n_slots + 1: a capsule's overflow list (if it has more than
                                      // kFixedPartners partners); [n_slots] their total
