@@ -1806,11 +1806,13 @@ eb_status step_with_contact(eb_sim* s, double dt, int64_t n_steps, bool diag) {
       continue;
     }
     uint32_t st = 0;
-    unsigned long long req = 0;
     EB_CUDA(cudaMemcpyAsync(&st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
-    EB_CUDA(cudaMemcpyAsync(&req, c.required, sizeof(req), cudaMemcpyDeviceToHost, s->stream));
     EB_CUDA(cudaStreamSynchronize(s->stream));
     if (st & eb::kStatusPairOverflow) {
+      // the pair total the lists needed, read only when they did not fit
+      unsigned long long req = 0;
+      EB_CUDA(cudaMemcpyAsync(&req, c.required, sizeof(req), cudaMemcpyDeviceToHost, s->stream));
+      EB_CUDA(cudaStreamSynchronize(s->stream));
       if (++regrowths > 8) return fail(EB_ERR_OUT_OF_MEMORY, "candidate pair buffer keeps overflowing");
       const int64_t want = std::max<int64_t>(2 * c.capacity, static_cast<int64_t>(req) + req / 2);
       if (want >= (int64_t(1) << 31)) return fail(EB_ERR_UNSUPPORTED, "more than 2^31 candidate pairs");
