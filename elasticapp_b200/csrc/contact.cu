@@ -213,6 +213,7 @@ __device__ __forceinline__ double inverse_cell(const ContactArgs& a) {
 
 __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
   const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (s == 0) a.pair_offset[a.n_slots] = 0;  // the pair search's overflow total
   if (s >= a.n_slots || a.cap_material[s] < 0) return;
   const int64_t S = a.stride;
   // a capsule whose box is not finite (a diverged state, already flagged by
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(kThreads) cell_kernel(const ContactArgs a) {
 
 __global__ void __launch_bounds__(kThreads) scatter_kernel(const ContactArgs a) {
   const int64_t s = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+  if (s == 0) *a.extent_bits = 0;  // read only by the cell kernel: zero for the next evaluation
   if (s >= a.n_slots || a.cap_material[s] < 0) return;
   const int64_t S = a.stride;
   const uint32_t b = a.bucket[s];
@@ -716,13 +718,11 @@ int64_t contact_scan_blocks(int64_t n) { return (n + kScanBlock - 1) / kScanBloc
 cudaError_t launch_contact(const ContactArgs& a, cudaStream_t stream, int64_t* launches) {
   if (a.n_slots <= 0) return cudaSuccess;
   const unsigned gs = static_cast<unsigned>((a.n_slots + kThreads - 1) / kThreads);
-  cudaError_t e = cudaMemsetAsync(a.extent_bits, 0, sizeof(unsigned long long), stream);
-  if (e != cudaSuccess) return e;
-  // the running total of the overflow lists
-  e = cudaMemsetAsync(a.pair_offset + a.n_slots, 0, sizeof(int64_t), stream);
-  if (e != cudaSuccess) return e;
-  // the bucket counts are zero here: allocated zeroed, and the scan sets
-  // each back to zero as it reads it
+  // the largest box extent and the bucket counts are zero here: allocated
+  // zeroed, the extent set back to zero by the scatter once the cell kernel
+  // has used it, and each count by the scan as it reads it; the cell kernel
+  // zeroes the overflow lists' running total
+  cudaError_t e = cudaSuccess;
   const int64_t table = static_cast<int64_t>(a.table_mask) + 1;
   capsule_kernel<<<gs, kThreads, 0, stream>>>(a);
   cell_kernel<<<gs, kThreads, 0, stream>>>(a);
