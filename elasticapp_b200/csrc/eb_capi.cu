@@ -548,7 +548,10 @@ eb_status setup_contact(eb_sim* s) {
   c.on = true;
   c.n_caps = static_cast<int32_t>(n_caps);
   int64_t table = 1024;
-  while (table < 2 * n_caps) table <<= 1;
+  // at least four buckets a capsule: every entry of another cell that shares
+  // a neighbour's bucket is one more dependent read in the pair search
+  // (contact step 0.646 -> 0.633 ms against two a capsule; eight: 0.645 ms)
+  while (table < 4 * n_caps) table <<= 1;
   c.table_mask = static_cast<uint32_t>(table - 1);
   c.capacity = std::max<int64_t>(int64_t(1) << 16, 4 * n_caps);  // overflow lists only
   const size_t nm = s->materials.size();
