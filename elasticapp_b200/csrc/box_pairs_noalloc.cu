@@ -19,8 +19,7 @@
 //   status) before use.  Calls whose GPU work overlaps (two streams, two host
 //   threads) race on it and give wrong results: serialise them;
 // * the first call on a device looks up the array's device address (with that
-//   device current) and caches it; make that first call before any stream
-//   capture begins.
+//   device current) and caches it for later calls.
 #include <cuda_runtime.h>
 
 #include <cstdint>

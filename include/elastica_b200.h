@@ -544,14 +544,15 @@ EB_API eb_status eb_server_request_status(const struct eb_server* server, int64_
  * (larger counts are rejected with EB_ERR_INVALID_ARGUMENT).  The grid's cell
  * edge is the largest box extent: with very uneven extents (one box spanning
  * the others) most boxes share a cell and the search costs up to O(n^2)
- * overlap tests.  pairs: device
+ * overlap tests; each box's partners are then sorted in place by one thread,
+ * O(cnt^2) for a box with cnt partners.  pairs: device
  * pointer to capacity pairs of int64 (i, j), i < j; the overlapping pairs are
  * written sorted by i then j.  *count (host) receives their number; when it
  * exceeds capacity nothing is written and EB_ERR_INVALID_ARGUMENT is
  * returned.  stream: a cudaStream_t of the current device (NULL = default
  * stream); the call returns after its work on the stream has finished.
  * The first call on a device finds the device address of the working array
- * (make it before any stream capture begins).  Every call shares that array:
+ * and keeps it for later calls.  Every call shares that array:
  * calls whose GPU work overlaps (other streams or host threads) race and must
  * be serialised by the caller. */
 EB_API eb_status eb_box_pairs_noalloc(const double* boxes, int64_t n_boxes, int64_t* pairs, int64_t capacity,
